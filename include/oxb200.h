@@ -1,0 +1,371 @@
+/*
+ * oxb200.h — C ABI of the B200 (sm_100a) GPU operator path of OxideLake.
+ *
+ * The entry points mirror, one to one, the object-safe `GpuBackend` trait of
+ * the reference (crates/oxidelake-device/src/backend.rs:44-198) and its
+ * argument bundles (crates/oxidelake-device/src/args.rs:10-86), so a Rust
+ * `extern "C"` binding can implement the trait over this library without any
+ * change to the `Gpu*Exec` plans above it.  Every signature uses plain C
+ * types, pointers and sizes.
+ *
+ * Conventions (crates/oxidelake-device/src/columns.rs:28-40):
+ *   - a column's values are tightly packed from row 0;
+ *   - a validity bitmap is LSB-first, bit 0 = row 0, re-based to bit 0;
+ *     a NULL validity pointer means "every row valid";
+ *   - a FixedSizeList<Float32, dim> column stores dim floats per row.
+ * Every call is synchronous towards the host unless it says otherwise (work
+ * is ordered on the stream it is given); every call is thread-safe.  A call
+ * that fails returns a status other than OXB_OK and leaves a message that
+ * oxb_last_error() returns on the calling thread.  No entry point falls
+ * back to the CPU: OXB_UNSUPPORTED is returned only for shapes outside
+ * coverage, exactly where the reference's backend returns
+ * EngineError::Unsupported (crates/oxidelake-core/src/error.rs:56-64).
+ */
+#ifndef OXB200_H
+#define OXB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define OXB_API __attribute__((visibility("default")))
+#else
+#define OXB_API
+#endif
+
+#define OXB_ABI_VERSION 1
+
+/* EngineError, crates/oxidelake-core/src/error.rs:17-73, plus the device-path
+ * statuses the reference has no variant for. */
+typedef enum oxb_status {
+    OXB_OK = 0,
+    OXB_UNSUPPORTED = 1,   /* EngineError::Unsupported: caller may take its CPU path */
+    OXB_DEVICE = 2,        /* EngineError::Device: a CUDA call failed */
+    OXB_EXECUTION = 3,     /* EngineError::Execution */
+    OXB_PLAN = 4,          /* EngineError::Plan: bad column index, type, shape */
+    OXB_ALLOCATION = 5,    /* EngineError::Allocation: device or pinned allocation failed */
+    OXB_OOM_ADMISSION = 6, /* serving: a request's estimated memory exceeds the budget */
+    OXB_TABLE_FULL = 7,    /* a device hash table ran out of slots */
+    OXB_TIMEOUT = 8        /* a bounded device wait gave up */
+} oxb_status;
+
+/* Arrow types the path reads (crates/oxidelake-core/src/params.rs:170-182,
+ * widened by Int32). */
+typedef enum oxb_type {
+    OXB_TYPE_INT64 = 1,
+    OXB_TYPE_FLOAT64 = 2,
+    OXB_TYPE_INT32 = 3,
+    OXB_TYPE_FLOAT32 = 4,
+    OXB_TYPE_VECTOR_F32 = 5 /* FixedSizeList<Float32, dim> */
+} oxb_type;
+
+/* Comparison, crates/oxidelake-core/src/params.rs:12-23. */
+typedef enum oxb_cmp {
+    OXB_CMP_EQ = 0,
+    OXB_CMP_LT = 1,
+    OXB_CMP_LTEQ = 2,
+    OXB_CMP_GT = 3,
+    OXB_CMP_GTEQ = 4
+} oxb_cmp;
+
+/* AggregateFunction, crates/oxidelake-core/src/params.rs:117-126, widened by
+ * AVG and COUNT(*) (DataFusion semantics: AVG -> Float64, COUNT(*) counts rows). */
+typedef enum oxb_agg_func {
+    OXB_AGG_SUM = 0,
+    OXB_AGG_COUNT = 1,
+    OXB_AGG_MIN = 2,
+    OXB_AGG_MAX = 3,
+    OXB_AGG_AVG = 4,
+    OXB_AGG_COUNT_STAR = 5
+} oxb_agg_func;
+
+/* DistanceMetric, crates/oxidelake-core/src/params.rs:151-156. */
+typedef enum oxb_metric { OXB_METRIC_L2 = 0, OXB_METRIC_COSINE = 1 } oxb_metric;
+
+/* One column, host- or device-resident (which one is said by the call). */
+typedef struct oxb_column {
+    int32_t type;            /* oxb_type */
+    int32_t dim;             /* list size for OXB_TYPE_VECTOR_F32, else 1 */
+    int64_t length;          /* rows */
+    const void* values;      /* length * width bytes, width = 8, 4 or 4 * dim */
+    const uint8_t* validity; /* ceil(length / 8) bytes, or NULL = all valid */
+} oxb_column;
+
+/* One comparison leaf of a predicate: `column <op> literal`.  A predicate is
+ * the AND of its leaves (Predicate::And of Predicate::Compare,
+ * crates/oxidelake-core/src/params.rs:60-72; a WHERE keeps a row only when
+ * every leaf is true, so the AND-tree flattens exactly).  The literal type
+ * must equal the column type, else the call returns OXB_UNSUPPORTED as the
+ * reference's evaluate_predicate does (cpu/kernels.rs:110-119). */
+typedef struct oxb_leaf {
+    int32_t column;
+    int32_t op;       /* oxb_cmp */
+    int32_t lit_type; /* OXB_TYPE_INT64, OXB_TYPE_FLOAT64 or OXB_TYPE_INT32 */
+    int32_t reserved;
+    union {
+        int64_t i;
+        double f;
+    } lit;
+} oxb_leaf;
+
+/* Most leaves one predicate may have (crates/oxidelake-compute/src/exec/mod.rs:31). */
+#define OXB_MAX_PREDICATE_LEAVES 64
+/* Most aggregates one grouped aggregation may compute. */
+#define OXB_MAX_AGGREGATES 16
+
+typedef struct oxb_backend oxb_backend;           /* CudaBackend: one device */
+typedef struct oxb_stream oxb_stream;             /* DeviceStream */
+typedef struct oxb_buffer oxb_buffer;             /* DeviceBuffer */
+typedef struct oxb_host_buffer oxb_host_buffer;   /* HostBuffer */
+typedef struct oxb_batch oxb_batch;               /* DeviceBatch */
+typedef struct oxb_join_table oxb_join_table;     /* DeviceJoinTable */
+typedef struct oxb_join_matches oxb_join_matches; /* DeviceJoinMatches */
+typedef struct oxb_vector_index oxb_vector_index; /* resident BF16 copy for top-k */
+
+/* MemoryInfo, crates/oxidelake-device/src/backend.rs:18-26. */
+typedef struct oxb_memory_info {
+    uint64_t total_bytes;
+    uint64_t free_bytes;
+    int32_t pinned_supported;
+    int32_t reserved;
+} oxb_memory_info;
+
+/* ---- errors and version ------------------------------------------------ */
+
+/* Message of the last failed call on this thread ("" when none). */
+OXB_API const char* oxb_last_error(void);
+OXB_API int32_t oxb_abi_version(void);
+
+/* ---- backend lifecycle (HardwareDetector::select -> CudaBackend::new,
+ *      crates/oxidelake-device/src/cuda/mod.rs:344) ---------------------- */
+
+OXB_API oxb_status oxb_backend_create(int32_t device, oxb_backend** out);
+OXB_API void oxb_backend_destroy(oxb_backend* backend);
+/* GpuBackend::kind (backend.rs:46): "cuda". */
+OXB_API const char* oxb_backend_kind(const oxb_backend* backend);
+/* GpuBackend::device_id (backend.rs:49). */
+OXB_API int32_t oxb_backend_device_id(const oxb_backend* backend);
+/* GpuBackend::memory_info (backend.rs:52). */
+OXB_API oxb_status oxb_memory_info_get(oxb_backend* backend, oxb_memory_info* out);
+
+/* ---- memory (backend.rs:55-59) ---------------------------------------- */
+
+/* GpuBackend::alloc_device: zeroed, 256-byte aligned (>= the 128 the
+ * reference requires, crates/oxidelake-core/src/layout.rs:9). */
+OXB_API oxb_status oxb_alloc_device(oxb_backend* backend, size_t bytes, oxb_buffer** out);
+OXB_API void* oxb_buffer_device_ptr(const oxb_buffer* buffer);
+OXB_API size_t oxb_buffer_len(const oxb_buffer* buffer);
+OXB_API void oxb_buffer_free(oxb_buffer* buffer);
+/* GpuBackend::alloc_pinned_host: page-locked when possible. */
+OXB_API oxb_status oxb_alloc_pinned_host(oxb_backend* backend, size_t bytes, oxb_host_buffer** out);
+OXB_API void* oxb_host_buffer_ptr(const oxb_host_buffer* buffer);
+OXB_API size_t oxb_host_buffer_len(const oxb_host_buffer* buffer);
+OXB_API int32_t oxb_host_buffer_is_pinned(const oxb_host_buffer* buffer);
+OXB_API void oxb_host_buffer_free(oxb_host_buffer* buffer);
+
+/* ---- streams and transfers (backend.rs:62-81) -------------------------- */
+
+OXB_API oxb_status oxb_stream_create(oxb_backend* backend, oxb_stream** out);
+/* Wraps a caller-owned cudaStream_t (not destroyed by oxb_stream_destroy). */
+OXB_API oxb_status oxb_stream_wrap(oxb_backend* backend, void* cuda_stream, oxb_stream** out);
+OXB_API void* oxb_stream_cuda_handle(const oxb_stream* stream);
+OXB_API oxb_status oxb_stream_synchronize(oxb_backend* backend, oxb_stream* stream);
+OXB_API void oxb_stream_destroy(oxb_stream* stream);
+/* GpuBackend::copy_h2d / copy_d2h: whole buffers, min of the two lengths. */
+OXB_API oxb_status oxb_copy_h2d(oxb_backend* backend, oxb_stream* stream, const oxb_host_buffer* src,
+                        oxb_buffer* dst);
+OXB_API oxb_status oxb_copy_d2h(oxb_backend* backend, oxb_stream* stream, const oxb_buffer* src,
+                        oxb_host_buffer* dst);
+
+/* ---- batches (backend.rs:84-95; handles.rs:130) ------------------------ */
+
+/* GpuBackend::upload: copies `ncols` host columns of `rows` rows to the
+ * device.  Queued on `stream`; the host buffers must stay alive until the
+ * stream is synchronized. */
+OXB_API oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column* columns,
+                      int32_t ncols, int64_t rows, oxb_batch** out);
+/* A batch over columns already in device memory (no copy; the caller keeps
+ * the memory alive for the batch's lifetime). */
+OXB_API oxb_status oxb_batch_from_device(oxb_backend* backend, const oxb_column* columns, int32_t ncols,
+                                 int64_t rows, oxb_batch** out);
+OXB_API int64_t oxb_batch_num_rows(const oxb_batch* batch);
+OXB_API int32_t oxb_batch_num_columns(const oxb_batch* batch);
+/* The device-side descriptor of column `index` (device pointers). */
+OXB_API oxb_status oxb_batch_column(const oxb_batch* batch, int32_t index, oxb_column* out);
+/* GpuBackend::download, column by column: copies column `index` into
+ * caller-allocated host memory (values: length * width bytes; validity:
+ * ceil(length / 8) bytes, written only when the column has a bitmap, which
+ * *has_validity reports).  Synchronizes `stream`. */
+OXB_API oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch,
+                               int32_t index, void* values, uint8_t* validity,
+                               int32_t* has_validity);
+OXB_API void oxb_batch_free(oxb_batch* batch);
+
+/* ---- operators --------------------------------------------------------- */
+
+/* FilterProjectArgs, args.rs:10-15 -> GpuBackend::filter_project
+ * (backend.rs:98).  Rows where every leaf is true, projected columns in
+ * projection order, row order kept. */
+typedef struct oxb_filter_project_args {
+    const oxb_batch* input;
+    const oxb_leaf* leaves;
+    int32_t nleaves;
+    const int32_t* projection;
+    int32_t nprojection;
+} oxb_filter_project_args;
+OXB_API oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream,
+                              const oxb_filter_project_args* args, oxb_batch** out);
+
+/* The host's index of a build side (cpu::kernels::JoinTable::runs and
+ * row_indices, cpu/kernels.rs:245-255): `ndistinct` runs (key, start,
+ * count) into `rows`, which groups the build rows with a non-NULL key by
+ * key, in build order.  JoinBuildArgs::index (args.rs:21-30). */
+typedef struct oxb_join_index {
+    const int64_t* keys;
+    const uint32_t* starts;
+    const uint32_t* counts;
+    int64_t ndistinct;
+    const uint32_t* rows;
+    int64_t nrows;
+} oxb_join_index;
+
+/* JoinBuildArgs -> GpuBackend::prepare_join_build (backend.rs:129).  With
+ * `index` NULL the device builds the same index itself from the key column
+ * (a stable sort by key keeps build order within a key). */
+typedef struct oxb_join_build_args {
+    const oxb_batch* build;
+    int32_t key;
+    int32_t reserved;
+    const oxb_join_index* index;
+} oxb_join_build_args;
+OXB_API oxb_status oxb_prepare_join_build(oxb_backend* backend, oxb_stream* stream,
+                                  const oxb_join_build_args* args, oxb_join_table** out);
+OXB_API int64_t oxb_join_table_distinct_keys(const oxb_join_table* table);
+OXB_API int64_t oxb_join_table_rows(const oxb_join_table* table);
+OXB_API void oxb_join_table_free(oxb_join_table* table);
+
+/* JoinProbeArgs -> GpuBackend::probe_join (backend.rs:153).  Matches are
+ * numbered in probe-row order, then build order (backend.rs:148-152). */
+typedef struct oxb_join_probe_args {
+    const oxb_batch* probe;
+    int32_t key;
+    int32_t reserved;
+    const oxb_join_table* table;
+} oxb_join_probe_args;
+OXB_API oxb_status oxb_probe_join(oxb_backend* backend, oxb_stream* stream,
+                          const oxb_join_probe_args* args, oxb_join_matches** out);
+OXB_API uint64_t oxb_join_matches_len(const oxb_join_matches* matches);
+OXB_API int64_t oxb_join_matches_probe_rows(const oxb_join_matches* matches);
+OXB_API void oxb_join_matches_free(oxb_join_matches* matches);
+
+/* HashJoinArgs -> GpuBackend::hash_join (backend.rs:114): matches
+ * first..first+rows as left columns ++ right columns, or the `projection`
+ * subset of that concatenation (NULL = all). */
+typedef struct oxb_hash_join_args {
+    const oxb_batch* left;
+    const oxb_batch* right;
+    const oxb_join_table* table;
+    const oxb_join_matches* matches;
+    uint64_t first;
+    uint64_t rows;
+    const int32_t* projection;
+    int32_t nprojection;
+    int32_t reserved;
+} oxb_hash_join_args;
+OXB_API oxb_status oxb_hash_join(oxb_backend* backend, oxb_stream* stream,
+                         const oxb_hash_join_args* args, oxb_batch** out);
+
+/* AggregateSpec, params.rs:142-147 -> AggregateArgs, args.rs:64-69 ->
+ * GpuBackend::aggregate (backend.rs:166).  Output: the key (nullable Int64
+ * or Int32, as the key column) then one column per aggregate, groups sorted
+ * by key with the NULL group last (crates/oxidelake-device/src/cuda/ops.rs:1037;
+ * cpu/kernels.rs:793-811).  Types: SUM(Int64|Int32) -> Int64 (wrapping),
+ * SUM(Float64) -> Float64, COUNT/COUNT(*) -> Int64, MIN/MAX keep the input
+ * type, AVG -> Float64.  For OXB_AGG_COUNT_STAR the column is ignored. */
+typedef struct oxb_aggregate_spec {
+    int32_t group_by;
+    int32_t naggregates;
+    int32_t funcs[OXB_MAX_AGGREGATES];   /* oxb_agg_func */
+    int32_t columns[OXB_MAX_AGGREGATES];
+} oxb_aggregate_spec;
+typedef struct oxb_aggregate_args {
+    const oxb_batch* input;
+    const oxb_aggregate_spec* spec;
+    /* Optional fused WHERE over `input` (NULL/0 = every row). */
+    const oxb_leaf* leaves;
+    int32_t nleaves;
+    int32_t reserved;
+} oxb_aggregate_args;
+OXB_API oxb_status oxb_aggregate(oxb_backend* backend, oxb_stream* stream,
+                         const oxb_aggregate_args* args, oxb_batch** out);
+
+/* VectorDistanceArgs, args.rs:72-84 -> GpuBackend::vector_distance
+ * (backend.rs:173): the input columns plus a Float32 distance column with
+ * the vector column's validity.  Distances follow cpu/kernels.rs:909-927
+ * bit for bit (Float32, summed in index order). */
+typedef struct oxb_vector_distance_args {
+    const oxb_batch* input;
+    int32_t column;
+    int32_t metric; /* oxb_metric */
+    const float* query; /* host pointer, dim floats */
+    int32_t dim;
+    int32_t reserved;
+} oxb_vector_distance_args;
+OXB_API oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream,
+                               const oxb_vector_distance_args* args, oxb_batch** out);
+
+/* ---- new forms beside the drop-in path --------------------------------- */
+
+/* One pass of `probe JOIN build ON probe.key = build.key WHERE <leaves on
+ * probe columns> GROUP BY <one column of either side>` computing the listed
+ * aggregates, over a join table prepared on `build`.  It has no counterpart
+ * in the reference, where this query runs as GpuHashJoinExec (probe_join +
+ * hash_join chunks, backend.rs:114-163) followed by an aggregate over the
+ * joined rows (cpu/kernels.rs:679-811); the output equals that plan's:
+ * groups sorted by key, NULL last, types as oxb_aggregate.  Sides: 0 =
+ * probe, 1 = build. */
+typedef struct oxb_join_aggregate_args {
+    const oxb_batch* probe;
+    int32_t probe_key;
+    int32_t reserved;
+    const oxb_join_table* table;
+    const oxb_batch* build;
+    const oxb_leaf* leaves;
+    int32_t nleaves;
+    int32_t group_side;
+    int32_t group_column;
+    int32_t naggregates;
+    int32_t funcs[OXB_MAX_AGGREGATES];
+    int32_t sides[OXB_MAX_AGGREGATES];
+    int32_t columns[OXB_MAX_AGGREGATES];
+} oxb_join_aggregate_args;
+OXB_API oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream,
+                              const oxb_join_aggregate_args* args, oxb_batch** out);
+
+/* ---- instrumentation (no counterpart in the reference) ------------------ */
+
+/* When enabled, each operator records CUDA events on its stream around its
+ * main kernel; oxb_last_kernel_time returns that kernel's name and duration
+ * for the last operator call on this thread. */
+OXB_API oxb_status oxb_set_kernel_timing(oxb_backend* backend, int32_t enabled);
+OXB_API oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_t name_len,
+                                        float* ms);
+/* Kernels this library has launched in this process. */
+OXB_API uint64_t oxb_kernel_launches(void);
+
+/* GpuBackend::supports_predicate / supports_hash_join / supports_aggregate
+ * (backend.rs:182-197): 1 when the call runs on the device. */
+OXB_API int32_t oxb_supports_predicate(const oxb_backend* backend, const oxb_leaf* leaves,
+                               int32_t nleaves);
+OXB_API int32_t oxb_supports_hash_join(const oxb_backend* backend);
+OXB_API int32_t oxb_supports_aggregate(const oxb_backend* backend);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OXB200_H */

@@ -1,0 +1,521 @@
+// The C ABI of liboxb200 (include/oxb200.h): handle lifetimes, memory,
+// streams, transfers, and the operator entry points.  Every entry point
+// catches the runtime's errors at the boundary, records the message for
+// oxb_last_error() and returns the status; nothing throws across the ABI
+// and nothing falls back to the CPU.
+#include <cstdio>
+#include <new>
+
+#include "internal.h"
+
+namespace oxb {
+
+namespace {
+thread_local std::string g_last_error;
+thread_local std::string g_last_kernel;
+thread_local float g_last_kernel_ms = 0.0f;
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+KernelTimer::KernelTimer(const Backend& b, const StreamRef& s, const char* name)
+    : on_(b.timing), name_(name), stream_(s->stream) {
+    if (on_) {
+        OXB_CUDA(cudaEventCreate(&start_));
+        OXB_CUDA(cudaEventCreate(&stop_));
+    }
+}
+
+void KernelTimer::begin() {
+    if (on_) OXB_CUDA(cudaEventRecord(start_, stream_));
+}
+
+void KernelTimer::end() {
+    if (on_) {
+        OXB_CUDA(cudaEventRecord(stop_, stream_));
+        ended_ = true;
+    }
+}
+
+KernelTimer::~KernelTimer() {
+    if (!on_) return;
+    if (ended_ && cudaEventSynchronize(stop_) == cudaSuccess) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, start_, stop_) == cudaSuccess) {
+            g_last_kernel = name_;
+            g_last_kernel_ms = ms;
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(start_);
+    cudaEventDestroy(stop_);
+}
+
+void fail(oxb_status status, const std::string& message) { throw Error{status, message}; }
+
+void check_cuda(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return;
+    cudaGetLastError();  // clear a non-sticky error so the context stays usable
+    fail(err == cudaErrorMemoryAllocation ? OXB_ALLOCATION : OXB_DEVICE,
+         std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+void check_status_word(uint32_t status, const char* what) {
+    if (status & kStatusTableFull) fail(OXB_TABLE_FULL, std::string(what) + ": device hash table full");
+    if (status & kStatusTimeout) fail(OXB_TIMEOUT, std::string(what) + ": a bounded device wait gave up");
+    if (status & kStatusBounds) fail(OXB_EXECUTION, std::string(what) + ": an index failed its bounds check");
+}
+
+StreamState::~StreamState() {
+    if (owned && stream) {
+        cudaSetDevice(device);
+        cudaStreamDestroy(stream);
+    }
+}
+
+DevAlloc::~DevAlloc() {
+    if (ptr) {
+        cudaSetDevice(stream->device);
+        cudaFreeAsync(ptr, stream->stream);
+    }
+}
+
+AllocRef dev_alloc(const StreamRef& s, size_t bytes, bool zero) {
+    auto a = std::make_shared<DevAlloc>();
+    a->stream = s;
+    a->bytes = bytes;
+    size_t rounded = ((bytes ? bytes : 1) + 255) & ~size_t(255);
+    cudaError_t e = cudaMallocAsync(&a->ptr, rounded, s->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        a->ptr = nullptr;
+        fail(OXB_ALLOCATION, "allocation of " + std::to_string(bytes) + " device bytes failed: " +
+                                 cudaGetErrorString(e));
+    }
+    if (((uintptr_t)a->ptr & 255) != 0) fail(OXB_DEVICE, "device allocation is not 256-byte aligned");
+    if (zero) OXB_CUDA(cudaMemsetAsync(a->ptr, 0, rounded, s->stream));
+    return a;
+}
+
+}  // namespace oxb
+
+using namespace oxb;
+
+#define OXB_TRY try {
+#define OXB_CATCH                                                                \
+    }                                                                            \
+    catch (const Error& e) {                                                     \
+        g_last_error = e.message;                                                \
+        return e.status;                                                         \
+    }                                                                            \
+    catch (const std::bad_alloc&) {                                              \
+        g_last_error = "host allocation failed";                                 \
+        return OXB_ALLOCATION;                                                   \
+    }                                                                            \
+    catch (const std::exception& e) {                                            \
+        g_last_error = e.what();                                                 \
+        return OXB_EXECUTION;                                                    \
+    }                                                                            \
+    return OXB_OK;
+
+namespace {
+
+void use_device(const oxb_backend* b) {
+    if (!b) fail(OXB_PLAN, "backend is null");
+    OXB_CUDA(cudaSetDevice(b->b.device));
+}
+
+const StreamRef& stream_of(const oxb_stream* s) {
+    if (!s) fail(OXB_PLAN, "stream is null");
+    return s->s;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oxb_last_error(void) { return g_last_error.c_str(); }
+
+int32_t oxb_abi_version(void) { return OXB_ABI_VERSION; }
+
+oxb_status oxb_backend_create(int32_t device, oxb_backend** out) {
+    OXB_TRY
+    if (!out) fail(OXB_PLAN, "out is null");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        fail(OXB_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count) fail(OXB_PLAN, "device " + std::to_string(device) + " does not exist");
+    OXB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    OXB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        fail(OXB_UNSUPPORTED, std::string("device ") + prop.name + " is not sm_100 (this library is built for sm_100a)");
+    OXB_CUDA(cudaFree(nullptr));
+    cudaMemPool_t pool;
+    OXB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t threshold = UINT64_MAX;  // keep freed blocks cached in the pool
+    OXB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    auto b = new oxb_backend();
+    b->b.device = device;
+    b->b.sms = prop.multiProcessorCount;
+    b->b.smem_optin = prop.sharedMemPerBlockOptin;
+    b->b.name = prop.name;
+    *out = b;
+    OXB_CATCH
+}
+
+void oxb_backend_destroy(oxb_backend* backend) { delete backend; }
+
+const char* oxb_backend_kind(const oxb_backend* backend) {
+    (void)backend;
+    return "cuda";
+}
+
+int32_t oxb_backend_device_id(const oxb_backend* backend) { return backend ? backend->b.device : -1; }
+
+oxb_status oxb_memory_info_get(oxb_backend* backend, oxb_memory_info* out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "out is null");
+    size_t free_b = 0, total_b = 0;
+    OXB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    out->total_bytes = total_b;
+    out->free_bytes = free_b;
+    out->pinned_supported = 1;
+    out->reserved = 0;
+    OXB_CATCH
+}
+
+oxb_status oxb_stream_create(oxb_backend* backend, oxb_stream** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "out is null");
+    auto st = std::make_shared<StreamState>();
+    st->device = backend->b.device;
+    st->owned = true;
+    OXB_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+    *out = new oxb_stream{st};
+    OXB_CATCH
+}
+
+oxb_status oxb_stream_wrap(oxb_backend* backend, void* cuda_stream, oxb_stream** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "out is null");
+    auto st = std::make_shared<StreamState>();
+    st->device = backend->b.device;
+    st->owned = false;
+    st->stream = (cudaStream_t)cuda_stream;
+    *out = new oxb_stream{st};
+    OXB_CATCH
+}
+
+void* oxb_stream_cuda_handle(const oxb_stream* stream) { return stream ? (void*)stream->s->stream : nullptr; }
+
+oxb_status oxb_stream_synchronize(oxb_backend* backend, oxb_stream* stream) {
+    OXB_TRY
+    use_device(backend);
+    OXB_CUDA(cudaStreamSynchronize(stream_of(stream)->stream));
+    OXB_CATCH
+}
+
+void oxb_stream_destroy(oxb_stream* stream) { delete stream; }
+
+oxb_status oxb_alloc_device(oxb_backend* backend, size_t bytes, oxb_buffer** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "out is null");
+    // Allocations made outside any call's stream live on a backend-wide stream.
+    static thread_local StreamRef alloc_stream;
+    if (!alloc_stream || alloc_stream->device != backend->b.device) {
+        alloc_stream = std::make_shared<StreamState>();
+        alloc_stream->device = backend->b.device;
+        alloc_stream->owned = true;
+        OXB_CUDA(cudaStreamCreateWithFlags(&alloc_stream->stream, cudaStreamNonBlocking));
+    }
+    AllocRef a = dev_alloc(alloc_stream, bytes, true);
+    OXB_CUDA(cudaStreamSynchronize(alloc_stream->stream));
+    auto buf = new oxb_buffer{a};
+    buf->a->bytes = bytes;
+    *out = buf;
+    OXB_CATCH
+}
+
+void* oxb_buffer_device_ptr(const oxb_buffer* buffer) { return buffer ? buffer->a->ptr : nullptr; }
+size_t oxb_buffer_len(const oxb_buffer* buffer) { return buffer ? buffer->a->bytes : 0; }
+void oxb_buffer_free(oxb_buffer* buffer) { delete buffer; }
+
+oxb_status oxb_alloc_pinned_host(oxb_backend* backend, size_t bytes, oxb_host_buffer** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "out is null");
+    auto h = new oxb_host_buffer();
+    h->bytes = bytes;
+    if (cudaMallocHost(&h->ptr, bytes ? bytes : 1) == cudaSuccess) {
+        h->pinned = true;
+    } else {
+        cudaGetLastError();
+        h->ptr = std::malloc(bytes ? bytes : 1);
+        h->pinned = false;
+        if (!h->ptr) {
+            delete h;
+            fail(OXB_ALLOCATION, "host allocation of " + std::to_string(bytes) + " bytes failed");
+        }
+    }
+    *out = h;
+    OXB_CATCH
+}
+
+void* oxb_host_buffer_ptr(const oxb_host_buffer* buffer) { return buffer ? buffer->ptr : nullptr; }
+size_t oxb_host_buffer_len(const oxb_host_buffer* buffer) { return buffer ? buffer->bytes : 0; }
+int32_t oxb_host_buffer_is_pinned(const oxb_host_buffer* buffer) { return buffer && buffer->pinned ? 1 : 0; }
+void oxb_host_buffer_free(oxb_host_buffer* buffer) {
+    if (!buffer) return;
+    if (buffer->pinned) cudaFreeHost(buffer->ptr);
+    else std::free(buffer->ptr);
+    delete buffer;
+}
+
+oxb_status oxb_copy_h2d(oxb_backend* backend, oxb_stream* stream, const oxb_host_buffer* src, oxb_buffer* dst) {
+    OXB_TRY
+    use_device(backend);
+    if (!src || !dst) fail(OXB_PLAN, "null buffer");
+    size_t n = std::min(src->bytes, dst->a->bytes);
+    OXB_CUDA(cudaMemcpyAsync(dst->a->ptr, src->ptr, n, cudaMemcpyHostToDevice, stream_of(stream)->stream));
+    OXB_CATCH
+}
+
+oxb_status oxb_copy_d2h(oxb_backend* backend, oxb_stream* stream, const oxb_buffer* src, oxb_host_buffer* dst) {
+    OXB_TRY
+    use_device(backend);
+    if (!src || !dst) fail(OXB_PLAN, "null buffer");
+    size_t n = std::min(src->a->bytes, dst->bytes);
+    OXB_CUDA(cudaMemcpyAsync(dst->ptr, src->a->ptr, n, cudaMemcpyDeviceToHost, stream_of(stream)->stream));
+    OXB_CATCH
+}
+
+}  // extern "C"
+
+namespace {
+
+void check_column_desc(const oxb_column& c, int64_t rows, int i) {
+    if (c.type < OXB_TYPE_INT64 || c.type > OXB_TYPE_VECTOR_F32)
+        fail(OXB_UNSUPPORTED, "column " + std::to_string(i) + " has an unsupported type " + std::to_string(c.type));
+    if (c.type == OXB_TYPE_VECTOR_F32 && c.dim <= 0) fail(OXB_PLAN, "vector column with dim <= 0");
+    if (c.length != rows)
+        fail(OXB_PLAN, "column " + std::to_string(i) + " has " + std::to_string(c.length) + " rows, the batch " +
+                           std::to_string(rows));
+    if (rows > 0 && !c.values) fail(OXB_PLAN, "column " + std::to_string(i) + " has no values");
+}
+
+}  // namespace
+
+extern "C" {
+
+oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column* columns, int32_t ncols, int64_t rows,
+                      oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    const StreamRef& s = stream_of(stream);
+    if (!out || (ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad upload arguments");
+    auto b = std::make_unique<oxb_batch>();
+    b->rows = rows;
+    for (int i = 0; i < ncols; i++) {
+        const oxb_column& c = columns[i];
+        check_column_desc(c, rows, i);
+        Column d;
+        d.type = c.type;
+        d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
+        d.length = rows;
+        if (rows > 0) {
+            size_t bytes = (size_t)rows * d.width();
+            d.owner_values = dev_alloc(s, bytes, false);
+            d.values = d.owner_values->ptr;
+            OXB_CUDA(cudaMemcpyAsync(d.values, c.values, bytes, cudaMemcpyHostToDevice, s->stream));
+            if (c.validity) {
+                size_t vb = ((size_t)rows + 7) / 8;
+                d.owner_validity = dev_alloc(s, vb, false);
+                d.validity = (uint8_t*)d.owner_validity->ptr;
+                OXB_CUDA(cudaMemcpyAsync(d.validity, c.validity, vb, cudaMemcpyHostToDevice, s->stream));
+            }
+        }
+        b->cols.push_back(std::move(d));
+    }
+    *out = b.release();
+    OXB_CATCH
+}
+
+oxb_status oxb_batch_from_device(oxb_backend* backend, const oxb_column* columns, int32_t ncols, int64_t rows,
+                                 oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out || (ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad batch arguments");
+    auto b = std::make_unique<oxb_batch>();
+    b->rows = rows;
+    for (int i = 0; i < ncols; i++) {
+        const oxb_column& c = columns[i];
+        check_column_desc(c, rows, i);
+        Column d;
+        d.type = c.type;
+        d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
+        d.length = rows;
+        d.values = const_cast<void*>(c.values);
+        d.validity = const_cast<uint8_t*>(c.validity);
+        b->cols.push_back(std::move(d));
+    }
+    *out = b.release();
+    OXB_CATCH
+}
+
+int64_t oxb_batch_num_rows(const oxb_batch* batch) { return batch ? batch->rows : -1; }
+int32_t oxb_batch_num_columns(const oxb_batch* batch) { return batch ? (int32_t)batch->cols.size() : -1; }
+
+oxb_status oxb_batch_column(const oxb_batch* batch, int32_t index, oxb_column* out) {
+    OXB_TRY
+    if (!batch || !out) fail(OXB_PLAN, "null argument");
+    if (index < 0 || index >= (int)batch->cols.size()) fail(OXB_PLAN, "column index out of range");
+    const Column& c = batch->cols[index];
+    out->type = c.type;
+    out->dim = c.dim;
+    out->length = c.length;
+    out->values = c.values;
+    out->validity = c.validity;
+    OXB_CATCH
+}
+
+oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch, int32_t index,
+                               void* values, uint8_t* validity, int32_t* has_validity) {
+    OXB_TRY
+    use_device(backend);
+    const StreamRef& s = stream_of(stream);
+    if (!batch) fail(OXB_PLAN, "batch is null");
+    if (index < 0 || index >= (int)batch->cols.size()) fail(OXB_PLAN, "column index out of range");
+    const Column& c = batch->cols[index];
+    if (has_validity) *has_validity = c.validity ? 1 : 0;
+    if (c.length > 0) {
+        if (!values) fail(OXB_PLAN, "values buffer is null");
+        OXB_CUDA(cudaMemcpyAsync(values, c.values, (size_t)c.length * c.width(), cudaMemcpyDeviceToHost, s->stream));
+        if (c.validity && validity)
+            OXB_CUDA(cudaMemcpyAsync(validity, c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
+                                     s->stream));
+    }
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    OXB_CATCH
+}
+
+void oxb_batch_free(oxb_batch* batch) { delete batch; }
+
+oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream, const oxb_filter_project_args* args,
+                              oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = filter_project(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+oxb_status oxb_prepare_join_build(oxb_backend* backend, oxb_stream* stream, const oxb_join_build_args* args,
+                                  oxb_join_table** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = prepare_join_build(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+int64_t oxb_join_table_distinct_keys(const oxb_join_table* table) { return table ? table->t.ndistinct : -1; }
+int64_t oxb_join_table_rows(const oxb_join_table* table) { return table ? table->t.nrows : -1; }
+void oxb_join_table_free(oxb_join_table* table) { delete table; }
+
+oxb_status oxb_probe_join(oxb_backend* backend, oxb_stream* stream, const oxb_join_probe_args* args,
+                          oxb_join_matches** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = probe_join(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+uint64_t oxb_join_matches_len(const oxb_join_matches* matches) { return matches ? matches->total : 0; }
+int64_t oxb_join_matches_probe_rows(const oxb_join_matches* matches) { return matches ? matches->probe_rows : -1; }
+void oxb_join_matches_free(oxb_join_matches* matches) { delete matches; }
+
+oxb_status oxb_hash_join(oxb_backend* backend, oxb_stream* stream, const oxb_hash_join_args* args, oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = hash_join(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+oxb_status oxb_aggregate(oxb_backend* backend, oxb_stream* stream, const oxb_aggregate_args* args, oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = aggregate(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream, const oxb_join_aggregate_args* args,
+                              oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = join_aggregate(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream, const oxb_vector_distance_args* args,
+                               oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = vector_distance(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
+int32_t oxb_supports_predicate(const oxb_backend* backend, const oxb_leaf* leaves, int32_t nleaves) {
+    (void)backend;
+    if (nleaves < 0 || nleaves > OXB_MAX_PREDICATE_LEAVES) return 0;
+    for (int i = 0; i < nleaves; i++) {
+        int t = leaves[i].lit_type;
+        if (t != OXB_TYPE_INT64 && t != OXB_TYPE_FLOAT64 && t != OXB_TYPE_INT32) return 0;
+        if (leaves[i].op < 0 || leaves[i].op > 4) return 0;
+    }
+    return 1;
+}
+
+oxb_status oxb_set_kernel_timing(oxb_backend* backend, int32_t enabled) {
+    OXB_TRY
+    if (!backend) fail(OXB_PLAN, "backend is null");
+    backend->b.timing = enabled != 0;
+    OXB_CATCH
+}
+
+oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_t name_len, float* ms) {
+    OXB_TRY
+    if (!backend || !ms) fail(OXB_PLAN, "null argument");
+    *ms = g_last_kernel_ms;
+    if (name && name_len > 0) {
+        std::snprintf(name, (size_t)name_len, "%s", g_last_kernel.c_str());
+    }
+    OXB_CATCH
+}
+
+uint64_t oxb_kernel_launches(void) { return g_launches.load(); }
+
+int32_t oxb_supports_hash_join(const oxb_backend* backend) {
+    (void)backend;
+    return 1;
+}
+
+int32_t oxb_supports_aggregate(const oxb_backend* backend) {
+    (void)backend;
+    return 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,247 @@
+// Fused filter + projection (GpuBackend::filter_project,
+// crates/oxidelake-device/src/backend.rs:98; semantics cpu/kernels.rs:99-152).
+//
+// Two passes over HBM-resident columns, no host scan:
+//   1. filter_mask_kernel: every leaf of the predicate at once, one ballot
+//      per 32 rows into a bit mask (n/8 bytes) and a count per 1024-row tile;
+//   2. scan_u32_to_u64 of the tile counts (device-wide, decoupled from the
+//      host), then one read of the total;
+//   3. filter_gather_kernel: each warp compacts its 32-row words by popcount
+//      ranks (stable) and writes every projected column and validity bitmap.
+// The reference needs 3 + 2·columns launches and a host round trip per batch
+// (crates/oxidelake-device/src/cuda/ops.rs:204-373); this needs 3 launches
+// plus the scan.
+#include "internal.h"
+
+namespace oxb {
+
+namespace {
+
+constexpr int kTileRows = 1024;  // 32 mask words
+constexpr int kWords = kTileRows / 32;
+constexpr int kThreads = 256;    // 8 warps, 4 words each
+constexpr int kMaxProj = 64;
+
+struct DevProjCol {
+    const void* src;
+    const uint8_t* src_valid;
+    void* dst;
+    unsigned int* dst_valid;  // u32 words, zeroed; null when the column has no bitmap
+    int width;
+};
+struct DevProjection {
+    int ncols;
+    DevProjCol cols[kMaxProj];
+};
+
+__global__ void __launch_bounds__(kThreads) filter_mask_kernel(DevPredicate pred, long long n,
+                                                               unsigned int* __restrict__ mask,
+                                                               unsigned int* __restrict__ tile_counts,
+                                                               long long ntiles) {
+    __shared__ unsigned int warp_counts[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        unsigned int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            long long word = tile * kWords + warp * 4 + j;
+            long long row = word * 32 + lane;
+            bool sel = row < n && predicate_holds(pred, row);
+            unsigned int bits = __ballot_sync(0xffffffffu, sel);
+            if (lane == 0 && word * 32 < n) mask[word] = bits;
+            cnt += __popc(bits);
+        }
+        if (lane == 0) warp_counts[warp] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int t = 0;
+#pragma unroll
+            for (int w = 0; w < kThreads / 32; w++) t += warp_counts[w];
+            tile_counts[tile] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// Copies one selected row of a projected column (width 4, 8 or 4·dim bytes).
+__device__ __forceinline__ void copy_row(const DevProjCol& c, long long src_row, long long dst_row) {
+    if (c.width == 8) {
+        ((unsigned long long*)c.dst)[dst_row] = __ldg((const unsigned long long*)c.src + src_row);
+    } else if (c.width == 4) {
+        ((unsigned int*)c.dst)[dst_row] = __ldg((const unsigned int*)c.src + src_row);
+    } else {
+        const unsigned int* s = (const unsigned int*)c.src + src_row * (c.width / 4);
+        unsigned int* d = (unsigned int*)c.dst + dst_row * (c.width / 4);
+        for (int k = 0; k < c.width / 4; k++) d[k] = __ldg(s + k);
+    }
+}
+
+// ORs `cnt` bits (bit i = output row base + i) into a zeroed u32 bitmap.
+__device__ __forceinline__ void or_bits(unsigned int* words, unsigned long long base, unsigned int bits) {
+    if (bits == 0) return;
+    unsigned long long w = base >> 5;
+    unsigned int sh = (unsigned int)(base & 31);
+    unsigned int lo = bits << sh;
+    if (lo) atomicOr(&words[w], lo);
+    if (sh) {
+        unsigned int hi = bits >> (32 - sh);
+        if (hi) atomicOr(&words[w + 1], hi);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) filter_gather_kernel(
+    const unsigned int* __restrict__ mask, const unsigned long long* __restrict__ tile_off, long long n,
+    long long ntiles, DevProjection proj) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long nwords = (n + 31) / 32;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // Prefix of the tile's 32 words, then of this warp's 4.
+        long long my_word = tile * kWords + lane;
+        unsigned int wbits = my_word < nwords ? __ldg(mask + my_word) : 0u;
+        unsigned int c = __popc(wbits), x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        unsigned int excl = x - c;
+        const unsigned long long toff = tile_off[tile];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int wi = warp * 4 + j;
+            unsigned int bits = __shfl_sync(0xffffffffu, wbits, wi);
+            unsigned int pre = __shfl_sync(0xffffffffu, excl, wi);
+            if (bits == 0) continue;  // uniform across the warp
+            const long long row = (tile * kWords + wi) * 32 + lane;
+            const bool sel = (bits >> lane) & 1u;
+            const unsigned int rank = __popc(bits & lanemask_lt());
+            const unsigned long long base = toff + pre;
+            for (int ci = 0; ci < proj.ncols; ci++) {
+                const DevProjCol& col = proj.cols[ci];
+                if (col.width <= 8) {
+                    if (sel) copy_row(col, row, (long long)(base + rank));
+                } else {
+                    // Wide rows: the warp copies one selected row at a time.
+                    unsigned int m = bits;
+                    const int words = col.width / 4;
+                    while (m) {
+                        int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        long long srow = (tile * kWords + wi) * 32 + b;
+                        long long drow = (long long)(base + __popc(bits & ((1u << b) - 1u)));
+                        const unsigned int* s = (const unsigned int*)col.src + srow * words;
+                        unsigned int* d = (unsigned int*)col.dst + drow * words;
+                        for (int k = lane; k < words; k += 32) d[k] = __ldg(s + k);
+                    }
+                }
+                if (col.dst_valid) {
+                    bool v = sel && valid_at(col.src_valid, row);
+                    unsigned int vb = __reduce_or_sync(0xffffffffu, v ? (1u << rank) : 0u);
+                    if (lane == 0) or_bits(col.dst_valid, base, vb);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace
+
+DevPredicate make_predicate(const oxb_batch& in, const oxb_leaf* leaves, int nleaves) {
+    if (nleaves < 0 || nleaves > kMaxLeaves)
+        fail(OXB_UNSUPPORTED, "predicate has " + std::to_string(nleaves) + " leaves; at most 64 run on the device");
+    if (nleaves > 0 && !leaves) fail(OXB_PLAN, "predicate leaves pointer is null");
+    DevPredicate p{};
+    p.nleaves = nleaves;
+    for (int l = 0; l < nleaves; l++) {
+        const oxb_leaf& lf = leaves[l];
+        if (lf.column < 0 || lf.column >= (int)in.cols.size())
+            fail(OXB_PLAN, "column index " + std::to_string(lf.column) + " out of range for a batch with " +
+                               std::to_string(in.cols.size()) + " columns");
+        const Column& c = in.cols[lf.column];
+        if (c.type != lf.lit_type)
+            fail(OXB_UNSUPPORTED, "column " + std::to_string(lf.column) + " has type " +
+                                      std::to_string(c.type) + " but the literal is type " +
+                                      std::to_string(lf.lit_type));
+        if (c.type != kInt64 && c.type != kFloat64 && c.type != kInt32)
+            fail(OXB_UNSUPPORTED, "predicate over a column of type " + std::to_string(c.type));
+        if (lf.op < 0 || lf.op > 4) fail(OXB_PLAN, "unknown comparison " + std::to_string(lf.op));
+        DevLeaf& d = p.leaves[l];
+        d.values = c.values;
+        d.validity = c.validity;
+        d.type = c.type;
+        d.op = lf.op;
+        if (c.type == kFloat64) {
+            long long bits;
+            std::memcpy(&bits, &lf.lit.f, 8);
+            if (bits == kEmptyKey) bits = 0;
+            d.lit = bits ^ (long long)(((unsigned long long)(bits >> 63)) >> 1);
+        } else {
+            d.lit = lf.lit.i;
+        }
+    }
+    return p;
+}
+
+oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a) {
+    if (!a.input) fail(OXB_PLAN, "filter_project: input batch is null");
+    const oxb_batch& in = *a.input;
+    DevPredicate pred = make_predicate(in, a.leaves, a.nleaves);
+    if (a.nprojection < 0 || a.nprojection > kMaxProj)
+        fail(OXB_UNSUPPORTED, "projection of more than 64 columns");
+    if (a.nprojection > 0 && !a.projection) fail(OXB_PLAN, "projection pointer is null");
+    for (int i = 0; i < a.nprojection; i++)
+        if (a.projection[i] < 0 || a.projection[i] >= (int)in.cols.size())
+            fail(OXB_PLAN, "projection index " + std::to_string(a.projection[i]) + " out of range");
+
+    const long long n = in.rows;
+    const long long ntiles = (n + kTileRows - 1) / kTileRows;
+    unsigned long long total = 0;
+    Scratch<unsigned int> mask, tile_counts;
+    Scratch<unsigned long long> tile_off;
+    if (n > 0) {
+        mask = Scratch<unsigned int>(s, (n + 31) / 32);
+        tile_counts = Scratch<unsigned int>(s, ntiles);
+        tile_off = Scratch<unsigned long long>(s, ntiles + 1);
+        int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+        note_launch(), filter_mask_kernel<<<grid, kThreads, 0, s->stream>>>(pred, n, mask.get(), tile_counts.get(), ntiles);
+        OXB_CUDA(cudaGetLastError());
+        scan_u32_to_u64(s, b, tile_counts.get(), tile_off.get(), ntiles);
+        OXB_CUDA(cudaMemcpyAsync(&total, tile_off.get() + ntiles, sizeof total, cudaMemcpyDeviceToHost,
+                                 s->stream));
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+    }
+
+    auto out = std::make_unique<oxb_batch>();
+    out->rows = (long long)total;
+    DevProjection proj{};
+    proj.ncols = a.nprojection;
+    for (int i = 0; i < a.nprojection; i++) {
+        const Column& src = in.cols[a.projection[i]];
+        Column dst;
+        dst.type = src.type;
+        dst.dim = src.dim;
+        dst.length = (long long)total;
+        if (total > 0) {
+            dst.owner_values = dev_alloc(s, total * (size_t)src.width(), false);
+            dst.values = dst.owner_values->ptr;
+            if (src.validity) {
+                dst.owner_validity = dev_alloc(s, ((total + 31) / 32) * 4, true);
+                dst.validity = (uint8_t*)dst.owner_validity->ptr;
+            }
+        }
+        proj.cols[i] = DevProjCol{src.values, src.validity, dst.values, (unsigned int*)dst.validity,
+                                  src.width()};
+        out->cols.push_back(std::move(dst));
+    }
+    if (total > 0 && a.nprojection > 0) {
+        int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+        KernelTimer timer(b, s, "filter_gather_kernel");
+        timer.begin();
+        note_launch(), filter_gather_kernel<<<grid, kThreads, 0, s->stream>>>(mask.get(), tile_off.get(), n, ntiles, proj);
+        timer.end();
+        OXB_CUDA(cudaGetLastError());
+    }
+    return out.release();
+}
+
+}  // namespace oxb

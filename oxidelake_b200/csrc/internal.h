@@ -1,0 +1,212 @@
+// Host-side runtime of liboxb200: handles behind the C ABI, the device
+// allocator, per-call error state and the operator entry points the ABI
+// layer (api.cu) dispatches to.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstring>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/oxb200.h"
+#include "common.cuh"
+
+namespace oxb {
+
+// ---- errors ---------------------------------------------------------------
+
+// A failed call: the status the ABI returns and the message oxb_last_error
+// reports.  Operators throw it; the ABI layer catches it at the boundary,
+// so no C++ exception ever crosses into the caller.
+struct Error {
+    oxb_status status;
+    std::string message;
+};
+
+[[noreturn]] void fail(oxb_status status, const std::string& message);
+void check_cuda(cudaError_t err, const char* what);
+#define OXB_CUDA(call) ::oxb::check_cuda((call), #call)
+
+// ---- streams and memory -------------------------------------------------
+
+struct StreamState {
+    cudaStream_t stream = nullptr;
+    bool owned = false;
+    int device = 0;
+    ~StreamState();
+};
+using StreamRef = std::shared_ptr<StreamState>;
+
+// One device allocation from the stream-ordered pool, freed on the stream
+// it was allocated on once the last reference goes away.
+struct DevAlloc {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    StreamRef stream;
+    ~DevAlloc();
+};
+using AllocRef = std::shared_ptr<DevAlloc>;
+
+AllocRef dev_alloc(const StreamRef& s, size_t bytes, bool zero);
+
+// Scratch memory that lives for one call, on that call's stream.
+template <typename T>
+struct Scratch {
+    AllocRef a;
+    T* ptr = nullptr;
+    Scratch() = default;
+    Scratch(const StreamRef& s, size_t n, bool zero = false) {
+        a = dev_alloc(s, n * sizeof(T) + 16, zero);
+        ptr = (T*)a->ptr;
+    }
+    T* get() const { return ptr; }
+};
+
+struct Backend {
+    int device = 0;
+    int sms = 148;
+    size_t smem_optin = 0;
+    std::string name;
+    bool timing = false;  // oxb_set_kernel_timing
+};
+
+// Counts every kernel this library launches (oxb_kernel_launches).
+void note_launch();
+
+// Times an operator's main kernel with CUDA events recorded on the stream it
+// is launched on, when timing is switched on; the elapsed time is read after
+// the stop event completes and kept for oxb_last_kernel_time on this thread.
+class KernelTimer {
+  public:
+    KernelTimer(const Backend& b, const StreamRef& s, const char* name);
+    ~KernelTimer();
+    void begin();
+    void end();
+
+  private:
+    bool on_;
+    const char* name_;
+    cudaStream_t stream_;
+    cudaEvent_t start_ = nullptr, stop_ = nullptr;
+    bool ended_ = false;
+};
+
+// ---- batches ----------------------------------------------------------------
+
+struct Column {
+    int type = 0;
+    int dim = 1;
+    long long length = 0;
+    void* values = nullptr;
+    uint8_t* validity = nullptr;
+    AllocRef owner_values;    // null when the memory belongs to the caller
+    AllocRef owner_validity;  // ditto
+    int width() const { return type_width(type, dim); }
+};
+
+}  // namespace oxb
+
+struct oxb_backend {
+    oxb::Backend b;
+};
+struct oxb_stream {
+    oxb::StreamRef s;
+};
+struct oxb_buffer {
+    oxb::AllocRef a;
+};
+struct oxb_host_buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool pinned = false;
+};
+struct oxb_batch {
+    long long rows = 0;
+    std::vector<oxb::Column> cols;
+};
+
+namespace oxb {
+
+// The build side of a hash join as the device probes it: an open-addressing
+// table of one slot per distinct key (key, start, count) into `rows`, the
+// build rows with a non-NULL key grouped by key, in build order.
+struct JoinSlot {
+    long long key;
+    unsigned int start;
+    unsigned int count;
+};
+struct JoinTableDev {
+    JoinSlot* slots = nullptr;  // capacity slots
+    unsigned int capacity = 0;  // power of two
+    unsigned int* rows = nullptr;
+    long long nrows = 0;
+    long long ndistinct = 0;
+    // The run of the key equal to kEmptyKey, which cannot live in a slot.
+    unsigned int special_start = 0;
+    unsigned int special_count = 0;
+    int key_type = kInt64;
+};
+
+}  // namespace oxb
+
+struct oxb_join_table {
+    oxb::JoinTableDev t;
+    oxb::AllocRef slots_mem, rows_mem;
+    const oxb_batch* build = nullptr;
+    long long build_rows = 0;
+};
+
+struct oxb_join_matches {
+    oxb::AllocRef offsets_mem;  // u64, probe_rows + 1
+    oxb::AllocRef starts_mem;   // u32, probe_rows
+    long long probe_rows = 0;
+    unsigned long long total = 0;
+    const oxb_join_table* table = nullptr;
+};
+
+namespace oxb {
+
+// ---- helpers shared by the operators --------------------------------------
+
+inline int grid_for(const Backend& b, long long work, int threads, int per_sm = 4) {
+    long long blocks = (work + threads - 1) / threads;
+    long long cap = (long long)b.sms * per_sm;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (int)blocks;
+}
+
+DevPredicate make_predicate(const oxb_batch& in, const oxb_leaf* leaves, int nleaves);
+void check_status_word(uint32_t status, const char* what);
+
+// Exclusive scan of n u32 counts into n + 1 u64 offsets (offsets[n] = total).
+void scan_u32_to_u64(const StreamRef& s, const Backend& b, const unsigned int* counts,
+                     unsigned long long* offsets, long long n);
+
+// Stable LSD radix sort of (key, value) pairs on bits [0, bits) of the key.
+void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
+                      unsigned int* values, long long n, int bits);
+
+// Minimum and maximum valid int key (as int64) of a column; false when none.
+bool key_range(const StreamRef& s, const Backend& b, const Column& key, long long n,
+               long long* lo, long long* hi, long long* count = nullptr);
+
+// Operators.
+oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a);
+oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b,
+                                   const oxb_join_build_args& a);
+oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_join_probe_args& a);
+oxb_batch* hash_join(const StreamRef& s, const Backend& b, const oxb_hash_join_args& a);
+oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_args& a);
+oxb_batch* vector_distance(const StreamRef& s, const Backend& b,
+                           const oxb_vector_distance_args& a);
+oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_aggregate_args& a);
+void launch_vector_distance(const StreamRef& s, const Backend& b, const Column& vec, long long n,
+                            const float* dquery, int metric, float* out);
+
+}  // namespace oxb

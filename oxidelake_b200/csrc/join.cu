@@ -1,0 +1,451 @@
+// Inner hash join on one integer key: build once, probe per batch, gather
+// output in ranges (GpuBackend::prepare_join_build / probe_join / hash_join,
+// crates/oxidelake-device/src/backend.rs:114-163; semantics
+// cpu/kernels.rs:185-472).
+//
+// The build side lives in one open-addressing table in HBM (16-byte slots
+// {key, start, count}, load <= 1/2, so a 1M-key build is 32 MB and stays in
+// the 126 MB L2 while the probe streams).  It is built on the device: from
+// the caller's host index (the reference's JoinBuildArgs::index) or, with no
+// index, from the key column itself by a stable radix sort, which yields the
+// same runs in build order.  Matches are numbered in probe-row order, then
+// build order (backend.rs:148-152).
+#include "internal.h"
+
+namespace oxb {
+
+namespace {
+
+__device__ __forceinline__ long long join_key_at(const void* v, int type, long long i) {
+    return load_key(v, type, i);
+}
+
+// Places run r at its key's slot; a key equal to kEmptyKey goes to the side
+// slot at index `capacity`.
+__global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int capacity,
+                                   const long long* __restrict__ keys, const unsigned int* __restrict__ starts,
+                                   const unsigned int* __restrict__ counts, long long nruns,
+                                   unsigned int* __restrict__ status) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nruns;
+         r += (long long)gridDim.x * blockDim.x) {
+        long long key = keys[r];
+        if (key == kEmptyKey) {
+            slots[capacity].start = starts[r];
+            slots[capacity].count = counts[r];
+            continue;
+        }
+        unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (capacity - 1u));
+        bool placed = false;
+        for (unsigned int p = 0; p < capacity; p++) {
+            unsigned long long old = atomicCAS((unsigned long long*)&slots[s].key,
+                                               (unsigned long long)kEmptyKey, (unsigned long long)key);
+            if (old == (unsigned long long)kEmptyKey || old == (unsigned long long)key) {
+                slots[s].start = starts[r];
+                slots[s].count = counts[r];
+                placed = true;
+                break;
+            }
+            s = (s + 1u) & (capacity - 1u);
+        }
+        if (!placed) atomicOr(status, kStatusTableFull);
+    }
+}
+
+__global__ void join_init_slots_kernel(JoinSlot* slots, unsigned int n) {
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        slots[i].key = kEmptyKey;
+        slots[i].start = 0;
+        slots[i].count = 0;
+    }
+}
+
+// Device build step 1: (key - lo, row) pairs; NULL keys sort after all others.
+__global__ void join_pairs_kernel(const void* __restrict__ kv, const uint8_t* __restrict__ kvalid, int type,
+                                  long long n, long long lo, unsigned long long null_key,
+                                  unsigned long long* __restrict__ ukeys, unsigned int* __restrict__ rows) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        ukeys[i] = valid_at(kvalid, i) ? (unsigned long long)(join_key_at(kv, type, i) - lo) : null_key;
+        rows[i] = (unsigned int)i;
+    }
+}
+
+// Device build step 2: 1 where a run of equal keys starts.
+__global__ void join_heads_kernel(const unsigned long long* __restrict__ ukeys, long long nvalid,
+                                  unsigned int* __restrict__ heads) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid;
+         i += (long long)gridDim.x * blockDim.x)
+        heads[i] = (i == 0 || ukeys[i] != ukeys[i - 1]) ? 1u : 0u;
+}
+
+// Device build step 3: each run's key and start; step 4: its count, from
+// the start of the next run.
+__global__ void join_runs_kernel(const unsigned long long* __restrict__ ukeys, long long nvalid,
+                                 const unsigned int* __restrict__ heads,
+                                 const unsigned long long* __restrict__ run_of, long long lo,
+                                 long long* __restrict__ rkeys, unsigned int* __restrict__ rstart) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!heads[i]) continue;
+        long long r = (long long)run_of[i];
+        rkeys[r] = (long long)(ukeys[i] + (unsigned long long)lo);
+        rstart[r] = (unsigned int)i;
+    }
+}
+
+__global__ void join_counts_kernel(const unsigned int* __restrict__ rstart, long long nruns, long long nvalid,
+                                   unsigned int* __restrict__ rcount) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nruns;
+         r += (long long)gridDim.x * blockDim.x) {
+        long long end = r + 1 < nruns ? (long long)rstart[r + 1] : nvalid;
+        rcount[r] = (unsigned int)(end - (long long)rstart[r]);
+    }
+}
+
+__device__ __forceinline__ bool join_lookup(const JoinTableDev& t, long long key, unsigned int* start,
+                                            unsigned int* count) {
+    if (key == kEmptyKey) {
+        *start = t.special_start;
+        *count = t.special_count;
+        return *count > 0;
+    }
+    unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (t.capacity - 1u));
+    for (unsigned int p = 0; p < t.capacity; p++) {
+        const int4 slot = __ldg((const int4*)&t.slots[s]);
+        long long k = ((long long)(unsigned int)slot.y << 32) | (unsigned int)slot.x;
+        if (k == key) {
+            *start = (unsigned int)slot.z;
+            *count = (unsigned int)slot.w;
+            return true;
+        }
+        if (k == kEmptyKey) return false;
+        s = (s + 1u) & (t.capacity - 1u);
+    }
+    return false;
+}
+
+__global__ void join_probe_kernel(JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid,
+                                  int type, long long n, unsigned int* __restrict__ counts,
+                                  unsigned int* __restrict__ starts) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned int st = 0, c = 0;
+        if (valid_at(kvalid, i) && !join_lookup(t, join_key_at(kv, type, i), &st, &c)) st = c = 0;
+        counts[i] = c;
+        starts[i] = st;
+    }
+}
+
+constexpr int kMaxOut = 128;
+struct DevGatherCol {
+    const void* src;
+    const uint8_t* src_valid;
+    void* dst;
+    unsigned int* dst_valid;
+    int width;
+    int side;  // 0 = left (probe), 1 = right (build)
+};
+struct DevGather {
+    int ncols;
+    DevGatherCol cols[kMaxOut];
+};
+
+// One thread per output row: the probe row holding match p is the last one
+// whose offset is <= p (cpu/kernels.rs:378-384), found by binary search.
+__global__ void join_gather_kernel(const unsigned long long* __restrict__ offsets,
+                                   const unsigned int* __restrict__ starts, long long nprobe,
+                                   const unsigned int* __restrict__ trows, long long ntrows,
+                                   long long right_rows, unsigned long long first, long long rows, DevGather g,
+                                   unsigned int* __restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t0 = blockIdx.x * (long long)blockDim.x; t0 < rows; t0 += stride) {
+        const long long t = t0 + threadIdx.x;
+        const bool live = t < rows;
+        long long lrow = 0, rrow = 0;
+        if (live) {
+            unsigned long long p = first + (unsigned long long)t;
+            long long lo = 0, hi = nprobe;  // invariant offsets[lo] <= p < offsets[hi]
+            while (hi - lo > 1) {
+                long long mid = lo + (hi - lo) / 2;
+                if (offsets[mid] <= p) lo = mid;
+                else hi = mid;
+            }
+            lrow = lo;
+            unsigned long long at = (unsigned long long)starts[lo] + (p - offsets[lo]);
+            if (at < (unsigned long long)ntrows) {
+                rrow = trows[at];
+                if (rrow >= right_rows) {
+                    rrow = 0;
+                    atomicOr(status, kStatusBounds);
+                }
+            } else {
+                atomicOr(status, kStatusBounds);
+            }
+        }
+        for (int ci = 0; ci < g.ncols; ci++) {
+            const DevGatherCol& c = g.cols[ci];
+            const long long srow = c.side == 0 ? lrow : rrow;
+            if (live) {
+                if (c.width == 8)
+                    ((unsigned long long*)c.dst)[t] = __ldg((const unsigned long long*)c.src + srow);
+                else if (c.width == 4)
+                    ((unsigned int*)c.dst)[t] = __ldg((const unsigned int*)c.src + srow);
+                else {
+                    const int w = c.width / 4;
+                    const unsigned int* s = (const unsigned int*)c.src + srow * w;
+                    unsigned int* d = (unsigned int*)c.dst + t * w;
+                    for (int k = 0; k < w; k++) d[k] = __ldg(s + k);
+                }
+            }
+            if (c.dst_valid) {
+                unsigned int bits = __ballot_sync(0xffffffffu, live && valid_at(c.src_valid, srow));
+                if (lane == 0 && t < rows) c.dst_valid[t >> 5] = bits;
+            }
+        }
+    }
+}
+
+unsigned int pow2_capacity(long long distinct) {
+    long long c = 16;
+    while (c < 2 * distinct) c <<= 1;
+    if (c > (1ll << 31)) fail(OXB_UNSUPPORTED, std::to_string(distinct) + " distinct join keys exceed the device index");
+    return (unsigned int)c;
+}
+
+}  // namespace
+
+oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const oxb_join_build_args& a) {
+    if (!a.build) fail(OXB_PLAN, "prepare_join_build: build batch is null");
+    const oxb_batch& build = *a.build;
+    if (a.key < 0 || a.key >= (int)build.cols.size())
+        fail(OXB_PLAN, "join key column " + std::to_string(a.key) + " out of range");
+    const Column& key = build.cols[a.key];
+    if (key.type != kInt64 && key.type != kInt32)
+        fail(OXB_UNSUPPORTED, "build join key column has type " + std::to_string(key.type) + "; Int64 and Int32 run on the device");
+    const long long n = build.rows;
+    if (n >= (1ll << 32)) fail(OXB_EXECUTION, "build side exceeds u32::MAX rows");
+
+    auto out = std::make_unique<oxb_join_table>();
+    out->build = a.build;
+    out->build_rows = n;
+    JoinTableDev& t = out->t;
+    t.key_type = key.type;
+    Scratch<unsigned int> status(s, 1, true);
+
+    Scratch<long long> rkeys;
+    Scratch<unsigned int> rstart, rcount;
+    long long nruns = 0;
+
+    if (a.index) {
+        // The host's index (JoinSlots::build checks, join_slots.rs:64-95).
+        const oxb_join_index& ix = *a.index;
+        if (ix.ndistinct < 0 || ix.nrows < 0) fail(OXB_EXECUTION, "negative join index sizes");
+        for (long long i = 0; i < ix.nrows; i++)
+            if (ix.rows[i] >= (unsigned long long)n)
+                fail(OXB_EXECUTION, "join table row " + std::to_string(ix.rows[i]) + " is out of range for a " +
+                                        std::to_string(n) + "-row build side");
+        for (long long r = 0; r < ix.ndistinct; r++) {
+            unsigned long long end = (unsigned long long)ix.starts[r] + ix.counts[r];
+            if (ix.counts[r] == 0 || end > (unsigned long long)ix.nrows)
+                fail(OXB_EXECUTION, "join table run " + std::to_string(ix.starts[r]) + "+" +
+                                        std::to_string(ix.counts[r]) + " is outside its " +
+                                        std::to_string(ix.nrows) + " rows");
+        }
+        nruns = ix.ndistinct;
+        t.nrows = ix.nrows;
+        out->rows_mem = dev_alloc(s, (size_t)(ix.nrows + 1) * 4, false);
+        t.rows = (unsigned int*)out->rows_mem->ptr;
+        if (ix.nrows > 0)
+            OXB_CUDA(cudaMemcpyAsync(t.rows, ix.rows, ix.nrows * 4, cudaMemcpyHostToDevice, s->stream));
+        if (nruns > 0) {
+            rkeys = Scratch<long long>(s, nruns);
+            rstart = Scratch<unsigned int>(s, nruns);
+            rcount = Scratch<unsigned int>(s, nruns);
+            OXB_CUDA(cudaMemcpyAsync(rkeys.get(), ix.keys, nruns * 8, cudaMemcpyHostToDevice, s->stream));
+            OXB_CUDA(cudaMemcpyAsync(rstart.get(), ix.starts, nruns * 4, cudaMemcpyHostToDevice, s->stream));
+            OXB_CUDA(cudaMemcpyAsync(rcount.get(), ix.counts, nruns * 4, cudaMemcpyHostToDevice, s->stream));
+            // The side slot is filled on the host for the kEmptyKey run.
+            for (long long r = 0; r < nruns; r++)
+                if (ix.keys[r] == kEmptyKey) {
+                    t.special_start = ix.starts[r];
+                    t.special_count = ix.counts[r];
+                }
+        }
+    } else {
+        // Device build: stable sort of (key, row) by key keeps build order.
+        long long lo = 0, hi = 0, nvalid = 0;
+        bool any = key_range(s, b, key, n, &lo, &hi, &nvalid);
+        Scratch<unsigned long long> ukeys;
+        Scratch<unsigned int> srows;
+        if (any) {
+            unsigned long long span = (unsigned long long)hi - (unsigned long long)lo;
+            unsigned long long null_key = span + 1;  // wraps to 0 only for the full i64 range
+            int bits = 64;
+            if (null_key != 0) {
+                bits = 0;
+                while (bits < 64 && (null_key >> bits) != 0) bits++;
+            }
+            ukeys = Scratch<unsigned long long>(s, n);
+            srows = Scratch<unsigned int>(s, n);
+            int grid = grid_for(b, n, 256, 8);
+            note_launch(), join_pairs_kernel<<<grid, 256, 0, s->stream>>>(key.values, key.validity, key.type, n, lo,
+                                                            null_key == 0 ? ~0ull : null_key, ukeys.get(), srows.get());
+            OXB_CUDA(cudaGetLastError());
+            radix_sort_pairs(s, b, ukeys.get(), srows.get(), n, bits);
+        }
+        t.nrows = nvalid;
+        out->rows_mem = dev_alloc(s, (size_t)(nvalid + 1) * 4, false);
+        t.rows = (unsigned int*)out->rows_mem->ptr;
+        if (nvalid > 0) {
+            OXB_CUDA(cudaMemcpyAsync(t.rows, srows.get(), nvalid * 4, cudaMemcpyDeviceToDevice, s->stream));
+            Scratch<unsigned int> heads(s, nvalid);
+            Scratch<unsigned long long> run_of(s, nvalid + 1);
+            int grid = grid_for(b, nvalid, 256, 8);
+            note_launch(), join_heads_kernel<<<grid, 256, 0, s->stream>>>(ukeys.get(), nvalid, heads.get());
+            scan_u32_to_u64(s, b, heads.get(), run_of.get(), nvalid);
+            unsigned long long nr = 0;
+            OXB_CUDA(cudaMemcpyAsync(&nr, run_of.get() + nvalid, 8, cudaMemcpyDeviceToHost, s->stream));
+            OXB_CUDA(cudaStreamSynchronize(s->stream));
+            nruns = (long long)nr;
+            rkeys = Scratch<long long>(s, nruns);
+            rstart = Scratch<unsigned int>(s, nruns);
+            rcount = Scratch<unsigned int>(s, nruns);
+            note_launch(), join_runs_kernel<<<grid, 256, 0, s->stream>>>(ukeys.get(), nvalid, heads.get(), run_of.get(), lo,
+                                                           rkeys.get(), rstart.get());
+            note_launch(), join_counts_kernel<<<grid_for(b, nruns, 256, 8), 256, 0, s->stream>>>(rstart.get(), nruns, nvalid,
+                                                                                  rcount.get());
+            OXB_CUDA(cudaGetLastError());
+            if (lo == kEmptyKey) {
+                // The smallest key sorts first: run 0.
+                unsigned int c = 0;
+                OXB_CUDA(cudaMemcpyAsync(&c, rcount.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+                OXB_CUDA(cudaStreamSynchronize(s->stream));
+                t.special_start = 0;
+                t.special_count = c;
+            }
+        }
+    }
+
+    t.ndistinct = nruns;
+    t.capacity = pow2_capacity(nruns);
+    out->slots_mem = dev_alloc(s, (size_t)(t.capacity + 1) * sizeof(JoinSlot), false);
+    t.slots = (JoinSlot*)out->slots_mem->ptr;
+    note_launch(), join_init_slots_kernel<<<grid_for(b, t.capacity + 1, 256, 8), 256, 0, s->stream>>>(t.slots, t.capacity + 1);
+    if (nruns > 0)
+        note_launch(), join_insert_kernel<<<grid_for(b, nruns, 256, 8), 256, 0, s->stream>>>(
+            t.slots, t.capacity, rkeys.get(), rstart.get(), rcount.get(), nruns, status.get());
+    OXB_CUDA(cudaGetLastError());
+    uint32_t st = 0;
+    OXB_CUDA(cudaMemcpyAsync(&st, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    check_status_word(st, "prepare_join_build");
+    return out.release();
+}
+
+oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_join_probe_args& a) {
+    if (!a.probe || !a.table) fail(OXB_PLAN, "probe_join: null probe or table");
+    const oxb_batch& probe = *a.probe;
+    if (a.key < 0 || a.key >= (int)probe.cols.size())
+        fail(OXB_PLAN, "probe key column " + std::to_string(a.key) + " out of range");
+    const Column& key = probe.cols[a.key];
+    if (key.type != kInt64 && key.type != kInt32)
+        fail(OXB_UNSUPPORTED, "probe join key column has type " + std::to_string(key.type));
+    const long long n = probe.rows;
+    if (n >= (1ll << 32)) fail(OXB_EXECUTION, "batch exceeds u32::MAX rows");
+    auto m = std::make_unique<oxb_join_matches>();
+    m->table = a.table;
+    m->probe_rows = n;
+    m->offsets_mem = dev_alloc(s, (size_t)(n + 1) * 8, false);
+    m->starts_mem = dev_alloc(s, (size_t)(n + 1) * 4, false);
+    auto* offsets = (unsigned long long*)m->offsets_mem->ptr;
+    auto* starts = (unsigned int*)m->starts_mem->ptr;
+    if (n > 0) {
+        Scratch<unsigned int> counts(s, n);
+        KernelTimer timer(b, s, "join_probe_kernel");
+        timer.begin();
+        note_launch(), join_probe_kernel<<<grid_for(b, n, 256, 8), 256, 0, s->stream>>>(a.table->t, key.values, key.validity,
+                                                                          key.type, n, counts.get(), starts);
+        timer.end();
+        OXB_CUDA(cudaGetLastError());
+        scan_u32_to_u64(s, b, counts.get(), offsets, n);
+    } else {
+        OXB_CUDA(cudaMemsetAsync(offsets, 0, 8, s->stream));
+    }
+    unsigned long long total = 0;
+    OXB_CUDA(cudaMemcpyAsync(&total, offsets + n, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    m->total = total;
+    return m.release();
+}
+
+oxb_batch* hash_join(const StreamRef& s, const Backend& b, const oxb_hash_join_args& a) {
+    if (!a.left || !a.right || !a.table || !a.matches) fail(OXB_PLAN, "hash_join: null argument");
+    const oxb_batch& left = *a.left;
+    const oxb_batch& right = *a.right;
+    const oxb_join_matches& m = *a.matches;
+    if (m.probe_rows != left.rows)
+        fail(OXB_EXECUTION, "join matches cover " + std::to_string(m.probe_rows) +
+                                " probe rows but the probe batch has " + std::to_string(left.rows));
+    if (m.table != a.table) fail(OXB_EXECUTION, "join matches were probed against another table");
+    if (a.table->build_rows != right.rows)
+        fail(OXB_EXECUTION, "the join table indexes " + std::to_string(a.table->build_rows) +
+                                " build rows but the build batch has " + std::to_string(right.rows));
+    if (a.first + a.rows < a.first || a.first + a.rows > m.total)
+        fail(OXB_EXECUTION, "matches " + std::to_string(a.first) + "..+" + std::to_string(a.rows) +
+                                " are outside a probe with " + std::to_string(m.total) + " matches");
+    const int width = (int)left.cols.size();
+    const int all = width + (int)right.cols.size();
+    std::vector<int> sel;
+    if (a.projection) {
+        for (int i = 0; i < a.nprojection; i++) {
+            if (a.projection[i] < 0 || a.projection[i] >= all)
+                fail(OXB_PLAN, "join projection index " + std::to_string(a.projection[i]) +
+                                   " out of range for " + std::to_string(all) + " columns");
+            sel.push_back(a.projection[i]);
+        }
+    } else {
+        for (int i = 0; i < all; i++) sel.push_back(i);
+    }
+    if ((int)sel.size() > kMaxOut) fail(OXB_UNSUPPORTED, "join output of more than 128 columns");
+    const long long rows = (long long)a.rows;
+    auto out = std::make_unique<oxb_batch>();
+    out->rows = rows;
+    DevGather g{};
+    g.ncols = (int)sel.size();
+    for (size_t i = 0; i < sel.size(); i++) {
+        int side = sel[i] < width ? 0 : 1;
+        const Column& src = side == 0 ? left.cols[sel[i]] : right.cols[sel[i] - width];
+        Column dst;
+        dst.type = src.type;
+        dst.dim = src.dim;
+        dst.length = rows;
+        if (rows > 0) {
+            dst.owner_values = dev_alloc(s, rows * (size_t)src.width(), false);
+            dst.values = dst.owner_values->ptr;
+            if (src.validity) {
+                dst.owner_validity = dev_alloc(s, ((rows + 31) / 32) * 4, true);
+                dst.validity = (uint8_t*)dst.owner_validity->ptr;
+            }
+        }
+        g.cols[i] = DevGatherCol{src.values, src.validity, dst.values, (unsigned int*)dst.validity, src.width(), side};
+        out->cols.push_back(std::move(dst));
+    }
+    if (rows > 0) {
+        Scratch<unsigned int> status(s, 1, true);
+        KernelTimer timer(b, s, "join_gather_kernel");
+        timer.begin();
+        note_launch(), join_gather_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(
+            (const unsigned long long*)m.offsets_mem->ptr, (const unsigned int*)m.starts_mem->ptr, m.probe_rows,
+            a.table->t.rows, a.table->t.nrows, right.rows, a.first, rows, g, status.get());
+        timer.end();
+        OXB_CUDA(cudaGetLastError());
+        uint32_t st = 0;
+        OXB_CUDA(cudaMemcpyAsync(&st, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+        check_status_word(st, "hash_join");
+    }
+    return out.release();
+}
+
+}  // namespace oxb

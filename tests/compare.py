@@ -1,0 +1,64 @@
+"""Result comparison for the parity tests: bit-exact for integers, indices,
+and any float the reference computes exactly; within a stated relative
+tolerance for Float64 SUM/AVG (1e-12, the path's stated bound)."""
+from __future__ import annotations
+
+import numpy as np
+import pyarrow as pa
+
+FLOAT_SUM_RTOL = 1e-12
+
+
+def _bits(arr: pa.Array) -> list:
+    if isinstance(arr, pa.ChunkedArray):
+        arr = arr.combine_chunks()
+    valid = arr.is_valid().to_numpy(zero_copy_only=False)
+    t = arr.type
+    if pa.types.is_float64(t):
+        v = arr.fill_null(0.0).to_numpy(zero_copy_only=False).view(np.uint64)
+    elif pa.types.is_float32(t):
+        v = arr.fill_null(0.0).to_numpy(zero_copy_only=False).view(np.uint32)
+    elif pa.types.is_fixed_size_list(t):
+        vals = arr.values.to_numpy(zero_copy_only=False).view(np.uint32)
+        off = arr.offset * t.list_size
+        v = [tuple(vals[off + i * t.list_size : off + (i + 1) * t.list_size]) for i in range(len(arr))]
+        return [x if ok else None for x, ok in zip(v, valid)]
+    else:
+        return [x if ok else None for x, ok in zip(arr.to_pylist(), valid)]
+    return [int(x) if ok else None for x, ok in zip(v, valid)]
+
+
+def assert_columns_equal(got: pa.Array, want: pa.Array, what: str = "") -> None:
+    assert len(got) == len(want), f"{what}: {len(got)} rows, want {len(want)}"
+    assert got.type == want.type, f"{what}: type {got.type}, want {want.type}"
+    g, w = _bits(got), _bits(want)
+    if g != w:
+        bad = [i for i, (a, b) in enumerate(zip(g, w)) if a != b][:5]
+        raise AssertionError(f"{what}: differs at rows {bad}: got {[g[i] for i in bad]} want {[w[i] for i in bad]}")
+
+
+def assert_close_f64(got: pa.Array, want: pa.Array, what: str = "", rtol: float = FLOAT_SUM_RTOL) -> None:
+    assert len(got) == len(want), what
+    gv, wv = got.is_valid().to_pylist(), want.is_valid().to_pylist()
+    assert gv == wv, f"{what}: validity differs"
+    g = got.fill_null(0.0).to_numpy(zero_copy_only=False)
+    w = want.fill_null(0.0).to_numpy(zero_copy_only=False)
+    same_nan = np.isnan(g) & np.isnan(w)
+    inf_eq = np.isinf(w) & (g == w)
+    err = np.abs(g - w)
+    ok = same_nan | inf_eq | (err <= rtol * np.abs(w)) | (g == w)
+    if not ok.all():
+        i = np.nonzero(~ok)[0][:5]
+        raise AssertionError(f"{what}: rel err > {rtol} at {i.tolist()}: got {g[i]} want {w[i]}")
+
+
+def assert_batches_equal(got: pa.RecordBatch, want: pa.RecordBatch, float_sum_cols=()) -> None:
+    """Bit-exact except the named Float64 SUM/AVG columns (1e-12 relative)."""
+    assert got.num_columns == want.num_columns, (got.schema, want.schema)
+    assert got.num_rows == want.num_rows, (got.num_rows, want.num_rows)
+    for i in range(want.num_columns):
+        name = want.schema.field(i).name
+        if i in float_sum_cols or name in float_sum_cols:
+            assert_close_f64(got.column(i), want.column(i), name)
+        else:
+            assert_columns_equal(got.column(i), want.column(i), name)
