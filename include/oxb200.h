@@ -356,6 +356,16 @@ OXB_API oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_
                                         float* ms);
 /* Kernels this library has launched in this process. */
 OXB_API uint64_t oxb_kernel_launches(void);
+/* When enabled, the first call of each query shape times every compiled
+ * variant of its main kernel (warp combining on/off, rows per thread) on
+ * that call's data and keeps the fastest for later calls in this process. */
+OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
+/* Pins the aggregation kernels' variant instead of the tuned one: combine
+ * -1 (automatic), 0 (per-row atomics), 1 (warp combining and caches), 2
+ * (tile sort-reduce), 3 (columns streamed by bulk copies) or 4 (streamed
+ * tile sort-reduce); rows_per_thread
+ * 0 (automatic), 1 or 2. */
+OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);
 
 /* GpuBackend::supports_predicate / supports_hash_join / supports_aggregate
  * (backend.rs:182-197): 1 when the call runs on the device. */

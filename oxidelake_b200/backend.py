@@ -483,6 +483,14 @@ class CudaBackend:
         _abi.check(_L().oxb_last_kernel_time(self.handle, buf, 64, C.byref(ms)))
         return buf.value.decode(), ms.value
 
+    def set_autotune(self, enabled: bool) -> None:
+        """First call per query shape times every kernel variant and keeps the fastest."""
+        _abi.check(_L().oxb_set_autotune(self.handle, 1 if enabled else 0))
+
+    def set_agg_variant(self, combine: int = -1, rows_per_thread: int = 0) -> None:
+        """Pins the aggregation kernel variant (-1 / 0: automatic)."""
+        _abi.check(_L().oxb_set_agg_variant(self.handle, combine, rows_per_thread))
+
     @staticmethod
     def kernel_launches() -> int:
         return int(_L().oxb_kernel_launches())

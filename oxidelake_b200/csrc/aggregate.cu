@@ -4,57 +4,88 @@
 // WHERE -> GROUP BY form that runs a whole join + aggregate query in one
 // pass over the probe side.
 //
-// One open-addressing table in HBM holds the groups: a key array (empty =
+// Groups live in one open-addressing table in HBM: a key array (empty =
 // kEmptyKey, claimed by one 64-bit CAS, so no publication wait is needed)
-// and structure-of-arrays accumulators beside it.  Each CTA first folds rows
-// into a private table in shared memory (bounded probing, half-full cap)
-// and merges it into the HBM table when its rows are done; rows whose key
-// does not fit the private table go straight to HBM.  Low-cardinality
-// queries therefore touch HBM only for their input columns.
+// and structure-of-arrays accumulators beside it.  Each CTA first folds its
+// rows into a private table in shared memory — direct-mapped when the keys
+// fall in a small range, hashed otherwise — and merges it into HBM when its
+// rows are done; rows whose key does not fit go straight to HBM.
 //
-// Float64 SUM/AVG: every atomicAdd returns the old sum, so the rounding
-// error of that very addition is recovered exactly (TwoSum) and accumulated
-// in a compensation array; the result is sum + compensation.  This keeps the
-// error to O(eps) relative independently of the order atomics land in.
-// Int64 SUM wraps (unsigned add), MIN/MAX over Float64 follow totalOrder via
+// Within a warp, lanes whose rows fall in the same group are combined first
+// (__match_any_sync on the slot): one leader lane folds its peers' values
+// and issues a single set of shared-memory atomics, so a Zipf-hot group
+// costs one update per warp instead of one per row.  Aggregates over the
+// same column share accumulators (SUM(x) and AVG(x) share one sum).
+//
+// Float64 sums: the leader's fold is an exact TwoSum chain, and every
+// atomicAdd returns the old sum, so the rounding error of that very addition
+// is recovered (TwoSum) and accumulated in a compensation array; the result
+// is sum + compensation, O(eps) relative whatever order atomics land in.
+// Int64 SUM wraps (unsigned add); MIN/MAX over Float64 follow totalOrder via
 // integer keys, exactly as the reference.
+#include <map>
+
+#include "async_copy.cuh"
 #include "internal.h"
 
 namespace oxb {
 
 namespace {
 
-constexpr int kMaxOps = OXB_MAX_AGGREGATES;
-constexpr int kMaxArrays = 1 + 3 * kMaxOps;
+constexpr int kMaxOuts = OXB_MAX_AGGREGATES;
+constexpr int kMaxAccs = OXB_MAX_AGGREGATES;
+constexpr int kMaxArrays = 1 + 2 * kMaxAccs;
+constexpr int kCombineAccs = 8;  // warp combining for up to this many accumulators
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 constexpr int kSmemProbes = 16;
+constexpr int kSlotNone = -1;    // the lane has no row to fold
+constexpr int kSlotGlobal = -2;  // the row folds straight into HBM
 
+enum : int { kAccCount = 1, kAccSumInt = 2, kAccSumF64 = 3, kAccMin = 4, kAccMax = 5 };
 enum : unsigned char { kInitZero = 0, kInitMax = 1, kInitMin = 2 };
 enum : unsigned char { kMergeAddU64 = 0, kMergeAddF64Comp = 1, kMergeAddF64 = 2, kMergeMin = 3, kMergeMax = 4 };
 
-struct DevAggOp {
+// One accumulator: what one column (of one side) contributes per row.
+struct DevAcc {
     const void* values;
     const uint8_t* validity;
-    int func;
+    int kind;
     int in_type;
     int side;  // 0: the input (probe) row, 1: the build row
-    int a0, a1, a2;
+    int arr;   // its array (a Float64 sum uses arr and arr + 1)
+};
+
+// One output column: the function, and where its value and count live.
+struct DevOut {
+    int func;
+    int in_type;
+    int arr;  // value array (COUNT: the count array)
+    int nn;   // array counting the rows with a non-NULL input (0 = rows)
 };
 
 struct AggProgram {
-    int nops;
+    int nacc;
+    DevAcc acc[kMaxAccs];
+    int nout;
+    DevOut out[kMaxOuts];
     int narrays;
-    DevAggOp ops[kMaxOps];
     unsigned char init[kMaxArrays];
     unsigned char merge[kMaxArrays];
-    long long* keys;           // capacity entries
-    unsigned long long* acc;   // narrays * stride entries
-    long long stride;          // capacity + 2: [capacity] NULL group, [capacity+1] key == kEmptyKey
+    long long* keys;          // capacity entries
+    unsigned long long* arr;  // narrays * stride entries
+    long long stride;         // capacity + 2: [capacity] NULL group, [capacity+1] key == kEmptyKey
     unsigned int capacity;
-    int smem_slots;            // power of two, 0 = no private table
+    int smem_slots;    // CTA table slots (power of two), 0 = none
+    int scratch_accs;  // accumulators per lane in the warps' combining scratch
+    int direct;        // CTA table indexed by key - direct_lo
+    long long direct_lo;
+    int wslots;        // slots of each warp's private cache (power of two), 0 = none
+    int wdirect;       // warp caches indexed by key - wdirect_lo (else tagged by key)
+    long long wdirect_lo;
     unsigned int* status;
-    unsigned long long* fill;      // keys placed in the HBM table
-    unsigned long long fill_limit; // 3/4 of capacity: no insert beyond it
+    unsigned long long* fill;       // keys placed in the HBM table
+    unsigned long long fill_limit;  // 3/4 of capacity: no insert beyond it
 };
 
 struct AggKey {
@@ -64,61 +95,78 @@ struct AggKey {
     int side;
 };
 
-__device__ __forceinline__ void add_f64_comp(double* sum, double* comp, double x) {
-    double old = atomicAdd(sum, x);
-    double s = __dadd_rn(old, x);
-    if (isfinite(s)) {
-        double bp = __dsub_rn(s, old);
-        double e = __dadd_rn(__dsub_rn(old, __dsub_rn(s, bp)), __dsub_rn(x, bp));
-        if (e != 0.0) atomicAdd(comp, e);
-    }
-}
-
 __device__ __forceinline__ long long load_int(const void* v, int type, long long row) {
     return type == kInt64 ? __ldg((const long long*)v + row) : (long long)__ldg((const int*)v + row);
 }
 
-// Folds one row into accumulators at `slot` (arrays `stride` entries apart).
-__device__ __forceinline__ void agg_apply(const AggProgram& P, unsigned long long* acc, long long stride,
-                                          long long slot, long long row_p, long long row_b) {
-    atomicAdd(&acc[slot], 1ull);  // array 0: rows of the group
-    for (int j = 0; j < P.nops; j++) {
-        const DevAggOp& op = P.ops[j];
-        if (op.func == OXB_AGG_COUNT_STAR) continue;
-        const long long row = op.side ? row_b : row_p;
-        if (!valid_at(op.validity, row)) continue;
-        unsigned long long* a0 = acc + op.a0 * stride + slot;
-        switch (op.func) {
-            case OXB_AGG_COUNT:
-                if (op.a0) atomicAdd(a0, 1ull);
-                continue;
-            case OXB_AGG_SUM:
-                if (op.in_type == kFloat64) {
-                    add_f64_comp((double*)a0, (double*)(acc + op.a1 * stride + slot),
-                                 __ldg((const double*)op.values + row));
-                    if (op.a2) atomicAdd(acc + op.a2 * stride + slot, 1ull);
-                } else {
-                    atomicAdd(a0, (unsigned long long)load_int(op.values, op.in_type, row));
-                    if (op.a1) atomicAdd(acc + op.a1 * stride + slot, 1ull);
-                }
-                continue;
-            case OXB_AGG_AVG: {
-                double x = op.in_type == kFloat64 ? __ldg((const double*)op.values + row)
-                                                  : (double)load_int(op.values, op.in_type, row);
-                add_f64_comp((double*)a0, (double*)(acc + op.a1 * stride + slot), x);
-                if (op.a2) atomicAdd(acc + op.a2 * stride + slot, 1ull);
-                continue;
-            }
-            case OXB_AGG_MIN:
-            case OXB_AGG_MAX: {
-                long long k = op.in_type == kFloat64 ? total_order_key(__ldg((const double*)op.values + row))
-                                                     : load_int(op.values, op.in_type, row);
-                if (op.func == OXB_AGG_MIN) atomicMin((long long*)a0, k);
-                else atomicMax((long long*)a0, k);
-                if (op.a1) atomicAdd(acc + op.a1 * stride + slot, 1ull);
-                continue;
-            }
-            default: continue;
+__device__ __forceinline__ double as_f64(unsigned long long u) { return __longlong_as_double((long long)u); }
+__device__ __forceinline__ unsigned long long as_u64(double d) { return (unsigned long long)__double_as_longlong(d); }
+
+// s + x with the rounding error of that addition added to *c (exact TwoSum);
+// no error term once the sum is not finite.
+__device__ __forceinline__ double two_sum_into(double s, double x, double* c) {
+    double t = __dadd_rn(s, x);
+    if (isfinite(t)) {
+        double bp = __dsub_rn(t, s);
+        *c = __dadd_rn(*c, __dadd_rn(__dsub_rn(s, __dsub_rn(t, bp)), __dsub_rn(x, bp)));
+    }
+    return t;
+}
+
+__device__ __forceinline__ void add_f64_comp(double* sum, double* comp, double x) {
+    double old = atomicAdd(sum, x);
+    double c = 0.0;
+    two_sum_into(old, x, &c);
+    if (c != 0.0) atomicAdd(comp, c);
+}
+
+// What accumulator `a` takes from one row (its identity when the value is NULL).
+__device__ __forceinline__ unsigned long long contribution(const DevAcc& a, long long row_p, long long row_b) {
+    const long long row = a.side ? row_b : row_p;
+    const bool v = valid_at(a.validity, row);
+    switch (a.kind) {
+        case kAccCount:
+            return v ? 1ull : 0ull;
+        case kAccSumInt:
+            return v ? (unsigned long long)load_int(a.values, a.in_type, row) : 0ull;
+        case kAccSumF64: {
+            double x = 0.0;
+            if (v) x = a.in_type == kFloat64 ? __ldg((const double*)a.values + row) : (double)load_int(a.values, a.in_type, row);
+            return as_u64(x);
+        }
+        case kAccMin:
+            if (!v) return 0x7fffffffffffffffull;
+            return (unsigned long long)(a.in_type == kFloat64 ? total_order_key(__ldg((const double*)a.values + row))
+                                                              : load_int(a.values, a.in_type, row));
+        default:
+            if (!v) return 0x8000000000000000ull;
+            return (unsigned long long)(a.in_type == kFloat64 ? total_order_key(__ldg((const double*)a.values + row))
+                                                              : load_int(a.values, a.in_type, row));
+    }
+}
+
+// Folds one row into the arrays at `slot`.
+__device__ __forceinline__ void apply_row(const AggProgram& P, unsigned long long* arr, long long stride, long long slot,
+                                          long long row_p, long long row_b) {
+    atomicAdd(&arr[slot], 1ull);  // array 0: rows of the group
+    for (int j = 0; j < P.nacc; j++) {
+        const DevAcc& a = P.acc[j];
+        const unsigned long long v = contribution(a, row_p, row_b);
+        unsigned long long* p = arr + a.arr * stride + slot;
+        switch (a.kind) {
+            case kAccCount:
+            case kAccSumInt:
+                if (v) atomicAdd(p, v);
+                break;
+            case kAccSumF64:
+                add_f64_comp((double*)p, (double*)(p + stride), as_f64(v));
+                break;
+            case kAccMin:
+                if (v != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)v);
+                break;
+            default:
+                if (v != 0x8000000000000000ull) atomicMax((long long*)p, (long long)v);
+                break;
         }
     }
 }
@@ -149,14 +197,20 @@ __device__ __forceinline__ long long global_slot(const AggProgram& P, bool kvali
     return -1;
 }
 
-// The private slot of a key, -1 when it is not there and cannot be added.
-__device__ __forceinline__ int smem_slot(long long key, long long* s_keys, int S, int* s_fill) {
+// The private slot of a valid key (kSlotGlobal when it has none).
+__device__ __forceinline__ int smem_slot(const AggProgram& P, long long key, long long* s_keys, int* s_fill) {
+    const int S = P.smem_slots;
+    if (S == 0 || key == kEmptyKey) return kSlotGlobal;
+    if (P.direct) {
+        unsigned long long d = (unsigned long long)(key - P.direct_lo);
+        return d < (unsigned long long)S ? (int)d : kSlotGlobal;
+    }
     unsigned int h = (unsigned int)(fmix64((unsigned long long)key) & (unsigned)(S - 1));
     for (int p = 0; p < kSmemProbes; p++) {
         long long k = ((volatile long long*)s_keys)[h];
         if (k == key) return (int)h;
         if (k == kEmptyKey) {
-            if (*(volatile int*)s_fill >= S / 2) return -1;
+            if (*(volatile int*)s_fill >= S / 2) return kSlotGlobal;
             unsigned long long old =
                 atomicCAS((unsigned long long*)&s_keys[h], (unsigned long long)kEmptyKey, (unsigned long long)key);
             if (old == (unsigned long long)kEmptyKey) {
@@ -167,102 +221,324 @@ __device__ __forceinline__ int smem_slot(long long key, long long* s_keys, int S
         }
         h = (h + 1u) & (unsigned)(S - 1);
     }
-    return -1;
+    return kSlotGlobal;
 }
 
-__device__ __forceinline__ void fold_row(const AggProgram& P, long long* s_keys, unsigned long long* s_acc,
-                                         int* s_fill, bool kvalid, long long key, long long row_p,
-                                         long long row_b) {
-    const int S = P.smem_slots;
-    if (S > 0 && kvalid && key != kEmptyKey) {
-        int ls = smem_slot(key, s_keys, S, s_fill);
-        if (ls >= 0) {
-            agg_apply(P, s_acc, S, ls, row_p, row_b);
-            return;
-        }
-    }
-    long long g = global_slot(P, kvalid, key);
-    if (g >= 0) agg_apply(P, P.acc, P.stride, g, row_p, row_b);
+// Shared memory of one CTA: its table (keys + arrays), each warp's private
+// cache (tags + arrays), the warps' combining scratch, the table's fill.
+struct SmemView {
+    long long* keys;              // S (hash mode)
+    unsigned long long* arr;      // narrays * S
+    long long* wtags;             // kWarps * Sw (tagged mode)
+    unsigned long long* warr;     // kWarps * narrays * Sw
+    unsigned long long* scratch;  // kWarps * scratch_accs * 32
+    int* fill;
+};
+
+__device__ __forceinline__ SmemView smem_view(const AggProgram& P, unsigned char* smem) {
+    SmemView v;
+    v.keys = (long long*)smem;
+    v.arr = (unsigned long long*)(v.keys + P.smem_slots);
+    v.wtags = (long long*)(v.arr + (long long)P.smem_slots * P.narrays);
+    v.warr = (unsigned long long*)(v.wtags + kWarps * P.wslots);
+    v.scratch = v.warr + (long long)kWarps * P.narrays * P.wslots;
+    v.fill = (int*)(v.scratch + kWarps * P.scratch_accs * 32);
+    return v;
+}
+
+size_t smem_bytes(int S, int Sw, int narrays, int scratch_accs) {
+    return 8ull * ((size_t)S * (1 + narrays) + (size_t)kWarps * Sw * (1 + narrays) + (size_t)kWarps * scratch_accs * 32) +
+           16;
 }
 
 __device__ __forceinline__ unsigned long long init_value(unsigned char tag) {
     return tag == kInitMax ? 0x7fffffffffffffffull : (tag == kInitMin ? 0x8000000000000000ull : 0ull);
 }
 
-__device__ void smem_init(const AggProgram& P, long long* s_keys, unsigned long long* s_acc, int* s_fill) {
-    const int S = P.smem_slots;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) s_keys[i] = kEmptyKey;
-    for (int i = threadIdx.x; i < S * P.narrays; i += blockDim.x) s_acc[i] = init_value(P.init[i / S]);
-    if (threadIdx.x == 0) *s_fill = 0;
+__device__ void smem_init(const AggProgram& P, const SmemView& v) {
+    const int S = P.smem_slots, W = kWarps * P.wslots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) v.keys[i] = kEmptyKey;
+    for (int i = threadIdx.x; i < S * P.narrays; i += blockDim.x) v.arr[i] = init_value(P.init[i / S]);
+    for (int i = threadIdx.x; i < W; i += blockDim.x) v.wtags[i] = kEmptyKey;
+    // warp w's cache: array a at warr[(w * narrays + a) * Sw]
+    for (int i = threadIdx.x; i < W * P.narrays; i += blockDim.x) v.warr[i] = init_value(P.init[(i / P.wslots) % P.narrays]);
+    if (threadIdx.x == 0) *v.fill = 0;
     __syncthreads();
 }
 
-// Merges the private table into HBM.
-__device__ void smem_flush(const AggProgram& P, long long* s_keys, unsigned long long* s_acc) {
+// Folds combined values into the arrays at `slot`: `rows` rows, per
+// accumulator its folded value and (Float64 sums) the folding error.
+template <int MAXACC>
+__device__ __forceinline__ void apply_vals(const AggProgram& P, unsigned long long* arr, long long stride,
+                                           long long slot, unsigned long long rows, const unsigned long long* val,
+                                           const double* comp) {
+    atomicAdd(&arr[slot], rows);  // array 0: rows of the group
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        if (j >= P.nacc) break;
+        const DevAcc& a = P.acc[j];
+        unsigned long long* p = arr + a.arr * stride + slot;
+        switch (a.kind) {
+            case kAccCount:
+            case kAccSumInt:
+                if (val[j]) atomicAdd(p, val[j]);
+                break;
+            case kAccSumF64: {
+                double* c = (double*)(p + stride);
+                add_f64_comp((double*)p, c, as_f64(val[j]));
+                if (comp[j] != 0.0) atomicAdd(c, comp[j]);
+                break;
+            }
+            case kAccMin:
+                if (val[j] != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)val[j]);
+                break;
+            default:
+                if (val[j] != 0x8000000000000000ull) atomicMax((long long*)p, (long long)val[j]);
+                break;
+        }
+    }
+}
+
+// Folds `val` into accumulator value `x` the way kind `kind` combines.
+__device__ __forceinline__ unsigned long long combine(int kind, unsigned long long acc, unsigned long long x,
+                                                      double* comp) {
+    switch (kind) {
+        case kAccCount:
+        case kAccSumInt: return acc + x;
+        case kAccSumF64: return as_u64(two_sum_into(as_f64(acc), as_f64(x), comp));
+        case kAccMin: return (long long)x < (long long)acc ? x : acc;
+        default: return (long long)x > (long long)acc ? x : acc;
+    }
+}
+
+// The slot of `key` in this warp's private cache, claiming a free one; -1
+// when the key has none.  Only this warp touches its cache, and lanes with
+// different keys that meet on one empty slot settle it with a CAS.
+__device__ __forceinline__ int warp_cache_slot(const AggProgram& P, const SmemView& v, int warp, long long key) {
+    const int Sw = P.wslots;
+    if (Sw == 0) return -1;
+    if (P.wdirect) {
+        const unsigned long long d = (unsigned long long)(key - P.wdirect_lo);
+        return d < (unsigned long long)Sw ? (int)d : -1;
+    }
+    long long* tags = v.wtags + warp * Sw;
+    const int h = (int)(fmix64((unsigned long long)key) & (unsigned)(Sw - 1));
+    const long long t = ((volatile long long*)tags)[h];
+    if (t == key) return h;
+    if (t != kEmptyKey) return -1;
+    const unsigned long long old =
+        atomicCAS((unsigned long long*)&tags[h], (unsigned long long)kEmptyKey, (unsigned long long)key);
+    return (old == (unsigned long long)kEmptyKey || (long long)old == key) ? h : -1;
+}
+
+// One group's folded update (rows, values, folding errors) into the warp's
+// cache (plain loads and stores: with lanes combined, one leader per key and
+// warp writes a slot, and no other warp does), else the CTA table
+// (atomics), else HBM.  Without combining the warp cache is skipped.
+template <int MAXACC, bool WARP_CACHE>
+__device__ __forceinline__ void update_group(const AggProgram& P, const SmemView& v, int warp, long long key,
+                                             unsigned long long rows, const unsigned long long* val,
+                                             const double* comp) {
+    const int ws = WARP_CACHE ? warp_cache_slot(P, v, warp, key) : -1;
+    if (ws >= 0) {
+        const int Sw = P.wslots;
+        unsigned long long* w = v.warr + (long long)warp * P.narrays * Sw + ws;
+        w[0] += rows;
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) {
+            if (j >= P.nacc) break;
+            const DevAcc& a = P.acc[j];
+            unsigned long long* p = w + a.arr * Sw;
+            if (a.kind == kAccSumF64) {
+                double c = as_f64(p[Sw]) + comp[j];
+                *p = as_u64(two_sum_into(as_f64(*p), as_f64(val[j]), &c));
+                p[Sw] = as_u64(c);
+            } else {
+                double unused = 0.0;
+                *p = combine(a.kind, *p, val[j], &unused);
+            }
+        }
+        return;
+    }
+    const int cs = smem_slot(P, key, v.keys, v.fill);
+    if (cs >= 0) {
+        apply_vals<MAXACC>(P, v.arr, P.smem_slots, cs, rows, val, comp);
+        return;
+    }
+    const long long g = global_slot(P, true, key);
+    if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, rows, val, comp);
+}
+
+// Folds one row (or nothing, when !live) of every lane of the warp; all 32
+// lanes call it together.  MAXACC bounds P.nacc at compile time, so the
+// per-accumulator values stay in registers.  With COMBINE, lanes of the same
+// group are merged first (exact TwoSum for Float64) and one leader updates.
+// NULL keys, and the key equal to kEmptyKey, fold straight into HBM.
+template <int MAXACC, bool COMBINE>
+__device__ __forceinline__ void fold(const AggProgram& P, const SmemView& v, bool live, bool kvalid, long long key,
+                                     long long row_p, long long row_b) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long val[MAXACC];
+    double comp[MAXACC];
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        comp[j] = 0.0;
+        val[j] = (j < P.nacc && live) ? contribution(P.acc[j], row_p, row_b) : 0ull;
+    }
+    const bool local = live && kvalid && key != kEmptyKey;
+    if (COMBINE) {
+        const unsigned locals = __ballot_sync(0xffffffffu, local);
+        const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)key) & locals;
+        unsigned long long* mine = v.scratch + warp * MAXACC * 32;
+        if (local) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++)
+                if (j < P.nacc) mine[j * 32 + lane] = val[j];
+        }
+        __syncwarp();
+        if (local && lane == __ffs(peers) - 1) {
+            for (unsigned m = peers & (peers - 1); m; m &= m - 1) {
+                const int l = __ffs(m) - 1;
+#pragma unroll
+                for (int j = 0; j < MAXACC; j++) {
+                    if (j >= P.nacc) break;
+                    val[j] = combine(P.acc[j].kind, val[j], mine[j * 32 + l], &comp[j]);
+                }
+            }
+            update_group<MAXACC, true>(P, v, warp, key, __popc(peers), val, comp);
+        }
+        __syncwarp();
+    } else if (local) {
+        update_group<MAXACC, false>(P, v, warp, key, 1, val, comp);
+    }
+    if (live && !local) {
+        const long long g = global_slot(P, kvalid, key);
+        if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+    }
+}
+
+// Merges one slot's arrays (src, arrays `sstride` apart) into another slot
+// (dst, arrays `dstride` apart) with atomics.
+__device__ __forceinline__ void merge_slot(const AggProgram& P, const unsigned long long* src, long long sstride,
+                                           unsigned long long* dst, long long dstride) {
+    for (int a = 0; a < P.narrays; a++) {
+        const unsigned long long x = src[a * sstride];
+        unsigned long long* d = dst + a * dstride;
+        switch (P.merge[a]) {
+            case kMergeAddU64:
+                if (x) atomicAdd(d, x);
+                break;
+            case kMergeAddF64Comp:
+                add_f64_comp((double*)d, (double*)(d + dstride), as_f64(x));
+                break;
+            case kMergeAddF64:
+                if (as_f64(x) != 0.0) atomicAdd((double*)d, as_f64(x));
+                break;
+            case kMergeMin:
+                if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)d, (long long)x);
+                break;
+            default:
+                if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)d, (long long)x);
+                break;
+        }
+    }
+}
+
+// Merges the warps' caches into the CTA table (or HBM), then the CTA table
+// into HBM.
+__device__ void smem_flush(const AggProgram& P, const SmemView& v) {
+    __syncthreads();
+    const int Sw = P.wslots;
+    for (int i = threadIdx.x; i < kWarps * Sw; i += blockDim.x) {
+        const int w = i / Sw, ws = i - w * Sw;
+        const unsigned long long* src = v.warr + (long long)w * P.narrays * Sw + ws;
+        if (src[0] == 0) continue;  // no rows in this slot
+        const long long key = P.wdirect ? P.wdirect_lo + ws : v.wtags[i];
+        const int cs = smem_slot(P, key, v.keys, v.fill);
+        if (cs >= 0) {
+            merge_slot(P, src, Sw, v.arr + cs, P.smem_slots);
+        } else {
+            const long long g = global_slot(P, true, key);
+            if (g >= 0) merge_slot(P, src, Sw, P.arr + g, P.stride);
+        }
+    }
     __syncthreads();
     const int S = P.smem_slots;
     for (int i = threadIdx.x; i < S; i += blockDim.x) {
-        long long key = s_keys[i];
-        if (key == kEmptyKey) continue;
-        long long g = global_slot(P, true, key);
+        if (v.arr[i] == 0) continue;  // no rows in this slot
+        const long long key = P.direct ? P.direct_lo + i : v.keys[i];
+        const long long g = global_slot(P, true, key);
         if (g < 0) continue;
         for (int a = 0; a < P.narrays; a++) {
-            unsigned long long v = s_acc[a * S + i];
-            unsigned long long* dst = P.acc + a * P.stride + g;
+            const unsigned long long x = v.arr[a * S + i];
+            unsigned long long* dst = P.arr + a * P.stride + g;
             switch (P.merge[a]) {
                 case kMergeAddU64:
-                    if (v) atomicAdd(dst, v);
+                    if (x) atomicAdd(dst, x);
                     break;
                 case kMergeAddF64Comp:
-                    add_f64_comp((double*)dst, (double*)(dst + P.stride), __longlong_as_double((long long)v));
+                    add_f64_comp((double*)dst, (double*)(dst + P.stride), as_f64(x));
                     break;
-                case kMergeAddF64: {
-                    double x = __longlong_as_double((long long)v);
-                    if (x != 0.0) atomicAdd((double*)dst, x);
+                case kMergeAddF64:
+                    if (as_f64(x) != 0.0) atomicAdd((double*)dst, as_f64(x));
                     break;
-                }
                 case kMergeMin:
-                    if ((long long)v != 0x7fffffffffffffffll) atomicMin((long long*)dst, (long long)v);
+                    if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)dst, (long long)x);
                     break;
                 default:
-                    if ((long long)v != (long long)0x8000000000000000ull) atomicMax((long long*)dst, (long long)v);
+                    if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)dst, (long long)x);
                     break;
             }
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) agg_rows_kernel(AggProgram P, DevPredicate pred, AggKey key,
-                                                            long long n) {
+// GROUP BY over the rows of one batch, with an optional fused WHERE; each
+// thread takes RPT rows per step (their loads in flight together).
+template <int MAXACC, bool COMBINE, int RPT>
+__global__ void __launch_bounds__(kThreads) agg_rows_kernel(const __grid_constant__ AggProgram P,
+                                                            const __grid_constant__ DevPredicate pred,
+                                                            const __grid_constant__ AggKey key, long long n) {
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* s_keys = (long long*)smem;
-    unsigned long long* s_acc = (unsigned long long*)(s_keys + P.smem_slots);
-    int* s_fill = (int*)(s_acc + (long long)P.smem_slots * P.narrays);
-    if (P.smem_slots) smem_init(P, s_keys, s_acc, s_fill);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        if (pred.nleaves && !predicate_holds(pred, i)) continue;
-        bool kv = valid_at(key.validity, i);
-        long long k = kv ? load_int(key.values, key.type, i) : 0;
-        fold_row(P, s_keys, s_acc, s_fill, kv, k, i, 0);
+    const SmemView v = smem_view(P, smem);
+    if (P.smem_slots || P.wslots) smem_init(P, v);
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long base = blockIdx.x * (long long)blockDim.x * RPT; base < n; base += step) {
+        bool live[RPT], kv[RPT];
+        long long k[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const long long i = base + r * (long long)blockDim.x + threadIdx.x;
+            live[r] = i < n && (pred.nleaves == 0 || predicate_holds(pred, i));
+            kv[r] = live[r] && valid_at(key.validity, i);
+            k[r] = kv[r] ? load_int(key.values, key.type, i) : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            fold<MAXACC, COMBINE>(P, v, live[r], kv[r], k[r], base + r * (long long)blockDim.x + threadIdx.x, 0);
     }
-    if (P.smem_slots) smem_flush(P, s_keys, s_acc);
+    if (P.smem_slots || P.wslots) smem_flush(P, v);
 }
 
+// A probe key's run: (start, count) and the run's first build row, which
+// lives beside the slot and is loaded in parallel with it.
 __device__ __forceinline__ bool jt_lookup(const JoinTableDev& t, long long key, unsigned int* start,
-                                          unsigned int* count) {
+                                          unsigned int* count, unsigned int* first) {
     if (key == kEmptyKey) {
         *start = t.special_start;
         *count = t.special_count;
+        *first = *count ? t.first_row[t.capacity] : 0u;
         return *count > 0;
     }
     unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (t.capacity - 1u));
     for (unsigned int p = 0; p < t.capacity; p++) {
         const int4 slot = __ldg((const int4*)&t.slots[s]);
+        const unsigned int fr = __ldg(&t.first_row[s]);
         long long k = ((long long)(unsigned int)slot.y << 32) | (unsigned int)slot.x;
         if (k == key) {
             *start = (unsigned int)slot.z;
             *count = (unsigned int)slot.w;
+            *first = fr;
             return true;
         }
         if (k == kEmptyKey) return false;
@@ -272,44 +548,1359 @@ __device__ __forceinline__ bool jt_lookup(const JoinTableDev& t, long long key, 
 }
 
 // probe JOIN build ON key WHERE <probe leaves> GROUP BY <key of either side>:
-// one thread per probe row walks its key's run in build order.
-__global__ void __launch_bounds__(kThreads) agg_join_kernel(AggProgram P, DevPredicate pred, AggKey gkey,
+// each lane looks up RPT probe rows at once (independent L2 chains), then
+// walks each row's matches in build order; the warp steps through match
+// m = 0, 1, ... together so its lanes can combine.
+template <int MAXACC, bool COMBINE, int RPT>
+__global__ void __launch_bounds__(kThreads) agg_join_kernel(const __grid_constant__ AggProgram P,
+                                                            const __grid_constant__ DevPredicate pred,
+                                                            const __grid_constant__ AggKey gkey,
                                                             const void* __restrict__ pk, const uint8_t* __restrict__ pkv,
-                                                            int pk_type, JoinTableDev jt, long long n) {
+                                                            int pk_type, const __grid_constant__ JoinTableDev jt,
+                                                            long long n) {
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* s_keys = (long long*)smem;
-    unsigned long long* s_acc = (unsigned long long*)(s_keys + P.smem_slots);
-    int* s_fill = (int*)(s_acc + (long long)P.smem_slots * P.narrays);
-    if (P.smem_slots) smem_init(P, s_keys, s_acc, s_fill);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        if (pred.nleaves && !predicate_holds(pred, i)) continue;
-        if (!valid_at(pkv, i)) continue;
-        unsigned int start, count;
-        if (!jt_lookup(jt, load_int(pk, pk_type, i), &start, &count)) continue;
-        for (unsigned int m = 0; m < count; m++) {
-            long long b = jt.rows[start + m];
-            long long grow = gkey.side ? b : i;
-            bool kv = valid_at(gkey.validity, grow);
-            long long k = kv ? load_int(gkey.values, gkey.type, grow) : 0;
-            fold_row(P, s_keys, s_acc, s_fill, kv, k, i, b);
+    const SmemView v = smem_view(P, smem);
+    if (P.smem_slots || P.wslots) smem_init(P, v);
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long base = blockIdx.x * (long long)blockDim.x * RPT; base < n; base += step) {
+        unsigned int start[RPT], count[RPT], first[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const long long i = base + r * (long long)blockDim.x + threadIdx.x;
+            count[r] = 0;
+            start[r] = first[r] = 0;
+            if (i < n && (pred.nleaves == 0 || predicate_holds(pred, i)) && valid_at(pkv, i)) {
+                if (!jt_lookup(jt, load_int(pk, pk_type, i), &start[r], &count[r], &first[r])) count[r] = 0;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const long long i = base + r * (long long)blockDim.x + threadIdx.x;
+            for (unsigned int m = 0; __any_sync(0xffffffffu, m < count[r]); m++) {
+                const bool live = m < count[r];
+                bool kv = false;
+                long long k = 0, b = 0;
+                if (live) {
+                    b = m == 0 ? first[r] : jt.rows[start[r] + m];
+                    const long long grow = gkey.side ? b : i;
+                    kv = valid_at(gkey.validity, grow);
+                    k = kv ? load_int(gkey.values, gkey.type, grow) : 0;
+                }
+                fold<MAXACC, COMBINE>(P, v, live, kv, k, i, b);
+            }
         }
     }
-    if (P.smem_slots) smem_flush(P, s_keys, s_acc);
+    if (P.smem_slots || P.wslots) smem_flush(P, v);
 }
 
-__global__ void agg_init_kernel(AggProgram P) {
+// ---- tile sort-reduce ----------------------------------------------------
+//
+// A CTA folds its rows tile by tile (kTileRows rows).  Each row's slot in
+// the CTA table is found, its rank within the slot taken with a native u32
+// shared atomic, and its values scattered so that every slot's rows are
+// contiguous (a counting sort in shared memory).  Each slot's run is then
+// reduced by one thread — or, for runs of kBigRun rows or more (Zipf-hot
+// groups), by a whole warp — with an exact TwoSum chain, and added to the
+// slot's accumulators with plain loads and stores: one writer per slot per
+// tile, no contention and no floating-point atomics.  Per row this costs a
+// handful of instructions whatever the skew.
+
+constexpr int kTileV = 4;                      // rows per thread per tile
+constexpr int kTileRows = kThreads * kTileV;   // 1024
+constexpr int kBigRun = 64;
+
+struct TileView {
+    long long* keys;          // S (hash mode)
+    unsigned long long* arr;  // narrays * S
+    unsigned int* cnt;        // S
+    unsigned int* off;        // S
+    unsigned long long* tval; // MAXACC * kTileRows
+    unsigned int* big;        // kTileRows / kBigRun
+    int* misc;                // [0] big runs, [1] table fill, [2..9] warp sums of the scan
+};
+
+size_t tile_smem_bytes(int S, int narrays, int maxacc) {
+    return 8ull * S * (1 + narrays) + 8ull * S + 8ull * maxacc * kTileRows + 4ull * (kTileRows / kBigRun) + 64;
+}
+
+__device__ __forceinline__ TileView tile_view(const AggProgram& P, unsigned char* smem, int maxacc) {
+    TileView t;
+    const int S = P.smem_slots;
+    t.keys = (long long*)smem;
+    t.arr = (unsigned long long*)(t.keys + S);
+    t.tval = t.arr + (long long)S * P.narrays;
+    t.cnt = (unsigned int*)(t.tval + (long long)maxacc * kTileRows);
+    t.off = t.cnt + S;
+    t.big = t.off + S;
+    t.misc = (int*)(t.big + kTileRows / kBigRun);
+    return t;
+}
+
+// Adds a folded run (rows, values, folding errors) to CTA slot `b` (plain
+// read-modify-write: the caller is the slot's only writer in this tile).
+template <int MAXACC>
+__device__ __forceinline__ void add_run(const AggProgram& P, const TileView& t, int b, unsigned long long rows,
+                                        const unsigned long long* val, const double* comp) {
+    const int S = P.smem_slots;
+    t.arr[b] += rows;
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        if (j >= P.nacc) break;
+        const DevAcc& a = P.acc[j];
+        unsigned long long* p = t.arr + a.arr * S + b;
+        if (a.kind == kAccSumF64) {
+            double c = as_f64(p[S]) + comp[j];
+            *p = as_u64(two_sum_into(as_f64(*p), as_f64(val[j]), &c));
+            p[S] = as_u64(c);
+        } else {
+            double unused = 0.0;
+            *p = combine(a.kind, *p, val[j], &unused);
+        }
+    }
+}
+
+// Block-wide exclusive scan of the S slot counts into t.off.
+__device__ __forceinline__ void scan_counts(const TileView& t, int S) {
+    const int per = (S + kThreads - 1) / kThreads;
+    const int lo = threadIdx.x * per, hi = min(lo + per, S);
+    unsigned int s = 0;
+    for (int b = lo; b < hi; b++) s += t.cnt[b];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned int x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    int* ws = t.misc + 2;
+    if (lane == 31) ws[warp] = (int)x;
+    __syncthreads();
+    unsigned int before = 0;
+    for (int w = 0; w < warp; w++) before += (unsigned int)ws[w];
+    unsigned int run = before + x - s;
+    for (int b = lo; b < hi; b++) {
+        t.off[b] = run;
+        run += t.cnt[b];
+    }
+}
+
+// Reduces every slot's run of this tile into the CTA table and clears the
+// counts for the next tile.
+template <int MAXACC>
+__device__ __forceinline__ void reduce_runs(const AggProgram& P, const TileView& t) {
+    const int S = P.smem_slots;
+    for (int b = threadIdx.x; b < S; b += blockDim.x) {
+        const unsigned int c = t.cnt[b];
+        if (c == 0) continue;
+        if (c >= kBigRun) {
+            t.big[atomicAdd(&t.misc[0], 1)] = b;
+            continue;
+        }
+        const unsigned int o = t.off[b];
+        unsigned long long val[MAXACC];
+        double comp[MAXACC];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) {
+            comp[j] = 0.0;
+            val[j] = j < P.nacc ? t.tval[j * kTileRows + o] : 0ull;
+        }
+        for (unsigned int e = 1; e < c; e++) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                val[j] = combine(P.acc[j].kind, val[j], t.tval[j * kTileRows + o + e], &comp[j]);
+            }
+        }
+        add_run<MAXACC>(P, t, b, c, val, comp);
+        t.cnt[b] = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nbig = t.misc[0];
+    for (int r = warp; r < nbig; r += kWarps) {
+        const int b = (int)t.big[r];
+        const unsigned int c = t.cnt[b], o = t.off[b];
+        unsigned long long val[MAXACC];
+        double comp[MAXACC];
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) comp[j] = 0.0;
+        for (unsigned int e = lane; e < c; e += 32) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                const unsigned long long x = t.tval[j * kTileRows + o + e];
+                val[j] = any ? combine(P.acc[j].kind, val[j], x, &comp[j]) : x;
+            }
+            any = true;
+        }
+        // every lane holds at least one element (c >= kBigRun >= 32)
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                const unsigned long long x = __shfl_xor_sync(0xffffffffu, val[j], d);
+                const double xc = __shfl_xor_sync(0xffffffffu, comp[j], d);
+                if (P.acc[j].kind == kAccSumF64) comp[j] += xc;
+                val[j] = combine(P.acc[j].kind, val[j], x, &comp[j]);
+            }
+        }
+        if (lane == 0) {
+            add_run<MAXACC>(P, t, b, c, val, comp);
+            t.cnt[b] = 0;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) t.misc[0] = 0;
+    __syncthreads();
+}
+
+// One round of a tile: the rows (`live`, key, contributing rows) each lane
+// holds for its kTileV positions.
+template <int MAXACC>
+__device__ __forceinline__ void tile_round(const AggProgram& P, const TileView& t, const bool* live, const bool* kv,
+                                           const long long* key, const long long* row_p, const long long* row_b) {
+    int slot[kTileV];
+    unsigned int rank[kTileV];
+    unsigned long long val[kTileV][MAXACC];
+#pragma unroll
+    for (int v = 0; v < kTileV; v++) {
+        slot[v] = kSlotNone;
+        if (!live[v]) continue;
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) val[v][j] = j < P.nacc ? contribution(P.acc[j], row_p[v], row_b[v]) : 0ull;
+        slot[v] = (kv[v] && key[v] != kEmptyKey) ? smem_slot(P, key[v], t.keys, t.misc + 1) : kSlotGlobal;
+        if (slot[v] >= 0) {
+            rank[v] = atomicAdd(&t.cnt[slot[v]], 1u);
+        } else {
+            double comp[MAXACC];
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) comp[j] = 0.0;
+            const long long g = global_slot(P, kv[v], key[v]);
+            if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val[v], comp);
+        }
+    }
+    __syncthreads();
+    scan_counts(t, P.smem_slots);
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < kTileV; v++) {
+        if (slot[v] < 0) continue;
+        const unsigned int pos = t.off[slot[v]] + rank[v];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++)
+            if (j < P.nacc) t.tval[j * kTileRows + pos] = val[v][j];
+    }
+    __syncthreads();
+    reduce_runs<MAXACC>(P, t);
+}
+
+template <int MAXACC>
+__device__ void tile_init(const AggProgram& P, const TileView& t) {
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        t.keys[i] = kEmptyKey;
+        t.cnt[i] = 0;
+    }
+    for (int i = threadIdx.x; i < S * P.narrays; i += blockDim.x) t.arr[i] = init_value(P.init[i / S]);
+    if (threadIdx.x < 16) t.misc[threadIdx.x] = 0;
+    __syncthreads();
+}
+
+template <int MAXACC>
+__device__ void tile_flush(const AggProgram& P, const TileView& t) {
+    __syncthreads();
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        if (t.arr[i] == 0) continue;  // no rows in this slot
+        const long long key = P.direct ? P.direct_lo + i : t.keys[i];
+        const long long g = global_slot(P, true, key);
+        if (g >= 0) merge_slot(P, t.arr + i, S, P.arr + g, P.stride);
+    }
+}
+
+template <int MAXACC>
+__global__ void __launch_bounds__(kThreads) agg_tile_rows_kernel(const __grid_constant__ AggProgram P,
+                                                                 const __grid_constant__ DevPredicate pred,
+                                                                 const __grid_constant__ AggKey key, long long n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const TileView t = tile_view(P, smem, MAXACC);
+    tile_init<MAXACC>(P, t);
+    for (long long base = blockIdx.x * (long long)kTileRows; base < n; base += (long long)gridDim.x * kTileRows) {
+        bool live[kTileV], kv[kTileV];
+        long long k[kTileV], rp[kTileV], rb[kTileV];
+#pragma unroll
+        for (int v = 0; v < kTileV; v++) {
+            const long long i = base + v * (long long)kThreads + threadIdx.x;
+            rp[v] = i;
+            rb[v] = 0;
+            live[v] = i < n && (pred.nleaves == 0 || predicate_holds(pred, i));
+            kv[v] = live[v] && valid_at(key.validity, i);
+            k[v] = kv[v] ? load_int(key.values, key.type, i) : 0;
+        }
+        tile_round<MAXACC>(P, t, live, kv, k, rp, rb);
+    }
+    tile_flush<MAXACC>(P, t);
+}
+
+template <int MAXACC>
+__global__ void __launch_bounds__(kThreads) agg_tile_join_kernel(const __grid_constant__ AggProgram P,
+                                                                 const __grid_constant__ DevPredicate pred,
+                                                                 const __grid_constant__ AggKey gkey,
+                                                                 const void* __restrict__ pk,
+                                                                 const uint8_t* __restrict__ pkv, int pk_type,
+                                                                 const __grid_constant__ JoinTableDev jt, long long n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const TileView t = tile_view(P, smem, MAXACC);
+    tile_init<MAXACC>(P, t);
+    for (long long base = blockIdx.x * (long long)kTileRows; base < n; base += (long long)gridDim.x * kTileRows) {
+        unsigned int start[kTileV], count[kTileV], first[kTileV];
+        unsigned int most = 0;
+#pragma unroll
+        for (int v = 0; v < kTileV; v++) {
+            const long long i = base + v * (long long)kThreads + threadIdx.x;
+            count[v] = 0;
+            start[v] = first[v] = 0;
+            if (i < n && (pred.nleaves == 0 || predicate_holds(pred, i)) && valid_at(pkv, i)) {
+                if (!jt_lookup(jt, load_int(pk, pk_type, i), &start[v], &count[v], &first[v])) count[v] = 0;
+            }
+            most = max(most, count[v]);
+        }
+        // Round m folds every row's m-th match (rows matching one build row: one round).
+        for (unsigned int m = 0; __syncthreads_or(m < most); m++) {
+            bool live[kTileV], kv[kTileV];
+            long long k[kTileV], rp[kTileV], rb[kTileV];
+#pragma unroll
+            for (int v = 0; v < kTileV; v++) {
+                rp[v] = base + v * (long long)kThreads + threadIdx.x;
+                live[v] = m < count[v];
+                rb[v] = live[v] ? (m == 0 ? first[v] : jt.rows[start[v] + m]) : 0;
+                const long long grow = gkey.side ? rb[v] : rp[v];
+                kv[v] = live[v] && valid_at(gkey.validity, grow);
+                k[v] = kv[v] ? load_int(gkey.values, gkey.type, grow) : 0;
+            }
+            tile_round<MAXACC>(P, t, live, kv, k, rp, rb);
+        }
+    }
+    tile_flush<MAXACC>(P, t);
+}
+
+// ---- streamed row loop ----------------------------------------------------
+//
+// One producer warp streams every input column the query reads from the
+// probe side (predicate, keys, aggregate inputs, validity bitmaps) into a
+// ring of kStages shared-memory stages with 1-D bulk copies (TMA), kStreamT
+// rows per stage, completing on an mbarrier; kConsumerWarps warps fold the
+// rows from shared memory.  One thread keeps ~kStages x 20 KB per CTA in
+// flight, which is what saturates HBM; the consumers see shared-memory
+// latency for the columns and spend their instructions on the fold.  A tile
+// whose columns are not whole 16-byte pieces (the last, partial one) is read
+// straight from global memory instead.  All waits are bounded.
+//
+// The CTA table is slot-major ("aos" arrays per slot) so a Float64 sum and
+// its compensation sit in one aligned 16-byte pair, updated together by a
+// 128-bit compare-and-swap with an exact TwoSum: compensated partials for
+// the price of one atomic.
+
+constexpr int kStreamT = 1024;  // rows per stage
+constexpr int kConsumerWarps = 8;
+constexpr int kStreamThreads = 32 * (1 + kConsumerWarps);
+constexpr int kStages = 3;
+constexpr int kMaxStreamCols = 8;
+
+struct StreamCol {
+    const void* values;
+    const uint8_t* validity;
+    int width;  // bytes per row: 4 or 8
+    int type;
+    int voff;   // offset of the values within a stage
+    int boff;   // offset of the validity bits within a stage (-1: none)
+};
+
+struct StreamPlan {
+    int ncols;
+    StreamCol cols[kMaxStreamCols];
+    int stage_bytes;
+    int tx_bytes;  // bytes the bulk copies of one full stage deliver
+    long long n, ntiles;
+    int leaf_col[kMaxLeaves];  // stream column of each predicate leaf
+    int acc_col[kMaxAccs];     // stream column of each probe-side accumulator, -1 otherwise
+    int key_col;               // group key (plain aggregate) or probe key (join)
+    int aos;                   // 8-byte words per CTA-table slot (even)
+    int aos_idx[kMaxArrays];   // word of each accumulator array within a slot
+};
+
+struct StreamView {
+    unsigned char* stages;
+    unsigned long long* full;
+    unsigned long long* empty;
+    int* direct;
+    long long* keys;          // S (hash mode)
+    unsigned long long* tab;  // S * aos
+    int* fill;
+    int* abort;
+};
+
+size_t stream_smem_bytes(int S, int stage_bytes, int aos) {
+    return (size_t)kStages * stage_bytes + 16 * kStages + 16 * kStages + 16 + 8ull * S * (1 + aos) + 64;
+}
+
+__device__ __forceinline__ StreamView stream_view(const AggProgram& P, const StreamPlan& SP, unsigned char* smem) {
+    StreamView v;
+    v.stages = smem;
+    unsigned char* p = smem + (size_t)kStages * SP.stage_bytes;
+    v.full = (unsigned long long*)p;
+    v.empty = v.full + kStages;
+    v.direct = (int*)(v.empty + kStages);
+    p = (unsigned char*)(v.direct + 4 * kStages);
+    p = (unsigned char*)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    v.keys = (long long*)p;
+    v.tab = (unsigned long long*)(v.keys + P.smem_slots);
+    v.fill = (int*)(v.tab + (long long)P.smem_slots * SP.aos);
+    v.abort = v.fill + 1;
+    return v;
+}
+
+// Column c of tile row r: from the stage, or (direct tiles) from global row g.
+__device__ __forceinline__ long long stream_raw(const StreamPlan& SP, int c, const unsigned char* stage, bool direct,
+                                                long long g, int r) {
+    const StreamCol& col = SP.cols[c];
+    if (!direct) {
+        const unsigned char* q = stage + col.voff + (size_t)r * col.width;
+        return col.width == 8 ? *(const long long*)q : (long long)*(const int*)q;
+    }
+    return col.width == 8 ? __ldcs((const long long*)col.values + g) : (long long)__ldcs((const int*)col.values + g);
+}
+
+__device__ __forceinline__ bool stream_valid(const StreamPlan& SP, int c, const unsigned char* stage, bool direct,
+                                             long long g, int r) {
+    const StreamCol& col = SP.cols[c];
+    if (!col.validity) return true;
+    if (!direct) return (stage[col.boff + (r >> 3)] >> (r & 7)) & 1;
+    return valid_at(col.validity, g);
+}
+
+__device__ __forceinline__ bool stream_predicate(const DevPredicate& pred, const StreamPlan& SP,
+                                                 const unsigned char* stage, bool direct, long long g, int r) {
+    for (int l = 0; l < pred.nleaves; l++) {
+        const int c = SP.leaf_col[l];
+        if (!stream_valid(SP, c, stage, direct, g, r)) return false;
+        const long long raw = stream_raw(SP, c, stage, direct, g, r);
+        const long long a = pred.leaves[l].type == kFloat64 ? filter_order_key(__longlong_as_double(raw)) : raw;
+        if (!cmp_holds(pred.leaves[l].op, a, pred.leaves[l].lit)) return false;
+    }
+    return true;
+}
+
+// What an accumulator takes from a value (its identity when NULL).
+__device__ __forceinline__ unsigned long long contribution_raw(int kind, int in_type, bool valid, long long raw) {
+    switch (kind) {
+        case kAccCount: return valid ? 1ull : 0ull;
+        case kAccSumInt: return valid ? (unsigned long long)raw : 0ull;
+        case kAccSumF64:
+            if (!valid) return 0ull;
+            return in_type == kFloat64 ? (unsigned long long)raw : as_u64((double)raw);
+        case kAccMin:
+            if (!valid) return 0x7fffffffffffffffull;
+            return (unsigned long long)(in_type == kFloat64 ? total_order_key(__longlong_as_double(raw)) : raw);
+        default:
+            if (!valid) return 0x8000000000000000ull;
+            return (unsigned long long)(in_type == kFloat64 ? total_order_key(__longlong_as_double(raw)) : raw);
+    }
+}
+
+// Folds one row's values into CTA slot `slot` (slot-major table).
+template <int MAXACC>
+__device__ __forceinline__ void stream_apply(const AggProgram& P, const StreamPlan& SP, const StreamView& v,
+                                             int slot, const unsigned long long* val) {
+    unsigned long long* t = v.tab + (long long)slot * SP.aos;
+    atomicAdd(&t[SP.aos_idx[0]], 1ull);
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        if (j >= P.nacc) break;
+        const DevAcc& a = P.acc[j];
+        unsigned long long* p = t + SP.aos_idx[a.arr];
+        switch (a.kind) {
+            case kAccCount:
+            case kAccSumInt:
+                if (val[j]) atomicAdd(p, val[j]);
+                break;
+            case kAccSumF64: {
+                const double x = as_f64(val[j]);
+                unsigned long long s = p[0], c = p[1];
+                int tries = 0;
+                for (; tries < (1 << 20); tries++) {
+                    double cs = as_f64(c);
+                    const double ns = two_sum_into(as_f64(s), x, &cs);
+                    unsigned long long os, oc;
+                    cas128_shared(smem_addr(p), s, c, as_u64(ns), as_u64(cs), &os, &oc);
+                    if (os == s && oc == c) break;
+                    s = os;
+                    c = oc;
+                }
+                if (tries == (1 << 20)) atomicOr(P.status, kStatusTimeout);
+                break;
+            }
+            case kAccMin:
+                if (val[j] != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)val[j]);
+                break;
+            default:
+                if (val[j] != 0x8000000000000000ull) atomicMax((long long*)p, (long long)val[j]);
+                break;
+        }
+    }
+}
+
+// One row: its group key (valid or not) and values, folded into the CTA
+// table, or straight into HBM when the key has no slot there.
+template <int MAXACC>
+__device__ __forceinline__ void stream_fold(const AggProgram& P, const StreamPlan& SP, const StreamView& v,
+                                            bool kvalid, long long key, const unsigned long long* val) {
+    const int slot = (kvalid && key != kEmptyKey) ? smem_slot(P, key, v.keys, v.fill) : kSlotGlobal;
+    if (slot >= 0) {
+        stream_apply<MAXACC>(P, SP, v, slot, val);
+    } else {
+        double comp[MAXACC];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) comp[j] = 0.0;
+        const long long g = global_slot(P, kvalid, key);
+        if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+    }
+}
+
+__device__ void stream_init(const AggProgram& P, const StreamPlan& SP, const StreamView& v) {
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) v.keys[i] = kEmptyKey;
+    for (int i = threadIdx.x; i < S * SP.aos; i += blockDim.x) {
+        const int w = i % SP.aos;
+        unsigned long long x = 0;
+        for (int a = 0; a < P.narrays; a++)
+            if (SP.aos_idx[a] == w) x = init_value(P.init[a]);
+        v.tab[i] = x;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&v.full[s], 1);
+            mbar_init(&v.empty[s], kConsumerWarps);
+        }
+        *v.fill = 0;
+        *v.abort = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+}
+
+// Merges the CTA table into HBM.
+__device__ void stream_flush(const AggProgram& P, const StreamPlan& SP, const StreamView& v) {
+    __syncthreads();
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        const unsigned long long* t = v.tab + (long long)i * SP.aos;
+        if (t[SP.aos_idx[0]] == 0) continue;  // no rows in this slot
+        const long long key = P.direct ? P.direct_lo + i : v.keys[i];
+        const long long g = global_slot(P, true, key);
+        if (g < 0) continue;
+        for (int a = 0; a < P.narrays; a++) {
+            const unsigned long long x = t[SP.aos_idx[a]];
+            unsigned long long* d = P.arr + a * P.stride + g;
+            switch (P.merge[a]) {
+                case kMergeAddU64:
+                    if (x) atomicAdd(d, x);
+                    break;
+                case kMergeAddF64Comp:
+                    add_f64_comp((double*)d, (double*)(d + P.stride), as_f64(x));
+                    break;
+                case kMergeAddF64:
+                    if (as_f64(x) != 0.0) atomicAdd((double*)d, as_f64(x));
+                    break;
+                case kMergeMin:
+                    if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)d, (long long)x);
+                    break;
+                default:
+                    if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)d, (long long)x);
+                    break;
+            }
+        }
+    }
+}
+
+// The producer: one lane streams this CTA's tiles into the stage ring.
+__device__ void stream_produce(const AggProgram& P, const StreamPlan& SP, const StreamView& v) {
+    const unsigned long long pol = policy_evict_first();
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < SP.ntiles; tile += gridDim.x, it++) {
+        const int st = it % kStages;
+        if (it >= kStages && !mbar_wait(&v.empty[st], ((it / kStages) - 1) & 1)) {
+            atomicOr(P.status, kStatusTimeout);
+            *(volatile int*)v.abort = 1;
+            break;
+        }
+        if (*(volatile int*)v.abort) break;
+        const long long base = tile * kStreamT;
+        const bool direct = SP.n - base < kStreamT;
+        v.direct[st] = direct;
+        if (direct) {
+            mbar_arrive(&v.full[st]);
+            continue;
+        }
+        unsigned char* stage = v.stages + (size_t)st * SP.stage_bytes;
+        mbar_arrive_expect_tx(&v.full[st], (unsigned)SP.tx_bytes);
+        for (int c = 0; c < SP.ncols; c++) {
+            const StreamCol& col = SP.cols[c];
+            bulk_copy_g2s(stage + col.voff, (const unsigned char*)col.values + base * col.width,
+                          (unsigned)(kStreamT * col.width), &v.full[st], pol);
+            if (col.validity)
+                bulk_copy_g2s(stage + col.boff, col.validity + base / 8, kStreamT / 8, &v.full[st], pol);
+        }
+    }
+    // Before leaving, wait for the copies still landing in this CTA's stages.
+    for (int k = 1; k <= kStages && k <= it; k++) {
+        const int use = it - k;
+        mbar_wait(&v.full[use % kStages], (use / kStages) & 1);
+    }
+}
+
+template <int MAXACC>
+__global__ void __launch_bounds__(kStreamThreads) agg_stream_rows_kernel(const __grid_constant__ AggProgram P,
+                                                                         const __grid_constant__ DevPredicate pred,
+                                                                         const __grid_constant__ StreamPlan SP) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const StreamView v = stream_view(P, SP, smem);
+    stream_init(P, SP, v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        if (lane == 0) stream_produce(P, SP, v);
+        __syncwarp();
+    } else {
+        const int ct = threadIdx.x - 32;
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < SP.ntiles; tile += gridDim.x, it++) {
+            const int st = it % kStages;
+            if (!mbar_wait(&v.full[st], (it / kStages) & 1) || *(volatile int*)v.abort) {
+                atomicOr(P.status, kStatusTimeout);
+                *(volatile int*)v.abort = 1;
+                break;
+            }
+            const bool direct = v.direct[st];
+            const unsigned char* stage = v.stages + (size_t)st * SP.stage_bytes;
+#pragma unroll
+            for (int k = 0; k < kStreamT / (32 * kConsumerWarps); k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                if (g >= SP.n) continue;
+                if (pred.nleaves && !stream_predicate(pred, SP, stage, direct, g, r)) continue;
+                const bool kv = stream_valid(SP, SP.key_col, stage, direct, g, r);
+                const long long key = kv ? stream_raw(SP, SP.key_col, stage, direct, g, r) : 0;
+                unsigned long long val[MAXACC];
+#pragma unroll
+                for (int j = 0; j < MAXACC; j++) {
+                    if (j >= P.nacc) break;
+                    const int c = SP.acc_col[j];
+                    val[j] = contribution_raw(P.acc[j].kind, P.acc[j].in_type, stream_valid(SP, c, stage, direct, g, r),
+                                              stream_raw(SP, c, stage, direct, g, r));
+                }
+                stream_fold<MAXACC>(P, SP, v, kv, key, val);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&v.empty[st]);
+        }
+    }
+    stream_flush(P, SP, v);
+}
+
+template <int MAXACC>
+__global__ void __launch_bounds__(kStreamThreads) agg_stream_join_kernel(const __grid_constant__ AggProgram P,
+                                                                         const __grid_constant__ DevPredicate pred,
+                                                                         const __grid_constant__ StreamPlan SP,
+                                                                         const __grid_constant__ AggKey gkey,
+                                                                         const __grid_constant__ JoinTableDev jt) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const StreamView v = stream_view(P, SP, smem);
+    stream_init(P, SP, v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        if (lane == 0) stream_produce(P, SP, v);
+        __syncwarp();
+    } else {
+        const unsigned long long keep = policy_evict_last();
+        const int ct = threadIdx.x - 32;
+        constexpr int kRows = kStreamT / (32 * kConsumerWarps);
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < SP.ntiles; tile += gridDim.x, it++) {
+            const int st = it % kStages;
+            if (!mbar_wait(&v.full[st], (it / kStages) & 1) || *(volatile int*)v.abort) {
+                atomicOr(P.status, kStatusTimeout);
+                *(volatile int*)v.abort = 1;
+                break;
+            }
+            const bool direct = v.direct[st];
+            const unsigned char* stage = v.stages + (size_t)st * SP.stage_bytes;
+            // Look every row's key up first: kRows independent L2 chains.
+            unsigned int start[kRows], count[kRows], first[kRows];
+#pragma unroll
+            for (int k = 0; k < kRows; k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                count[k] = 0;
+                start[k] = first[k] = 0;
+                if (g >= SP.n) continue;
+                if (pred.nleaves && !stream_predicate(pred, SP, stage, direct, g, r)) continue;
+                if (!stream_valid(SP, SP.key_col, stage, direct, g, r)) continue;
+                const long long pkey = stream_raw(SP, SP.key_col, stage, direct, g, r);
+                if (pkey == kEmptyKey) {
+                    start[k] = jt.special_start;
+                    count[k] = jt.special_count;
+                    first[k] = count[k] ? jt.first_row[jt.capacity] : 0u;
+                    continue;
+                }
+                unsigned int s = (unsigned int)(fmix64((unsigned long long)pkey) & (jt.capacity - 1u));
+                for (unsigned int p = 0; p < jt.capacity; p++) {
+                    const int4 slot = ld_keep_v4(&jt.slots[s], keep);
+                    const unsigned int fr = ld_keep_u32(&jt.first_row[s], keep);
+                    const long long sk = ((long long)(unsigned int)slot.y << 32) | (unsigned int)slot.x;
+                    if (sk == pkey) {
+                        start[k] = (unsigned int)slot.z;
+                        count[k] = (unsigned int)slot.w;
+                        first[k] = fr;
+                        break;
+                    }
+                    if (sk == kEmptyKey) break;
+                    s = (s + 1u) & (jt.capacity - 1u);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kRows; k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                for (unsigned int m = 0; m < count[k]; m++) {
+                    const long long b = m == 0 ? first[k] : jt.rows[start[k] + m];
+                    const long long grow = gkey.side ? b : g;
+                    bool kv;
+                    long long key;
+                    if (gkey.side) {
+                        kv = valid_at(gkey.validity, grow);
+                        key = kv ? (gkey.type == kInt64 ? ld_keep_s64((const long long*)gkey.values + grow, keep)
+                                                        : (long long)(int)ld_keep_u32((const int*)gkey.values + grow, keep))
+                                 : 0;
+                    } else {
+                        kv = valid_at(gkey.validity, grow);
+                        key = kv ? load_int(gkey.values, gkey.type, grow) : 0;
+                    }
+                    unsigned long long val[MAXACC];
+#pragma unroll
+                    for (int j = 0; j < MAXACC; j++) {
+                        if (j >= P.nacc) break;
+                        const DevAcc& a = P.acc[j];
+                        const int c = SP.acc_col[j];
+                        if (c >= 0) {
+                            val[j] = contribution_raw(a.kind, a.in_type, stream_valid(SP, c, stage, direct, g, r),
+                                                      stream_raw(SP, c, stage, direct, g, r));
+                        } else {
+                            val[j] = contribution(a, g, b);
+                        }
+                    }
+                    stream_fold<MAXACC>(P, SP, v, kv, key, val);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&v.empty[st]);
+        }
+    }
+    stream_flush(P, SP, v);
+}
+
+// ---- streamed tile sort-reduce ----------------------------------------------
+//
+// The producer warp streams the columns as above; the consumer warps take
+// a stage's rows into registers and release the stage at once (so the next
+// copies overlap the rest of the tile), then counting-sort the rows by CTA
+// slot in shared memory and reduce each slot's run with one writer per slot
+// (a thread, or a warp for runs of kBigRun rows or more): no atomics on the
+// accumulators, no contention whatever the skew, compensated Float64 sums.
+// Only the consumer warps meet at their barriers (named barrier 1).
+
+constexpr int kSTRows = kStreamT / (32 * kConsumerWarps);  // rows per consumer thread per stage
+
+__device__ __forceinline__ void consumer_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(32 * kConsumerWarps) : "memory");
+}
+
+// A consumer-warps barrier that also ORs a flag across them.
+__device__ __forceinline__ bool consumer_sync_or(bool x) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((unsigned)x), "n"(32 * kConsumerWarps)
+        : "memory");
+    return r != 0;
+}
+
+struct STView {
+    unsigned char* stages;
+    unsigned long long* full;
+    unsigned long long* empty;
+    int* direct;
+    long long* keys;           // S (hash mode)
+    unsigned long long* arr;   // narrays * S
+    unsigned long long* tval;  // maxacc * kStreamT
+    unsigned int* cnt;         // S
+    unsigned int* off;         // S
+    unsigned int* big;         // kStreamT / kBigRun
+    int* misc;                 // [0] big runs, [1] table fill, [2..9] scan warp sums, [10] abort
+};
+
+size_t stile_smem_bytes(int S, int stage_bytes, int narrays, int maxacc) {
+    return (size_t)kStages * stage_bytes + 16 * kStages + 16 * kStages + 16 + 8ull * S * (1 + narrays) +
+           8ull * maxacc * kStreamT + 8ull * S + 4ull * (kStreamT / kBigRun) + 64;
+}
+
+__device__ __forceinline__ STView stile_view(const AggProgram& P, const StreamPlan& SP, unsigned char* smem,
+                                             int maxacc) {
+    STView v;
+    const int S = P.smem_slots;
+    v.stages = smem;
+    unsigned char* p = smem + (size_t)kStages * SP.stage_bytes;
+    v.full = (unsigned long long*)p;
+    v.empty = v.full + kStages;
+    v.direct = (int*)(v.empty + kStages);
+    p = (unsigned char*)(v.direct + 4 * kStages);
+    p = (unsigned char*)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    v.keys = (long long*)p;
+    v.arr = (unsigned long long*)(v.keys + S);
+    v.tval = v.arr + (long long)S * P.narrays;
+    v.cnt = (unsigned int*)(v.tval + (long long)maxacc * kStreamT);
+    v.off = v.cnt + S;
+    v.big = v.off + S;
+    v.misc = (int*)(v.big + kStreamT / kBigRun);
+    return v;
+}
+
+// add_run over the stream-tile layout.
+template <int MAXACC>
+__device__ __forceinline__ void st_add_run(const AggProgram& P, const STView& v, int b, unsigned long long rows,
+                                           const unsigned long long* val, const double* comp) {
+    const int S = P.smem_slots;
+    v.arr[b] += rows;
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        if (j >= P.nacc) break;
+        const DevAcc& a = P.acc[j];
+        unsigned long long* p = v.arr + a.arr * S + b;
+        if (a.kind == kAccSumF64) {
+            double c = as_f64(p[S]) + comp[j];
+            *p = as_u64(two_sum_into(as_f64(*p), as_f64(val[j]), &c));
+            p[S] = as_u64(c);
+        } else {
+            double unused = 0.0;
+            *p = combine(a.kind, *p, val[j], &unused);
+        }
+    }
+}
+
+// One tile round among the consumer threads (ct in 0..255): rank every row
+// in its slot, scan the counts, scatter, reduce the runs.
+template <int MAXACC>
+__device__ __forceinline__ void st_round(const AggProgram& P, const STView& v, int ct, const int* slot,
+                                         unsigned long long (*val)[MAXACC]) {
+    const int S = P.smem_slots;
+    unsigned int rank[kSTRows];
+#pragma unroll
+    for (int k = 0; k < kSTRows; k++)
+        if (slot[k] >= 0) rank[k] = atomicAdd(&v.cnt[slot[k]], 1u);
+    consumer_sync();
+    {  // exclusive scan of the counts
+        const int nt = 32 * kConsumerWarps;
+        const int per = (S + nt - 1) / nt;
+        const int lo = ct * per, hi = min(lo + per, S);
+        unsigned int sum = 0;
+        for (int b = lo; b < hi; b++) sum += v.cnt[b];
+        const int lane = ct & 31, w = ct >> 5;
+        unsigned int x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) v.misc[2 + w] = (int)x;
+        consumer_sync();
+        unsigned int run = x - sum;
+        for (int q = 0; q < w; q++) run += (unsigned int)v.misc[2 + q];
+        for (int b = lo; b < hi; b++) {
+            v.off[b] = run;
+            run += v.cnt[b];
+        }
+    }
+    consumer_sync();
+#pragma unroll
+    for (int k = 0; k < kSTRows; k++) {
+        if (slot[k] < 0) continue;
+        const unsigned int pos = v.off[slot[k]] + rank[k];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++)
+            if (j < P.nacc) v.tval[j * kStreamT + pos] = val[k][j];
+    }
+    consumer_sync();
+    // small runs: one thread per slot
+    for (int b = ct; b < S; b += 32 * kConsumerWarps) {
+        const unsigned int c = v.cnt[b];
+        if (c == 0) continue;
+        if (c >= kBigRun) {
+            v.big[atomicAdd(&v.misc[0], 1)] = b;
+            continue;
+        }
+        const unsigned int o = v.off[b];
+        unsigned long long acc[MAXACC];
+        double comp[MAXACC];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) {
+            comp[j] = 0.0;
+            acc[j] = j < P.nacc ? v.tval[j * kStreamT + o] : 0ull;
+        }
+        for (unsigned int e = 1; e < c; e++) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                acc[j] = combine(P.acc[j].kind, acc[j], v.tval[j * kStreamT + o + e], &comp[j]);
+            }
+        }
+        st_add_run<MAXACC>(P, v, b, c, acc, comp);
+        v.cnt[b] = 0;
+    }
+    consumer_sync();
+    // big runs: one warp per slot
+    const int lane = ct & 31, w = ct >> 5;
+    const int nbig = v.misc[0];
+    for (int r = w; r < nbig; r += kConsumerWarps) {
+        const int b = (int)v.big[r];
+        const unsigned int c = v.cnt[b], o = v.off[b];
+        unsigned long long acc[MAXACC];
+        double comp[MAXACC];
+#pragma unroll
+        for (int j = 0; j < MAXACC; j++) {
+            comp[j] = 0.0;
+            acc[j] = j < P.nacc ? v.tval[j * kStreamT + o + lane] : 0ull;
+        }
+        for (unsigned int e = lane + 32; e < c; e += 32) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                acc[j] = combine(P.acc[j].kind, acc[j], v.tval[j * kStreamT + o + e], &comp[j]);
+            }
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                const unsigned long long x = __shfl_xor_sync(0xffffffffu, acc[j], d);
+                const double xc = __shfl_xor_sync(0xffffffffu, comp[j], d);
+                if (P.acc[j].kind == kAccSumF64) comp[j] += xc;
+                acc[j] = combine(P.acc[j].kind, acc[j], x, &comp[j]);
+            }
+        }
+        if (lane == 0) {
+            st_add_run<MAXACC>(P, v, b, c, acc, comp);
+            v.cnt[b] = 0;
+        }
+    }
+    consumer_sync();
+    if (ct == 0) v.misc[0] = 0;
+}
+
+template <int MAXACC, bool JOIN>
+__global__ void __launch_bounds__(kStreamThreads) agg_stile_kernel(const __grid_constant__ AggProgram P,
+                                                                   const __grid_constant__ DevPredicate pred,
+                                                                   const __grid_constant__ StreamPlan SP,
+                                                                   const __grid_constant__ AggKey gkey,
+                                                                   const __grid_constant__ JoinTableDev jt) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const STView v = stile_view(P, SP, smem, MAXACC);
+    {  // init
+        const int S = P.smem_slots;
+        for (int i = threadIdx.x; i < S; i += blockDim.x) {
+            v.keys[i] = kEmptyKey;
+            v.cnt[i] = 0;
+        }
+        for (int i = threadIdx.x; i < S * P.narrays; i += blockDim.x) v.arr[i] = init_value(P.init[i / S]);
+        if (threadIdx.x < 16) v.misc[threadIdx.x] = 0;
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < kStages; s++) {
+                mbar_init(&v.full[s], 1);
+                mbar_init(&v.empty[s], kConsumerWarps);
+            }
+            fence_barrier_init();
+        }
+        __syncthreads();
+    }
+    StreamView sv;  // the producer's view of the same ring
+    sv.stages = v.stages;
+    sv.full = v.full;
+    sv.empty = v.empty;
+    sv.direct = v.direct;
+    sv.abort = v.misc + 10;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        if (lane == 0) stream_produce(P, SP, sv);
+        __syncwarp();
+    } else {
+        const unsigned long long keep = policy_evict_last();
+        const int ct = threadIdx.x - 32;
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < SP.ntiles; tile += gridDim.x, it++) {
+            const int st = it % kStages;
+            // Every consumer waits, so they all agree on whether to go on.
+            const bool ok = mbar_wait(&v.full[st], (it / kStages) & 1) && !*(volatile int*)sv.abort;
+            if (consumer_sync_or(!ok)) {
+                if (ct == 0) {
+                    atomicOr(P.status, kStatusTimeout);
+                    *(volatile int*)sv.abort = 1;
+                }
+                break;
+            }
+            const bool direct = v.direct[st];
+            const unsigned char* stage = v.stages + (size_t)st * SP.stage_bytes;
+            int slot[kSTRows];
+            unsigned long long val[kSTRows][MAXACC];
+            unsigned int start[kSTRows], count[kSTRows];
+            long long brow[kSTRows];
+#pragma unroll
+            for (int k = 0; k < kSTRows; k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                slot[k] = kSlotNone;
+                count[k] = 0;
+                start[k] = 0;
+                brow[k] = 0;
+                if (g >= SP.n) continue;
+                if (pred.nleaves && !stream_predicate(pred, SP, stage, direct, g, r)) continue;
+                bool kv;
+                long long key;
+                if (JOIN) {
+                    if (!stream_valid(SP, SP.key_col, stage, direct, g, r)) continue;
+                    const long long pkey = stream_raw(SP, SP.key_col, stage, direct, g, r);
+                    unsigned int first = 0;
+                    if (pkey == kEmptyKey) {
+                        start[k] = jt.special_start;
+                        count[k] = jt.special_count;
+                        first = count[k] ? jt.first_row[jt.capacity] : 0u;
+                    } else {
+                        unsigned int s = (unsigned int)(fmix64((unsigned long long)pkey) & (jt.capacity - 1u));
+                        for (unsigned int p = 0; p < jt.capacity; p++) {
+                            const int4 sl = ld_keep_v4(&jt.slots[s], keep);
+                            const unsigned int fr = ld_keep_u32(&jt.first_row[s], keep);
+                            const long long sk = ((long long)(unsigned int)sl.y << 32) | (unsigned int)sl.x;
+                            if (sk == pkey) {
+                                start[k] = (unsigned int)sl.z;
+                                count[k] = (unsigned int)sl.w;
+                                first = fr;
+                                break;
+                            }
+                            if (sk == kEmptyKey) break;
+                            s = (s + 1u) & (jt.capacity - 1u);
+                        }
+                    }
+                    if (count[k] == 0) continue;
+                    brow[k] = first;
+                    const long long grow = gkey.side ? brow[k] : g;
+                    kv = valid_at(gkey.validity, grow);
+                    key = 0;
+                    if (kv)
+                        key = gkey.side ? (gkey.type == kInt64 ? ld_keep_s64((const long long*)gkey.values + grow, keep)
+                                                               : (long long)(int)ld_keep_u32((const int*)gkey.values + grow, keep))
+                                        : load_int(gkey.values, gkey.type, grow);
+                } else {
+                    kv = stream_valid(SP, SP.key_col, stage, direct, g, r);
+                    key = kv ? stream_raw(SP, SP.key_col, stage, direct, g, r) : 0;
+                }
+#pragma unroll
+                for (int j = 0; j < MAXACC; j++) {
+                    if (j >= P.nacc) break;
+                    const int c = SP.acc_col[j];
+                    val[k][j] = c >= 0 ? contribution_raw(P.acc[j].kind, P.acc[j].in_type,
+                                                          stream_valid(SP, c, stage, direct, g, r),
+                                                          stream_raw(SP, c, stage, direct, g, r))
+                                       : contribution(P.acc[j], g, brow[k]);
+                }
+                slot[k] = (kv && key != kEmptyKey) ? smem_slot(P, key, v.keys, v.misc + 1) : kSlotGlobal;
+                if (slot[k] == kSlotGlobal) {
+                    double comp[MAXACC];
+#pragma unroll
+                    for (int j = 0; j < MAXACC; j++) comp[j] = 0.0;
+                    const long long gs = global_slot(P, kv, key);
+                    if (gs >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, gs, 1, val[k], comp);
+                }
+            }
+            // A join row's further matches (a key repeated on the build side)
+            // read the stage too, so they fold into HBM before it is released.
+            if (JOIN) {
+#pragma unroll
+                for (int k = 0; k < kSTRows; k++) {
+                    const int r = ct + k * 32 * kConsumerWarps;
+                    const long long g = tile * kStreamT + r;
+                    for (unsigned int m = 1; m < count[k]; m++) {
+                        const long long b = jt.rows[start[k] + m];
+                        const long long grow = gkey.side ? b : g;
+                        const bool kv = valid_at(gkey.validity, grow);
+                        const long long key = kv ? load_int(gkey.values, gkey.type, grow) : 0;
+                        unsigned long long x[MAXACC];
+                        double comp[MAXACC];
+#pragma unroll
+                        for (int j = 0; j < MAXACC; j++) {
+                            comp[j] = 0.0;
+                            if (j >= P.nacc) break;
+                            const int c = SP.acc_col[j];
+                            x[j] = c >= 0 ? contribution_raw(P.acc[j].kind, P.acc[j].in_type,
+                                                             stream_valid(SP, c, stage, direct, g, r),
+                                                             stream_raw(SP, c, stage, direct, g, r))
+                                          : contribution(P.acc[j], g, b);
+                        }
+                        const long long gs = global_slot(P, kv, key);
+                        if (gs >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, gs, 1, x, comp);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&v.empty[st]);  // the stage may be refilled now
+            st_round<MAXACC>(P, v, ct, slot, val);
+        }
+    }
+    __syncthreads();
+    // flush the CTA table into HBM
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        if (v.arr[i] == 0) continue;
+        const long long key = P.direct ? P.direct_lo + i : v.keys[i];
+        const long long g = global_slot(P, true, key);
+        if (g >= 0) merge_slot(P, v.arr + i, S, P.arr + g, P.stride);
+    }
+}
+
+// ---- fused probe table: the join + aggregate hot path -----------------------
+//
+// For `probe JOIN build GROUP BY <build column>` with every aggregate input
+// on the probe side, the group a probe row lands in depends only on the join
+// slot it matches.  A pre-pass writes, per join slot, {key, CTA slot of that
+// key's group, count} into a 16-byte entry, so a probe row needs one L2 load
+// to know both whether it matches and where it folds.  The row loop then
+// runs at full occupancy (small shared footprint) with plain coalesced loads,
+// and folds with per-lane shared atomics: native 64-bit adds, and for Float64
+// sums one 128-bit CAS of the (sum, compensation) pair.  Keys repeated on the
+// build side, NULL group keys and groups outside the CTA table's range take a
+// slow path that is correct for any shape.
+
+struct FusedSlot {
+    long long key;
+    int cslot;           // the group's CTA slot, -1: none (slow path)
+    unsigned int count;  // matches (0: empty slot)
+};
+
+constexpr int kFusedThreads = 256;
+
+__global__ void fuse_table_kernel(const __grid_constant__ JoinTableDev jt, const __grid_constant__ AggKey gkey,
+                                  long long lo, int S, FusedSlot* __restrict__ out) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < jt.capacity;
+         s += (long long)gridDim.x * blockDim.x) {
+        const JoinSlot js = jt.slots[s];
+        FusedSlot f;
+        f.key = js.key;
+        f.count = js.count;
+        f.cslot = -1;
+        if (js.count == 1) {
+            const unsigned int b = jt.first_row[s];
+            if (valid_at(gkey.validity, b)) {
+                const unsigned long long d = (unsigned long long)(load_int(gkey.values, gkey.type, b) - lo);
+                if (d < (unsigned long long)S) f.cslot = (int)d;
+            }
+        }
+        out[s] = f;
+    }
+}
+
+struct FusedTab {
+    const FusedSlot* slots;
+    int aos;                  // 8-byte words per CTA slot (even)
+    int aos_idx[kMaxArrays];  // word of each array within a slot
+};
+
+// The slow path of one probe row: every match, folded into HBM.
+template <int MAXACC>
+__device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const JoinTableDev& jt, long long s_or_special,
+                               long long i, const unsigned long long* val) {
+    unsigned int start, count, first;
+    if (s_or_special < 0) {
+        start = jt.special_start;
+        count = jt.special_count;
+        first = count ? jt.first_row[jt.capacity] : 0u;
+    } else {
+        start = jt.slots[s_or_special].start;
+        count = jt.slots[s_or_special].count;
+        first = jt.first_row[s_or_special];
+    }
+    double comp[MAXACC];
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) comp[j] = 0.0;
+    for (unsigned int m = 0; m < count; m++) {
+        const long long b = m == 0 ? first : jt.rows[start + m];
+        const bool kv = valid_at(gkey.validity, b);
+        const long long key = kv ? load_int(gkey.values, gkey.type, b) : 0;
+        const long long g = global_slot(P, kv, key);
+        if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+    }
+    (void)i;
+}
+
+template <int MAXACC, int RPT>
+__global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
+    const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
+    const __grid_constant__ FusedTab ft, long long n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int S = P.smem_slots;
+    unsigned long long* tab = (unsigned long long*)smem;  // S * aos words, slot-major
+    for (int i = threadIdx.x; i < S * ft.aos; i += blockDim.x) {
+        const int w = i % ft.aos;
+        unsigned long long x = 0;
+        for (int a = 0; a < P.narrays; a++)
+            if (ft.aos_idx[a] == w) x = init_value(P.init[a]);
+        tab[i] = x;
+    }
+    __syncthreads();
+    const unsigned long long keep = policy_evict_last();
+    const unsigned int cap_mask = jt.capacity - 1u;
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long base = blockIdx.x * (long long)blockDim.x * RPT; base < n; base += step) {
+        long long sidx[RPT];  // matched join slot, -1 special key, -2 no match
+        int cslot[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const long long i = base + r * (long long)blockDim.x + threadIdx.x;
+            sidx[r] = -2;
+            cslot[r] = -1;
+            if (i >= n) continue;
+            if (pred.nleaves && !predicate_holds(pred, i)) continue;
+            if (!valid_at(pkv, i)) continue;
+            const long long key = pk_type == kInt64 ? __ldcs((const long long*)pk + i) : (long long)__ldcs((const int*)pk + i);
+            if (key == kEmptyKey) {
+                if (jt.special_count) sidx[r] = -1;
+                continue;
+            }
+            unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & cap_mask);
+            for (unsigned int p = 0; p <= cap_mask; p++) {
+                const int4 e = ld_keep_v4(&ft.slots[s], keep);
+                const long long k = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
+                if (k == key) {
+                    sidx[r] = s;
+                    cslot[r] = (unsigned int)e.w == 1u ? e.z : -1;
+                    break;
+                }
+                if (k == kEmptyKey) break;
+                s = (s + 1u) & cap_mask;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            if (sidx[r] == -2) continue;
+            const long long i = base + r * (long long)blockDim.x + threadIdx.x;
+            unsigned long long val[MAXACC];
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                const DevAcc& a = P.acc[j];
+                const bool v = valid_at(a.validity, i);
+                long long raw = 0;
+                if (v) raw = a.in_type == kInt32 ? (long long)__ldcs((const int*)a.values + i)
+                                                 : __ldcs((const long long*)a.values + i);
+                val[j] = contribution_raw(a.kind, a.in_type, v, raw);
+            }
+            if (cslot[r] < 0) {
+                fused_slow_row<MAXACC>(P, gkey, jt, sidx[r], i, val);
+                continue;
+            }
+            unsigned long long* t = tab + (long long)cslot[r] * ft.aos;
+            atomicAdd(&t[ft.aos_idx[0]], 1ull);
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                if (j >= P.nacc) break;
+                const DevAcc& a = P.acc[j];
+                unsigned long long* p = t + ft.aos_idx[a.arr];
+                switch (a.kind) {
+                    case kAccCount:
+                    case kAccSumInt:
+                        if (val[j]) atomicAdd(p, val[j]);
+                        break;
+                    case kAccSumF64: {
+                        const double x = as_f64(val[j]);
+                        unsigned long long sv = p[0], cv = p[1];
+                        int tries = 0;
+                        for (; tries < (1 << 20); tries++) {
+                            double cs = as_f64(cv);
+                            const double ns = two_sum_into(as_f64(sv), x, &cs);
+                            unsigned long long os, oc;
+                            cas128_shared(smem_addr(p), sv, cv, as_u64(ns), as_u64(cs), &os, &oc);
+                            if (os == sv && oc == cv) break;
+                            sv = os;
+                            cv = oc;
+                        }
+                        if (tries == (1 << 20)) atomicOr(P.status, kStatusTimeout);
+                        break;
+                    }
+                    case kAccMin:
+                        if (val[j] != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)val[j]);
+                        break;
+                    default:
+                        if (val[j] != 0x8000000000000000ull) atomicMax((long long*)p, (long long)val[j]);
+                        break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        const unsigned long long* t = tab + (long long)i * ft.aos;
+        if (t[ft.aos_idx[0]] == 0) continue;
+        const long long g = global_slot(P, true, P.direct_lo + i);
+        if (g < 0) continue;
+        for (int a = 0; a < P.narrays; a++) {
+            const unsigned long long x = t[ft.aos_idx[a]];
+            unsigned long long* d = P.arr + a * P.stride + g;
+            switch (P.merge[a]) {
+                case kMergeAddU64:
+                    if (x) atomicAdd(d, x);
+                    break;
+                case kMergeAddF64Comp:
+                    add_f64_comp((double*)d, (double*)(d + P.stride), as_f64(x));
+                    break;
+                case kMergeAddF64:
+                    if (as_f64(x) != 0.0) atomicAdd((double*)d, as_f64(x));
+                    break;
+                case kMergeMin:
+                    if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)d, (long long)x);
+                    break;
+                default:
+                    if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)d, (long long)x);
+                    break;
+            }
+        }
+    }
+}
+
+__global__ void agg_init_kernel(const __grid_constant__ AggProgram P) {
     const long long total = (long long)P.narrays * P.stride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x)
-        P.acc[i] = init_value(P.init[i / P.stride]);
+        P.arr[i] = init_value(P.init[i / P.stride]);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P.capacity;
          i += (long long)gridDim.x * blockDim.x)
         P.keys[i] = kEmptyKey;
 }
 
 // Occupied slots (the NULL group aside) as 0/1 flags; also the key range.
-__global__ void agg_flags_kernel(AggProgram P, unsigned int* __restrict__ flags,
+__global__ void agg_flags_kernel(const __grid_constant__ AggProgram P, unsigned int* __restrict__ flags,
                                  unsigned long long* __restrict__ range /* min, max of ordered keys */) {
     unsigned long long lo = ~0ull, hi = 0;
     const long long m = (long long)P.capacity + 2;
@@ -325,7 +1916,7 @@ __global__ void agg_flags_kernel(AggProgram P, unsigned int* __restrict__ flags,
             key = 0;
         } else {
             key = kEmptyKey;
-            occ = P.acc[s] > 0;  // rows of the kEmptyKey group
+            occ = P.arr[s] > 0;  // rows of the kEmptyKey group
         }
         flags[s] = occ ? 1u : 0u;
         if (occ) {
@@ -346,7 +1937,7 @@ __global__ void agg_flags_kernel(AggProgram P, unsigned int* __restrict__ flags,
     }
 }
 
-__global__ void agg_compact_kernel(AggProgram P, const unsigned int* __restrict__ flags,
+__global__ void agg_compact_kernel(const __grid_constant__ AggProgram P, const unsigned int* __restrict__ flags,
                                    const unsigned long long* __restrict__ pos, unsigned long long lo,
                                    unsigned long long* __restrict__ skeys, unsigned int* __restrict__ sslots) {
     const long long m = (long long)P.capacity + 2;
@@ -366,11 +1957,11 @@ struct OutCol {
 struct AggOutput {
     OutCol key;
     int key_type;
-    OutCol cols[kMaxOps];
+    OutCol cols[kMaxOuts];
 };
 
 // One output row per thread: the group at sorted position r, the NULL group last.
-__global__ void agg_emit_kernel(AggProgram P, AggOutput O, const unsigned long long* __restrict__ skeys,
+__global__ void agg_emit_kernel(const __grid_constant__ AggProgram P, const __grid_constant__ AggOutput O, const unsigned long long* __restrict__ skeys,
                                 const unsigned int* __restrict__ sslots, unsigned long long lo, long long G,
                                 long long rows) {
     const int lane = threadIdx.x & 31;
@@ -389,44 +1980,41 @@ __global__ void agg_emit_kernel(AggProgram P, AggOutput O, const unsigned long l
             unsigned int bits = __ballot_sync(0xffffffffu, live && !is_null_group);
             if (lane == 0 && r < rows) O.key.validity[r >> 5] = bits;
         }
-        const unsigned long long* acc = P.acc;
+        const unsigned long long* A = P.arr;
         const long long st = P.stride;
-        for (int j = 0; j < P.nops; j++) {
-            const DevAggOp& op = P.ops[j];
+        for (int j = 0; j < P.nout; j++) {
+            const DevOut& o = P.out[j];
             bool valid = true;
             if (live) {
-                unsigned long long a0 = acc[op.a0 * st + slot];
-                switch (op.func) {
+                const unsigned long long a0 = A[o.arr * st + slot];
+                const unsigned long long nn = A[o.nn * st + slot];
+                switch (o.func) {
                     case OXB_AGG_COUNT:
                     case OXB_AGG_COUNT_STAR:
                         ((unsigned long long*)O.cols[j].values)[r] = a0;
                         break;
                     case OXB_AGG_SUM:
-                        if (op.in_type == kFloat64) {
-                            double s = __longlong_as_double((long long)a0);
-                            double c = __longlong_as_double((long long)acc[op.a1 * st + slot]);
+                        valid = nn > 0;
+                        if (o.in_type == kFloat64) {
+                            double s = as_f64(a0), c = as_f64(A[(o.arr + 1) * st + slot]);
                             ((double*)O.cols[j].values)[r] = isfinite(s) ? __dadd_rn(s, c) : s;
-                            valid = acc[op.a2 * st + slot] > 0;
                         } else {
                             ((unsigned long long*)O.cols[j].values)[r] = a0;
-                            valid = acc[op.a1 * st + slot] > 0;
                         }
                         break;
                     case OXB_AGG_AVG: {
-                        double s = __longlong_as_double((long long)a0);
-                        double c = __longlong_as_double((long long)acc[op.a1 * st + slot]);
-                        unsigned long long cnt = acc[op.a2 * st + slot];
+                        double s = as_f64(a0), c = as_f64(A[(o.arr + 1) * st + slot]);
                         double t = isfinite(s) ? __dadd_rn(s, c) : s;
-                        ((double*)O.cols[j].values)[r] = cnt ? __ddiv_rn(t, (double)cnt) : 0.0;
-                        valid = cnt > 0;
+                        ((double*)O.cols[j].values)[r] = nn ? __ddiv_rn(t, (double)nn) : 0.0;
+                        valid = nn > 0;
                         break;
                     }
                     default: {
-                        valid = acc[op.a1 * st + slot] > 0;
+                        valid = nn > 0;
                         long long k = (long long)a0;
-                        if (op.in_type == kFloat64)
+                        if (o.in_type == kFloat64)
                             ((double*)O.cols[j].values)[r] = valid ? from_total_order_key(k) : 0.0;
-                        else if (op.in_type == kInt64)
+                        else if (o.in_type == kInt64)
                             ((long long*)O.cols[j].values)[r] = valid ? k : 0;
                         else
                             ((int*)O.cols[j].values)[r] = valid ? (int)k : 0;
@@ -442,9 +2030,9 @@ __global__ void agg_emit_kernel(AggProgram P, AggOutput O, const unsigned long l
     }
 }
 
-// Distinct keys among a strided sample of rows (an estimate of the table size).
-__global__ void agg_sample_kernel(AggKey key, long long n, long long samples, long long* __restrict__ table,
-                                  unsigned int tcap, unsigned int* __restrict__ distinct) {
+// Distinct keys, and their range, among a strided sample of rows.
+__global__ void agg_sample_kernel(const __grid_constant__ AggKey key, long long n, long long samples, long long* __restrict__ table,
+                                  unsigned int tcap, unsigned long long* __restrict__ out /* distinct, min, max */) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < samples;
          i += (long long)gridDim.x * blockDim.x) {
         long long row = (long long)((double)i * (double)n / (double)samples);
@@ -452,12 +2040,14 @@ __global__ void agg_sample_kernel(AggKey key, long long n, long long samples, lo
         if (!valid_at(key.validity, row)) continue;
         long long k = load_int(key.values, key.type, row);
         if (k == kEmptyKey) continue;
+        atomicMin((long long*)&out[1], k);
+        atomicMax((long long*)&out[2], k);
         unsigned int h = (unsigned int)(fmix64((unsigned long long)k) & (tcap - 1u));
         for (unsigned int p = 0; p < tcap; p++) {
             unsigned long long old =
                 atomicCAS((unsigned long long*)&table[h], (unsigned long long)kEmptyKey, (unsigned long long)k);
             if (old == (unsigned long long)kEmptyKey) {
-                atomicAdd(distinct, 1u);
+                atomicAdd(&out[0], 1ull);
                 break;
             }
             if ((long long)old == k) break;
@@ -478,9 +2068,10 @@ unsigned int next_pow2(long long v, long long floor_v) {
     return (unsigned int)c;
 }
 
-// One aggregate as the kernels run it: a column or the build side.
+// One aggregate as the kernels read it: a column of the input (side 0) or of
+// the build side (side 1); no column for COUNT(*).
 struct AggInputCol {
-    const Column* col;  // null for COUNT(*)
+    const Column* col;
     int side;
 };
 
@@ -493,7 +2084,6 @@ struct AggPlan {
 AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInputCol>& inputs, int key_type) {
     AggPlan plan;
     AggProgram& P = plan.P;
-    P.nops = (int)funcs.size();
     int na = 1;  // array 0: rows per group
     P.init[0] = kInitZero;
     P.merge[0] = kMergeAddU64;
@@ -502,53 +2092,71 @@ AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInput
         P.merge[na] = merge;
         return na++;
     };
-    for (int j = 0; j < P.nops; j++) {
-        DevAggOp& op = P.ops[j];
-        op.func = funcs[j];
+    // Accumulators are shared by every aggregate that needs the same one.
+    auto acc_for = [&](int kind, const Column* c, int side) -> int {
+        for (int j = 0; j < P.nacc; j++)
+            if (P.acc[j].kind == kind && P.acc[j].values == c->values && P.acc[j].side == side &&
+                P.acc[j].validity == c->validity && P.acc[j].in_type == c->type)
+                return P.acc[j].arr;
+        if (P.nacc == kMaxAccs) fail(OXB_UNSUPPORTED, "too many distinct aggregate inputs");
+        DevAcc& a = P.acc[P.nacc++];
+        a.values = c->values;
+        a.validity = c->validity;
+        a.kind = kind;
+        a.in_type = c->type;
+        a.side = side;
+        switch (kind) {
+            case kAccSumF64:
+                a.arr = add_array(kInitZero, kMergeAddF64Comp);
+                add_array(kInitZero, kMergeAddF64);
+                break;
+            case kAccMin: a.arr = add_array(kInitMax, kMergeMin); break;
+            case kAccMax: a.arr = add_array(kInitMin, kMergeMax); break;
+            default: a.arr = add_array(kInitZero, kMergeAddU64); break;
+        }
+        return a.arr;
+    };
+    P.nout = (int)funcs.size();
+    for (int j = 0; j < P.nout; j++) {
+        DevOut& o = P.out[j];
+        o.func = funcs[j];
         const Column* c = inputs[j].col;
-        op.side = inputs[j].side;
-        op.values = c ? c->values : nullptr;
-        op.validity = c ? c->validity : nullptr;
-        op.in_type = c ? c->type : kInt64;
-        const bool nullable = c && c->validity;
-        auto nn = [&]() { return nullable ? add_array(kInitZero, kMergeAddU64) : 0; };
+        const int side = inputs[j].side;
+        o.in_type = c ? c->type : kInt64;
+        // Rows with a non-NULL input: the group's rows when the column has no bitmap.
+        auto nn = [&]() { return c && c->validity ? acc_for(kAccCount, c, side) : 0; };
         int out_type = kInt64;
-        switch (op.func) {
+        switch (o.func) {
             case OXB_AGG_COUNT_STAR:
-                op.a0 = 0;
+                o.arr = 0;
+                o.nn = 0;
                 break;
             case OXB_AGG_COUNT:
-                op.a0 = nn();
+                o.arr = nn();
+                o.nn = 0;
                 break;
             case OXB_AGG_SUM:
-                if (op.in_type == kFloat64) {
-                    op.a0 = add_array(kInitZero, kMergeAddF64Comp);
-                    op.a1 = add_array(kInitZero, kMergeAddF64);
-                    op.a2 = nn();
-                    out_type = kFloat64;
-                } else {
-                    op.a0 = add_array(kInitZero, kMergeAddU64);
-                    op.a1 = nn();
-                }
+                o.arr = acc_for(o.in_type == kFloat64 ? kAccSumF64 : kAccSumInt, c, side);
+                o.nn = nn();
+                out_type = o.in_type == kFloat64 ? kFloat64 : kInt64;
                 break;
             case OXB_AGG_AVG:
-                op.a0 = add_array(kInitZero, kMergeAddF64Comp);
-                op.a1 = add_array(kInitZero, kMergeAddF64);
-                op.a2 = nn();
+                o.arr = acc_for(kAccSumF64, c, side);
+                o.nn = nn();
                 out_type = kFloat64;
                 break;
             case OXB_AGG_MIN:
-                op.a0 = add_array(kInitMax, kMergeMin);
-                op.a1 = nn();
-                out_type = op.in_type;
+                o.arr = acc_for(kAccMin, c, side);
+                o.nn = nn();
+                out_type = o.in_type;
                 break;
             case OXB_AGG_MAX:
-                op.a0 = add_array(kInitMin, kMergeMax);
-                op.a1 = nn();
-                out_type = op.in_type;
+                o.arr = acc_for(kAccMax, c, side);
+                o.nn = nn();
+                out_type = o.in_type;
                 break;
             default:
-                fail(OXB_PLAN, "unknown aggregate function " + std::to_string(op.func));
+                fail(OXB_PLAN, "unknown aggregate function " + std::to_string(o.func));
         }
         plan.out_types.push_back(out_type);
     }
@@ -565,58 +2173,358 @@ void check_agg_input(int func, const Column* c, int index) {
                                   std::to_string(c->type) + "; Int64, Int32 and Float64 run on the device");
 }
 
+// One compiled shape of the row-loop kernels: the accumulator bound, warp
+// combining, and rows per thread per step.  The autotuner picks among them.
+struct AggVariant {
+    int maxacc;
+    bool combine;
+    int rpt;
+    bool tile;    // the tile sort-reduce kernels (combine/rpt unused)
+    bool stream = false;  // the streamed kernels (combine/rpt unused)
+    bool stile = false;   // the streamed tile sort-reduce kernels
+};
+
+// The streamed kernels' plan: the probe-side columns (deduplicated) with
+// their places in a stage, and the slot-major CTA-table layout (Float64
+// (sum, compensation) pairs first, on even words).  False when a column
+// cannot be streamed (a base not 16-byte aligned, too many columns).
+bool plan_stream(const AggProgram& P, const DevPredicate& pred, const void* key_values, const uint8_t* key_validity,
+                 int key_type, long long n, StreamPlan* SP) {
+    *SP = StreamPlan{};
+    auto add = [&](const void* values, const uint8_t* validity, int type) -> int {
+        for (int c = 0; c < SP->ncols; c++)
+            if (SP->cols[c].values == values && SP->cols[c].validity == validity) return c;
+        if (SP->ncols == kMaxStreamCols) return -2;
+        if (((uintptr_t)values & 15) || ((uintptr_t)validity & 15)) return -2;
+        if (type != kInt64 && type != kFloat64 && type != kInt32) return -2;
+        StreamCol& c = SP->cols[SP->ncols];
+        c.values = values;
+        c.validity = validity;
+        c.type = type;
+        c.width = type_width(type, 1);
+        return SP->ncols++;
+    };
+    for (int l = 0; l < pred.nleaves; l++) {
+        SP->leaf_col[l] = add(pred.leaves[l].values, pred.leaves[l].validity, pred.leaves[l].type);
+        if (SP->leaf_col[l] < 0) return false;
+    }
+    SP->key_col = add(key_values, key_validity, key_type);
+    if (SP->key_col < 0) return false;
+    for (int j = 0; j < P.nacc; j++) {
+        SP->acc_col[j] = -1;
+        if (P.acc[j].side != 0) continue;
+        SP->acc_col[j] = add(P.acc[j].values, P.acc[j].validity, P.acc[j].in_type);
+        if (SP->acc_col[j] < 0) return false;
+    }
+    int off = 0;
+    SP->tx_bytes = 0;
+    for (int c = 0; c < SP->ncols; c++) {
+        SP->cols[c].voff = off;
+        off += kStreamT * SP->cols[c].width;
+        SP->tx_bytes += kStreamT * SP->cols[c].width + (SP->cols[c].validity ? kStreamT / 8 : 0);
+        SP->cols[c].boff = -1;
+        if (SP->cols[c].validity) {
+            SP->cols[c].boff = off;
+            off += kStreamT / 8;
+        }
+        off = (off + 127) & ~127;
+    }
+    SP->stage_bytes = off;
+    SP->n = n;
+    SP->ntiles = (n + kStreamT - 1) / kStreamT;
+    int w = 0;
+    for (int a = 0; a < P.narrays; a++)
+        if (P.merge[a] == kMergeAddF64Comp) {
+            SP->aos_idx[a] = w;
+            SP->aos_idx[a + 1] = w + 1;
+            w += 2;
+        }
+    for (int a = 0; a < P.narrays; a++) {
+        if (P.merge[a] == kMergeAddF64Comp) {
+            a++;
+            continue;
+        }
+        SP->aos_idx[a] = w++;
+    }
+    SP->aos = (w + 1) & ~1;
+    return true;
+}
+
+int maxacc_for(int nacc) { return nacc <= 2 ? 2 : (nacc <= 4 ? 4 : kMaxAccs); }
+
+using RowsKernel = void (*)(const AggProgram, const DevPredicate, const AggKey, long long);
+using JoinKernel = void (*)(const AggProgram, const DevPredicate, const AggKey, const void*, const uint8_t*, int,
+                            const JoinTableDev, long long);
+
+#define OXB_AGG_VARIANTS(X)                                                                                    \
+    X(2, false, 1) X(2, false, 2) X(2, true, 1) X(2, true, 2) X(4, false, 1) X(4, false, 2) X(4, true, 1)      \
+        X(4, true, 2) X(16, false, 1) X(16, false, 2)
+
+RowsKernel rows_kernel_for(const AggVariant& v) {
+    if (v.tile) {
+        if (v.maxacc == 2) return agg_tile_rows_kernel<2>;
+        if (v.maxacc == 4) return agg_tile_rows_kernel<4>;
+    }
+#define OXB_PICK(M, C, R) \
+    if (v.maxacc == M && v.combine == C && v.rpt == R) return agg_rows_kernel<M, C, R>;
+    OXB_AGG_VARIANTS(OXB_PICK)
+#undef OXB_PICK
+    fail(OXB_EXECUTION, "no aggregate kernel for this variant");
+}
+
+JoinKernel join_kernel_for(const AggVariant& v) {
+    if (v.tile) {
+        if (v.maxacc == 2) return agg_tile_join_kernel<2>;
+        if (v.maxacc == 4) return agg_tile_join_kernel<4>;
+    }
+#define OXB_PICK(M, C, R) \
+    if (v.maxacc == M && v.combine == C && v.rpt == R) return agg_join_kernel<M, C, R>;
+    OXB_AGG_VARIANTS(OXB_PICK)
+#undef OXB_PICK
+    fail(OXB_EXECUTION, "no join-aggregate kernel for this variant");
+}
+
+using StreamRowsKernel = void (*)(const AggProgram, const DevPredicate, const StreamPlan);
+using StreamJoinKernel = void (*)(const AggProgram, const DevPredicate, const StreamPlan, const AggKey,
+                                  const JoinTableDev);
+
+using StileKernel = void (*)(const AggProgram, const DevPredicate, const StreamPlan, const AggKey, const JoinTableDev);
+
+StileKernel stile_kernel_for(int maxacc, bool join) {
+    if (join) return maxacc == 2 ? agg_stile_kernel<2, true> : agg_stile_kernel<4, true>;
+    return maxacc == 2 ? agg_stile_kernel<2, false> : agg_stile_kernel<4, false>;
+}
+
+StreamRowsKernel stream_rows_kernel_for(int maxacc) {
+    if (maxacc == 2) return agg_stream_rows_kernel<2>;
+    if (maxacc == 4) return agg_stream_rows_kernel<4>;
+    return agg_stream_rows_kernel<kMaxAccs>;
+}
+
+StreamJoinKernel stream_join_kernel_for(int maxacc) {
+    if (maxacc == 2) return agg_stream_join_kernel<2>;
+    if (maxacc == 4) return agg_stream_join_kernel<4>;
+    return agg_stream_join_kernel<kMaxAccs>;
+}
+
+std::string variant_name(const char* base, const AggVariant& v) {
+    if (v.stile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream-tile>";
+    if (v.stream) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream>";
+    if (v.tile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",tile>";
+    return std::string(base) + "<" + std::to_string(v.maxacc) + (v.combine ? ",combine," : ",atomic,") +
+           std::to_string(v.rpt) + ">";
+}
+
+// Choices the autotuner made, per query shape, for this process.
+std::mutex g_tune_mu;
+std::map<std::string, AggVariant> g_tuned;
+
 // Runs the planned aggregation kernel(s) and emits the sorted output batch.
+// launch(P, smem, variant) launches the row-loop kernel of that variant.
 template <typename Launch>
 oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, const AggKey& key_for_sample,
-                         long long sample_rows, long long max_groups, const char* kernel_name, Launch&& launch) {
+                         long long sample_rows, long long max_groups, const char* kernel_name, const StreamPlan* SP,
+                         Launch&& launch) {
     AggProgram& P = plan.P;
-    // Size the table: a strided sample decides between a small table
-    // (keys repeat) and one that holds every row's key.
+    const int maxacc = maxacc_for(P.nacc);
+    P.scratch_accs = maxacc <= 4 ? maxacc : 0;
+
+    // Size the HBM table and the shared-memory levels from a strided sample:
+    // a small HBM table when keys repeat, room for every row otherwise; warp
+    // caches direct-mapped when the sampled keys span at most 64 keys (no
+    // CTA table then), tagged otherwise; the CTA table direct-mapped when the
+    // span fits it.  Keys outside a sampled span still fold correctly, one
+    // level further out.
     unsigned int cap;
+    long long sampled_distinct = 0;
+    unsigned long long span = ~0ull;
+    long long span_lo = 0;
     {
         long long samples = sample_rows < 8192 ? sample_rows : 8192;
-        unsigned int d = 0;
+        unsigned long long h[3] = {0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
         if (samples > 0) {
             const unsigned int tcap = 16384;
             Scratch<long long> t(s, tcap);
-            Scratch<unsigned int> dist(s, 1, true);
+            Scratch<unsigned long long> out(s, 3);
+            OXB_CUDA(cudaMemcpyAsync(out.get(), h, sizeof h, cudaMemcpyHostToDevice, s->stream));
             note_launch(), fill_i64_kernel<<<16, 256, 0, s->stream>>>(t.get(), tcap, kEmptyKey);
-            note_launch(), agg_sample_kernel<<<grid_for(b, samples, 256, 2), 256, 0, s->stream>>>(key_for_sample, sample_rows,
-                                                                                   samples, t.get(), tcap, dist.get());
+            note_launch(), agg_sample_kernel<<<grid_for(b, samples, 256, 2), 256, 0, s->stream>>>(
+                key_for_sample, sample_rows, samples, t.get(), tcap, out.get());
             OXB_CUDA(cudaGetLastError());
-            OXB_CUDA(cudaMemcpyAsync(&d, dist.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+            OXB_CUDA(cudaMemcpyAsync(h, out.get(), sizeof h, cudaMemcpyDeviceToHost, s->stream));
             OXB_CUDA(cudaStreamSynchronize(s->stream));
         }
-        long long full = max_groups < 1 ? 1 : max_groups;
-        if ((long long)d * 8 <= samples) cap = next_pow2(std::min<long long>(2 * full, 64ll * d + 4096), 4096);
+        const long long d = (long long)h[0];
+        sampled_distinct = d;
+        const long long full = max_groups < 1 ? 1 : max_groups;
+        if (d * 8 <= samples) cap = next_pow2(std::min<long long>(2 * full, 64ll * d + 4096), 4096);
         else cap = next_pow2(2 * full, 4096);
+        if (d > 0) {
+            span_lo = (long long)h[1];
+            span = (unsigned long long)(long long)h[2] - (unsigned long long)span_lo;
+        }
     }
-    // Private table size: as many slots as fit in 48 KB (power of two, <= 2048).
-    const long long per_slot = 8ll * (1 + P.narrays);
-    int S = 2048;
-    while (S > 0 && S * per_slot + 16 > 48 * 1024) S >>= 1;
-    if (S < 64) S = 0;
-    P.smem_slots = S;
-    const size_t smem = S ? (size_t)S * per_slot + 16 : 0;
+    // A base below the sampled minimum, leaving `room` slots of margin, that
+    // does not wrap below the int64 range.
+    auto direct_base = [&](int slots) {
+        long long margin = (long long)(((unsigned long long)slots - 1 - span) / 2);
+        return span_lo < LLONG_MIN + slots ? span_lo : span_lo - margin;
+    };
+    const size_t kBudget = 64 * 1024;
+    // Shared-memory layout of the row-loop kernels (warp caches + CTA table)
+    // and of the tile sort-reduce kernels (a bigger CTA table, no caches).
+    struct SmemPlan {
+        int S = 0, Sw = 0, direct = 0, wdirect = 0;
+        long long direct_lo = 0, wdirect_lo = 0;
+        size_t bytes = 0;
+    };
+    SmemPlan cp, tp;
+    if (P.scratch_accs == 0) {
+        // no combining, so no warp caches: the CTA table and HBM only
+        for (cp.S = 2048; cp.S >= 64 && smem_bytes(cp.S, 0, P.narrays, 0) > kBudget; cp.S >>= 1) {
+        }
+    } else if (span < 64) {
+        cp.Sw = 2;
+        while ((unsigned long long)cp.Sw <= span) cp.Sw <<= 1;
+        cp.wdirect = 1;
+        cp.wdirect_lo = direct_base(cp.Sw);
+    } else {
+        for (cp.Sw = 64; cp.Sw > 8 && smem_bytes(0, cp.Sw, P.narrays, P.scratch_accs) > kBudget / 3; cp.Sw >>= 1) {
+        }
+        for (cp.S = 2048; cp.S >= 64 && smem_bytes(cp.S, cp.Sw, P.narrays, P.scratch_accs) > kBudget; cp.S >>= 1) {
+        }
+    }
+    if (cp.S < 64) cp.S = 0;
+    if (cp.S > 0 && span < (unsigned long long)cp.S) {
+        cp.direct = 1;
+        cp.direct_lo = direct_base(cp.S);
+    }
+    cp.bytes = smem_bytes(cp.S, cp.Sw, P.narrays, P.scratch_accs);
+    if (maxacc <= 4) {
+        for (tp.S = 2048; tp.S >= 64 && tile_smem_bytes(tp.S, P.narrays, maxacc) > kBudget; tp.S >>= 1) {
+        }
+        if (tp.S < 64) tp.S = 0;
+        if (tp.S > 0 && span < (unsigned long long)tp.S) {
+            tp.direct = 1;
+            tp.direct_lo = direct_base(tp.S);
+        }
+        tp.bytes = tile_smem_bytes(tp.S, P.narrays, maxacc);
+    }
+    SmemPlan sp, stp;
+    if (SP && SP->n >= 4ll * kStreamT && maxacc <= 4) {
+        for (stp.S = 2048; stp.S >= 64 && stile_smem_bytes(stp.S, SP->stage_bytes, P.narrays, maxacc) > 110 * 1024;
+             stp.S >>= 1) {
+        }
+        if (stp.S < 64) stp.S = 0;
+        if (stp.S > 0 && span < (unsigned long long)stp.S) {
+            stp.direct = 1;
+            stp.direct_lo = direct_base(stp.S);
+        }
+        stp.bytes = stile_smem_bytes(stp.S, SP->stage_bytes, P.narrays, maxacc);
+    }
+    if (SP && SP->n >= 4ll * kStreamT) {
+        for (sp.S = 2048; sp.S >= 64 && stream_smem_bytes(sp.S, SP->stage_bytes, SP->aos) > 110 * 1024; sp.S >>= 1) {
+        }
+        if (sp.S < 64) sp.S = 0;
+        if (sp.S > 0 && span < (unsigned long long)sp.S) {
+            sp.direct = 1;
+            sp.direct_lo = direct_base(sp.S);
+        }
+        sp.bytes = stream_smem_bytes(sp.S, SP->stage_bytes, SP->aos);
+    }
+    auto configure = [&](const AggVariant& v) {
+        const SmemPlan& p = v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp));
+        P.smem_slots = p.S;
+        P.wslots = p.Sw;
+        P.direct = p.direct;
+        P.direct_lo = p.direct_lo;
+        P.wdirect = p.wdirect;
+        P.wdirect_lo = p.wdirect_lo;
+        return p.bytes;
+    };
+
+    // The variant: the tuned one for this shape, else the default; the
+    // autotuner (when on) times every candidate on this call's data once.
+    // Warp caches need combining; without a CTA table the atomic-only path
+    // would send every row to HBM, so it is no candidate then either.
+    std::vector<AggVariant> candidates;
+    if (stp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, false, true});
+    if (sp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, true});
+    if (tp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, true});
+    for (int c = 0; c < (maxacc <= 4 ? 2 : 1); c++) {
+        if (c == 0 && maxacc <= 4 && cp.S == 0) continue;
+        for (int r = 1; r <= 2; r++) candidates.push_back(AggVariant{maxacc, c == 1, r, false});
+    }
+    const int S = tp.S > 0 ? tp.S : cp.S;
+    int cap_class = 0;
+    while ((1u << cap_class) < cap) cap_class++;
+    const std::string shape = std::string(kernel_name) + "/" + std::to_string(maxacc) + "/" +
+                              std::to_string(cp.wdirect) + std::to_string(cp.direct) + std::to_string(tp.direct) + "/" +
+                              std::to_string(sampled_distinct * 8 <= 8192) + "/" + std::to_string(cap_class);
+    AggVariant chosen{maxacc, maxacc <= 4, 2, tp.S > 0 && sp.S == 0, sp.S > 0 && stp.S == 0, stp.S > 0};
+    bool tune = false;
+    if (b.force_combine >= 0 || b.force_rpt > 0) {
+        if (b.force_combine >= 0) {
+            chosen.stile = b.force_combine == 4 && stp.S > 0;
+            chosen.stream = b.force_combine == 3 && sp.S > 0;
+            chosen.tile = b.force_combine == 2 && tp.S > 0;
+            chosen.combine = b.force_combine == 1 && maxacc <= 4;
+        }
+        if (b.force_rpt > 0) chosen.rpt = b.force_rpt;
+    } else {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(shape);
+        if (it != g_tuned.end()) chosen = it->second;
+        else tune = b.autotune;
+    }
 
     for (int attempt = 0; attempt < 2; attempt++) {
         P.capacity = cap;
         P.stride = (long long)cap + 2;
         AllocRef keys_mem = dev_alloc(s, (size_t)cap * 8, false);
-        AllocRef acc_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
+        AllocRef arr_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
         Scratch<unsigned int> status(s, 1, true);
         Scratch<unsigned long long> fill(s, 1, true);
         P.keys = (long long*)keys_mem->ptr;
-        P.acc = (unsigned long long*)acc_mem->ptr;
+        P.arr = (unsigned long long*)arr_mem->ptr;
         P.status = status.get();
         P.fill = fill.get();
         P.fill_limit = (unsigned long long)cap / 4 * 3;
-        note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(P);
-        OXB_CUDA(cudaGetLastError());
+        auto init = [&]() {
+            OXB_CUDA(cudaMemsetAsync(status.get(), 0, 4, s->stream));
+            OXB_CUDA(cudaMemsetAsync(fill.get(), 0, 8, s->stream));
+            note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(P);
+            OXB_CUDA(cudaGetLastError());
+        };
+        if (tune && attempt == 0) {
+            float best = 1e30f;
+            for (const AggVariant& v : candidates) {
+                init();
+                cudaEvent_t e0, e1;
+                OXB_CUDA(cudaEventCreate(&e0));
+                OXB_CUDA(cudaEventCreate(&e1));
+                OXB_CUDA(cudaEventRecord(e0, s->stream));
+                launch(P, configure(v), v);
+                OXB_CUDA(cudaEventRecord(e1, s->stream));
+                OXB_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.0f;
+                OXB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (ms < best) {
+                    best = ms;
+                    chosen = v;
+                }
+            }
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tuned[shape] = chosen;
+        }
+        init();
         {
-            KernelTimer timer(b, s, kernel_name);
+            const std::string name = variant_name(kernel_name, chosen);
+            KernelTimer timer(b, s, name.c_str());
             timer.begin();
-            launch(P, smem);
+            launch(P, configure(chosen), chosen);
             timer.end();
         }
         OXB_CUDA(cudaGetLastError());
@@ -637,7 +2545,7 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         } h{};
         OXB_CUDA(cudaMemcpyAsync(&h.G, pos.get() + m, 8, cudaMemcpyDeviceToHost, s->stream));
         OXB_CUDA(cudaMemcpyAsync(&h.lo, range.get(), 16, cudaMemcpyDeviceToHost, s->stream));
-        OXB_CUDA(cudaMemcpyAsync(&h.null_rows, P.acc + cap, 8, cudaMemcpyDeviceToHost, s->stream));
+        OXB_CUDA(cudaMemcpyAsync(&h.null_rows, P.arr + cap, 8, cudaMemcpyDeviceToHost, s->stream));
         OXB_CUDA(cudaMemcpyAsync(&h.status, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
         OXB_CUDA(cudaStreamSynchronize(s->stream));
         if ((h.status & kStatusTableFull) && attempt == 0) {
@@ -654,7 +2562,7 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         unsigned long long lo = G > 0 ? h.lo : 0;
         if (G > 0) {
             note_launch(), agg_compact_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), pos.get(), lo,
-                                                                               skeys.get(), sslots.get());
+                                                                                            skeys.get(), sslots.get());
             OXB_CUDA(cudaGetLastError());
             unsigned long long span = h.hi - h.lo;
             int bits = 0;
@@ -682,21 +2590,36 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         };
         out->cols.push_back(make_col(plan.key_type, has_null));
         O.key = OutCol{out->cols[0].values, (unsigned int*)out->cols[0].validity};
-        for (int j = 0; j < P.nops; j++) {
-            const int f = P.ops[j].func;
+        for (int j = 0; j < P.nout; j++) {
+            const int f = P.out[j].func;
             const bool nullable = !(f == OXB_AGG_COUNT || f == OXB_AGG_COUNT_STAR);
             out->cols.push_back(make_col(plan.out_types[j], nullable));
             O.cols[j] = OutCol{out->cols.back().values, (unsigned int*)out->cols.back().validity};
         }
         if (rows > 0) {
-            note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, skeys.get(), sslots.get(), lo, G,
-                                                                               rows);
+            note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, skeys.get(), sslots.get(),
+                                                                                            lo, G, rows);
             OXB_CUDA(cudaGetLastError());
             OXB_CUDA(cudaStreamSynchronize(s->stream));
         }
         return out.release();
     }
     fail(OXB_TABLE_FULL, "aggregate hash table full after a retry");
+}
+
+template <typename K>
+void set_smem(K kernel, size_t smem) {
+    if (smem > 48 * 1024) OXB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
+// As many CTAs as fit on the GPU at once (the row loops are grid-strided),
+// fewer when there is less work.
+template <typename K>
+int resident_grid(const Backend& b, K kernel, size_t smem, long long work) {
+    int per_sm = 0;
+    OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    return grid_for(b, work, kThreads, per_sm);
 }
 
 }  // namespace
@@ -713,7 +2636,7 @@ oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_a
     if (key.type != kInt64 && key.type != kInt32)
         fail(OXB_UNSUPPORTED, "group key column " + std::to_string(spec.group_by) + " has type " +
                                   std::to_string(key.type) + "; Int64 and Int32 run on the device");
-    if (spec.naggregates < 0 || spec.naggregates > kMaxOps) fail(OXB_UNSUPPORTED, "too many aggregates");
+    if (spec.naggregates < 0 || spec.naggregates > kMaxOuts) fail(OXB_UNSUPPORTED, "too many aggregates");
     std::vector<int> funcs;
     std::vector<AggInputCol> inputs;
     for (int j = 0; j < spec.naggregates; j++) {
@@ -732,11 +2655,32 @@ oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_a
     AggPlan plan = plan_aggregate(funcs, inputs, key.type);
     const long long n = in.rows;
     AggKey k{key.values, key.validity, key.type, 0};
-    return run_aggregate(s, b, plan, k, n, n, "agg_rows_kernel", [&](AggProgram& P, size_t smem) {
+    StreamPlan SP;
+    const bool streamable = plan_stream(plan.P, pred, key.values, key.validity, key.type, n, &SP);
+    return run_aggregate(s, b, plan, k, n, n, "agg_rows_kernel", streamable ? &SP : nullptr,
+                         [&](AggProgram& P, size_t smem, const AggVariant& v) {
         if (n == 0) return;
-        if (smem > 48 * 1024)
-            OXB_CUDA(cudaFuncSetAttribute(agg_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        note_launch(), agg_rows_kernel<<<grid_for(b, n, kThreads, 4), kThreads, smem, s->stream>>>(P, pred, k, n);
+        if (v.stile) {
+            StileKernel kern = stile_kernel_for(v.maxacc, false);
+            set_smem(kern, smem);
+            int per_sm = 0;
+            OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
+            const long long grid = std::min<long long>(SP.ntiles, (long long)b.sms * std::max(per_sm, 1));
+            note_launch(), kern<<<(unsigned)grid, kStreamThreads, smem, s->stream>>>(P, pred, SP, k, JoinTableDev{});
+            return;
+        }
+        if (v.stream) {
+            StreamRowsKernel kern = stream_rows_kernel_for(v.maxacc);
+            set_smem(kern, smem);
+            int per_sm = 0;
+            OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
+            const long long grid = std::min<long long>(SP.ntiles, (long long)b.sms * std::max(per_sm, 1));
+            note_launch(), kern<<<(unsigned)grid, kStreamThreads, smem, s->stream>>>(P, pred, SP);
+            return;
+        }
+        RowsKernel kern = rows_kernel_for(v);
+        set_smem(kern, smem);
+        note_launch(), kern<<<resident_grid(b, kern, smem, (n + v.rpt - 1) / v.rpt), kThreads, smem, s->stream>>>(P, pred, k, n);
     });
 }
 
@@ -751,14 +2695,14 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
     const Column& pk = probe.cols[a.probe_key];
     if (pk.type != kInt64 && pk.type != kInt32) fail(OXB_UNSUPPORTED, "probe join key must be Int64 or Int32");
     auto side_col = [&](int side, int col) -> const Column* {
-        const oxb_batch& bt = side ? build : probe;
         if (side != 0 && side != 1) fail(OXB_PLAN, "side must be 0 (probe) or 1 (build)");
+        const oxb_batch& bt = side ? build : probe;
         if (col < 0 || col >= (int)bt.cols.size()) fail(OXB_PLAN, "column index " + std::to_string(col) + " out of range");
         return &bt.cols[col];
     };
     const Column* gk = side_col(a.group_side, a.group_column);
     if (gk->type != kInt64 && gk->type != kInt32) fail(OXB_UNSUPPORTED, "group key must be Int64 or Int32");
-    if (a.naggregates < 0 || a.naggregates > kMaxOps) fail(OXB_UNSUPPORTED, "too many aggregates");
+    if (a.naggregates < 0 || a.naggregates > kMaxOuts) fail(OXB_UNSUPPORTED, "too many aggregates");
     std::vector<int> funcs;
     std::vector<AggInputCol> inputs;
     for (int j = 0; j < a.naggregates; j++) {
@@ -774,16 +2718,36 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
     // The groups are at most the distinct group keys of the side they come
     // from; the sample is taken over that side's column.
     const long long group_rows = a.group_side ? build.rows : probe.rows;
-    const long long max_groups = a.group_side ? build.rows : probe.rows;
     AggKey sample_key{gk->values, gk->validity, gk->type, 0};
     const JoinTableDev jt = a.table->t;
-    return run_aggregate(s, b, plan, sample_key, group_rows, max_groups, "agg_join_kernel", [&](AggProgram& P, size_t smem) {
-        if (n == 0) return;
-        if (smem > 48 * 1024)
-            OXB_CUDA(cudaFuncSetAttribute(agg_join_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        note_launch(), agg_join_kernel<<<grid_for(b, n, kThreads, 4), kThreads, smem, s->stream>>>(P, pred, k, pk.values, pk.validity,
-                                                                                    pk.type, jt, n);
-    });
+    StreamPlan SP;
+    const bool streamable = plan_stream(plan.P, pred, pk.values, pk.validity, pk.type, n, &SP);
+    return run_aggregate(s, b, plan, sample_key, group_rows, group_rows, "agg_join_kernel", streamable ? &SP : nullptr,
+                         [&](AggProgram& P, size_t smem, const AggVariant& v) {
+                             if (n == 0) return;
+                             if (v.stile) {
+                                 StileKernel kern = stile_kernel_for(v.maxacc, true);
+                                 set_smem(kern, smem);
+                                 int per_sm = 0;
+                                 OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
+                                 const long long grid = std::min<long long>(SP.ntiles, (long long)b.sms * std::max(per_sm, 1));
+                                 note_launch(), kern<<<(unsigned)grid, kStreamThreads, smem, s->stream>>>(P, pred, SP, k, jt);
+                                 return;
+                             }
+                             if (v.stream) {
+                                 StreamJoinKernel kern = stream_join_kernel_for(v.maxacc);
+                                 set_smem(kern, smem);
+                                 int per_sm = 0;
+                                 OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads, smem));
+                                 const long long grid = std::min<long long>(SP.ntiles, (long long)b.sms * std::max(per_sm, 1));
+                                 note_launch(), kern<<<(unsigned)grid, kStreamThreads, smem, s->stream>>>(P, pred, SP, k, jt);
+                                 return;
+                             }
+                             JoinKernel kern = join_kernel_for(v);
+                             set_smem(kern, smem);
+                             note_launch(), kern<<<resident_grid(b, kern, smem, (n + v.rpt - 1) / v.rpt), kThreads, smem,
+                                                   s->stream>>>(P, pred, k, pk.values, pk.validity, pk.type, jt, n);
+                         });
 }
 
 }  // namespace oxb

@@ -508,6 +508,24 @@ oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_t name_l
 
 uint64_t oxb_kernel_launches(void) { return g_launches.load(); }
 
+oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread) {
+    OXB_TRY
+    if (!backend) fail(OXB_PLAN, "backend is null");
+    if (combine < -1 || combine > 4) fail(OXB_PLAN, "combine must be -1 or 0..4");
+    if (rows_per_thread != 0 && rows_per_thread != 1 && rows_per_thread != 2)
+        fail(OXB_UNSUPPORTED, "rows per thread must be 0 (automatic), 1 or 2");
+    backend->b.force_combine = combine;
+    backend->b.force_rpt = rows_per_thread;
+    OXB_CATCH
+}
+
+oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled) {
+    OXB_TRY
+    if (!backend) fail(OXB_PLAN, "backend is null");
+    backend->b.autotune = enabled != 0;
+    OXB_CATCH
+}
+
 int32_t oxb_supports_hash_join(const oxb_backend* backend) {
     (void)backend;
     return 1;

@@ -34,7 +34,7 @@ struct DevProjection {
     DevProjCol cols[kMaxProj];
 };
 
-__global__ void __launch_bounds__(kThreads) filter_mask_kernel(DevPredicate pred, long long n,
+__global__ void __launch_bounds__(kThreads) filter_mask_kernel(const __grid_constant__ DevPredicate pred, long long n,
                                                                unsigned int* __restrict__ mask,
                                                                unsigned int* __restrict__ tile_counts,
                                                                long long ntiles) {
@@ -91,7 +91,7 @@ __device__ __forceinline__ void or_bits(unsigned int* words, unsigned long long 
 
 __global__ void __launch_bounds__(kThreads) filter_gather_kernel(
     const unsigned int* __restrict__ mask, const unsigned long long* __restrict__ tile_off, long long n,
-    long long ntiles, DevProjection proj) {
+    long long ntiles, const __grid_constant__ DevProjection proj) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long nwords = (n + 31) / 32;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {

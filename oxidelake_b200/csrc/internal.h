@@ -72,7 +72,10 @@ struct Backend {
     int sms = 148;
     size_t smem_optin = 0;
     std::string name;
-    bool timing = false;  // oxb_set_kernel_timing
+    bool timing = false;    // oxb_set_kernel_timing
+    bool autotune = false;  // oxb_set_autotune
+    int force_combine = -1;  // oxb_set_agg_variant: -1 = tuned/default
+    int force_rpt = 0;
 };
 
 // Counts every kernel this library launches (oxb_kernel_launches).
@@ -143,6 +146,10 @@ struct JoinSlot {
 struct JoinTableDev {
     JoinSlot* slots = nullptr;  // capacity slots
     unsigned int capacity = 0;  // power of two
+    // rows[start] of each slot's run, beside the slots: indexed by the same
+    // slot number, so a probe loads it in parallel with the slot and a
+    // unique key needs no second dependent load to find its build row.
+    unsigned int* first_row = nullptr;  // capacity + 1 entries
     unsigned int* rows = nullptr;
     long long nrows = 0;
     long long ndistinct = 0;

@@ -22,9 +22,10 @@ __device__ __forceinline__ long long join_key_at(const void* v, int type, long l
 
 // Places run r at its key's slot; a key equal to kEmptyKey goes to the side
 // slot at index `capacity`.
-__global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int capacity,
-                                   const long long* __restrict__ keys, const unsigned int* __restrict__ starts,
-                                   const unsigned int* __restrict__ counts, long long nruns,
+__global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int* __restrict__ first_row,
+                                   unsigned int capacity, const long long* __restrict__ keys,
+                                   const unsigned int* __restrict__ starts, const unsigned int* __restrict__ counts,
+                                   long long nruns, const unsigned int* __restrict__ rows,
                                    unsigned int* __restrict__ status) {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nruns;
          r += (long long)gridDim.x * blockDim.x) {
@@ -32,6 +33,7 @@ __global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int ca
         if (key == kEmptyKey) {
             slots[capacity].start = starts[r];
             slots[capacity].count = counts[r];
+            first_row[capacity] = rows[starts[r]];
             continue;
         }
         unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (capacity - 1u));
@@ -42,6 +44,7 @@ __global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int ca
             if (old == (unsigned long long)kEmptyKey || old == (unsigned long long)key) {
                 slots[s].start = starts[r];
                 slots[s].count = counts[r];
+                first_row[s] = rows[starts[r]];
                 placed = true;
                 break;
             }
@@ -124,7 +127,7 @@ __device__ __forceinline__ bool join_lookup(const JoinTableDev& t, long long key
     return false;
 }
 
-__global__ void join_probe_kernel(JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid,
+__global__ void join_probe_kernel(const __grid_constant__ JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid,
                                   int type, long long n, unsigned int* __restrict__ counts,
                                   unsigned int* __restrict__ starts) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -155,7 +158,7 @@ struct DevGather {
 __global__ void join_gather_kernel(const unsigned long long* __restrict__ offsets,
                                    const unsigned int* __restrict__ starts, long long nprobe,
                                    const unsigned int* __restrict__ trows, long long ntrows,
-                                   long long right_rows, unsigned long long first, long long rows, DevGather g,
+                                   long long right_rows, unsigned long long first, long long rows, const __grid_constant__ DevGather g,
                                    unsigned int* __restrict__ status) {
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -329,12 +332,13 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
 
     t.ndistinct = nruns;
     t.capacity = pow2_capacity(nruns);
-    out->slots_mem = dev_alloc(s, (size_t)(t.capacity + 1) * sizeof(JoinSlot), false);
+    out->slots_mem = dev_alloc(s, (size_t)(t.capacity + 1) * (sizeof(JoinSlot) + 4), false);
     t.slots = (JoinSlot*)out->slots_mem->ptr;
+    t.first_row = (unsigned int*)(t.slots + t.capacity + 1);
     note_launch(), join_init_slots_kernel<<<grid_for(b, t.capacity + 1, 256, 8), 256, 0, s->stream>>>(t.slots, t.capacity + 1);
     if (nruns > 0)
         note_launch(), join_insert_kernel<<<grid_for(b, nruns, 256, 8), 256, 0, s->stream>>>(
-            t.slots, t.capacity, rkeys.get(), rstart.get(), rcount.get(), nruns, status.get());
+            t.slots, t.first_row, t.capacity, rkeys.get(), rstart.get(), rcount.get(), nruns, t.rows, status.get());
     OXB_CUDA(cudaGetLastError());
     uint32_t st = 0;
     OXB_CUDA(cudaMemcpyAsync(&st, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
