@@ -220,6 +220,40 @@ typedef struct oxb_filter_project_args {
 OXB_API oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream,
                               const oxb_filter_project_args* args, oxb_batch** out);
 
+/* No counterpart in the reference: oxb_filter_project that allocates
+ * nothing, neither device nor pinned memory.
+ *
+ * Why: some callers must not allocate per call.  An executor that admitted
+ * a query against a fixed device-memory budget and reserved its output
+ * buffers up front cannot let an operator take more memory in the middle of
+ * the pipeline, where the allocation could fail or push the device past the
+ * budget the admission promised; and a caller that manages its own buffer
+ * pool wants the call's footprint known before the call, not drawn from the
+ * stream-ordered pool behind its back.
+ *
+ * Output: projected column i goes to out_values[i] (device memory, room for
+ * `capacity` rows of that column's width, 8-byte aligned for 8-byte and
+ * wider rows, else 4-byte) and, when the source column has a validity
+ * bitmap, to out_validity[i] (device memory, ceil(capacity / 32) 32-bit
+ * words, LSB-first; this call clears the words it uses).  *out_rows receives
+ * the selected row count; when it exceeds `capacity` the call writes no
+ * output and returns OXB_EXECUTION, with *out_rows still set.
+ *
+ * Limit: at most OXB_NOALLOC_MAX_ROWS input rows (OXB_UNSUPPORTED beyond).
+ * The mask, tile counts, tile offsets and scan partials live in one static
+ * device array of about 2.2 MiB per device.  The first call on each device
+ * looks that array's address up with cudaGetSymbolAddress (which can load
+ * the module); make that first call before any stream capture begins.
+ * Calls whose work overlaps on one device (other streams, other threads)
+ * race on that array: the caller serialises them.  The call synchronizes
+ * `stream` once (to read the selected count) and returns with the gather
+ * still queued on it. */
+#define OXB_NOALLOC_MAX_ROWS (1 << 24)
+OXB_API oxb_status oxb_filter_project_noalloc(oxb_backend* backend, oxb_stream* stream,
+                                              const oxb_filter_project_args* args, void* const* out_values,
+                                              uint32_t* const* out_validity, int64_t capacity,
+                                              int64_t* out_rows);
+
 /* The host's index of a build side (cpu::kernels::JoinTable::runs and
  * row_indices, cpu/kernels.rs:245-255): `ndistinct` runs (key, start,
  * count) into `rows`, which groups the build rows with a non-NULL key by

@@ -15,6 +15,7 @@ LIB_PATH = Path(os.environ.get("OXB200_LIB", Path(__file__).resolve().parent / "
 
 OXB_MAX_AGGREGATES = 16
 OXB_MAX_PREDICATE_LEAVES = 64
+OXB_NOALLOC_MAX_ROWS = 1 << 24
 
 TYPE_INT64, TYPE_FLOAT64, TYPE_INT32, TYPE_FLOAT32, TYPE_VECTOR_F32 = 1, 2, 3, 4, 5
 
@@ -190,6 +191,10 @@ PROTOTYPES = {
     "oxb_download_column": (_S, [_P, _P, _P, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "oxb_batch_free": (None, [_P]),
     "oxb_filter_project": (_S, [_P, _P, C.POINTER(FilterProjectArgs), _PP]),
+    "oxb_filter_project_noalloc": (
+        _S,
+        [_P, _P, C.POINTER(FilterProjectArgs), _PP, _PP, C.c_int64, C.POINTER(C.c_int64)],
+    ),
     "oxb_prepare_join_build": (_S, [_P, _P, C.POINTER(JoinBuildArgs), _PP]),
     "oxb_join_table_distinct_keys": (C.c_int64, [_P]),
     "oxb_join_table_rows": (C.c_int64, [_P]),

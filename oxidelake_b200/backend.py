@@ -317,6 +317,34 @@ class CudaBackend:
                 raise Plan(f"projection index {p} out of range")
         return DeviceBatch(h.value, pa.schema([input.schema.field(p) for p in projection]))
 
+    def filter_project_noalloc(
+        self,
+        stream: DeviceStream,
+        input: DeviceBatch,
+        predicate: Optional[Predicate],
+        projection: Sequence[int],
+        out_values: Sequence[int],
+        out_validity: Sequence[Optional[int]],
+        capacity: int,
+    ) -> int:
+        """filter_project into caller-owned device buffers (addresses in
+        out_values / out_validity, one per projected column), allocating
+        nothing; returns the selected row count.  No reference counterpart:
+        the C header states the buffer sizes, the row limit and the
+        sharing rule."""
+        lv, nl = _leaf_array(predicate)
+        proj = _i32_array(projection)
+        a = _abi.FilterProjectArgs(input.handle, lv, nl, proj, len(projection))
+        vals = (C.c_void_p * max(1, len(projection)))(*[C.c_void_p(v) for v in out_values])
+        valid = (C.c_void_p * max(1, len(projection)))(*[C.c_void_p(v or 0) for v in out_validity])
+        rows = C.c_int64(0)
+        status = _L().oxb_filter_project_noalloc(
+            self.handle, stream.handle, C.byref(a), vals, valid, capacity, C.byref(rows)
+        )
+        self.last_noalloc_rows = rows.value
+        _abi.check(status)
+        return rows.value
+
     def prepare_join_build(
         self, stream: DeviceStream, build: DeviceBatch, key: int, index=None
     ) -> DeviceJoinTable:

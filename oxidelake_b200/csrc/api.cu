@@ -418,6 +418,23 @@ oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream, const ox
     OXB_CATCH
 }
 
+oxb_status oxb_filter_project_noalloc(oxb_backend* backend, oxb_stream* stream, const oxb_filter_project_args* args,
+                                      void* const* out_values, uint32_t* const* out_validity, int64_t capacity,
+                                      int64_t* out_rows) {
+    OXB_TRY
+    use_device(backend);
+    if (!args) fail(OXB_PLAN, "null argument");
+    long long rows = 0;
+    try {
+        filter_project_noalloc(stream_of(stream), backend->b, *args, out_values, out_validity, capacity, &rows);
+    } catch (...) {
+        if (out_rows) *out_rows = rows;
+        throw;
+    }
+    if (out_rows) *out_rows = rows;
+    OXB_CATCH
+}
+
 oxb_status oxb_prepare_join_build(oxb_backend* backend, oxb_stream* stream, const oxb_join_build_args* args,
                                   oxb_join_table** out) {
     OXB_TRY

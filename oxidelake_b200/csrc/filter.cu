@@ -244,4 +244,112 @@ oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter
     return out.release();
 }
 
+// ---- filter + projection into caller buffers, with static scratch ----------
+//
+// The same three steps as filter_project, but nothing is allocated: the
+// mask, the tile counts, the tile offsets and the scan's block partials live
+// in one file-scope device array sized for OXB_NOALLOC_MAX_ROWS input rows,
+// and the output goes to buffers the caller owns.  Every scratch word that
+// is read is written first by this call (the mask and tile counts for every
+// tile of the input, the offsets and partials by the scan), so only the
+// output validity bitmaps, which the gather ORs into, are cleared.  There is
+// one array per device: calls whose work overlaps on one device race on it.
+
+namespace {
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr long long kNoAllocRows = OXB_NOALLOC_MAX_ROWS;
+constexpr long long kNoAllocTiles = kNoAllocRows / kTileRows;
+constexpr size_t kNaMaskOff = 0;
+constexpr size_t kNaCountsOff = align256(kNaMaskOff + (size_t)kNoAllocRows / 32 * 4);
+constexpr size_t kNaOffsOff = align256(kNaCountsOff + (size_t)kNoAllocTiles * 4);
+constexpr size_t kNaPartialsOff = align256(kNaOffsOff + (size_t)(kNoAllocTiles + 1) * 8);
+constexpr long long kNaPartials = 32;
+constexpr size_t kNaScratchBytes = align256(kNaPartialsOff + (size_t)kNaPartials * 8);
+static_assert(kNoAllocRows % kTileRows == 0, "the row limit is a whole number of tiles");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaScratchBytes];
+
+constexpr int kMaxDevices = 64;
+
+// The scratch array's address on `device` (the current device), looked up
+// once per device.
+unsigned char* noalloc_scratch(int device) {
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) fail(OXB_UNSUPPORTED, "device ordinal beyond 63");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[device]) OXB_CUDA(cudaGetSymbolAddress(&addr[device], g_noalloc_scratch));
+    return (unsigned char*)addr[device];
+}
+
+}  // namespace
+
+void filter_project_noalloc(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a,
+                            void* const* out_values, uint32_t* const* out_validity, long long capacity,
+                            long long* out_rows) {
+    if (!a.input) fail(OXB_PLAN, "filter_project_noalloc: input batch is null");
+    const oxb_batch& in = *a.input;
+    DevPredicate pred = make_predicate(in, a.leaves, a.nleaves);
+    if (a.nprojection < 0 || a.nprojection > kMaxProj)
+        fail(OXB_UNSUPPORTED, "projection of more than 64 columns");
+    if (a.nprojection > 0 && !a.projection) fail(OXB_PLAN, "projection pointer is null");
+    for (int i = 0; i < a.nprojection; i++)
+        if (a.projection[i] < 0 || a.projection[i] >= (int)in.cols.size())
+            fail(OXB_PLAN, "projection index " + std::to_string(a.projection[i]) + " out of range");
+    const long long n = in.rows;
+    if (n > kNoAllocRows)
+        fail(OXB_UNSUPPORTED, "filter_project_noalloc takes at most " + std::to_string(kNoAllocRows) +
+                                  " input rows; the batch has " + std::to_string(n));
+    if (capacity < 0) fail(OXB_PLAN, "negative output capacity");
+    if (capacity > 0 && a.nprojection > 0 && !out_values) fail(OXB_PLAN, "output values array is null");
+    for (int i = 0; i < a.nprojection && capacity > 0; i++) {
+        const Column& src = in.cols[a.projection[i]];
+        const size_t align = src.width() >= 8 ? 8 : 4;
+        if (!out_values[i] || ((uintptr_t)out_values[i] % align))
+            fail(OXB_PLAN, "output values buffer " + std::to_string(i) + " is null or not " +
+                               std::to_string(align) + "-byte aligned");
+        if (src.validity && (!out_validity || !out_validity[i] || ((uintptr_t)out_validity[i] & 3)))
+            fail(OXB_PLAN, "projected column " + std::to_string(i) +
+                               " has a validity bitmap: its output bitmap must be a 4-byte aligned buffer");
+    }
+
+    const long long ntiles = (n + kTileRows - 1) / kTileRows;
+    unsigned long long total = 0;
+    unsigned char* scratch = nullptr;
+    if (n > 0) {
+        scratch = noalloc_scratch(b.device);
+        unsigned int* mask = (unsigned int*)(scratch + kNaMaskOff);
+        unsigned int* tile_counts = (unsigned int*)(scratch + kNaCountsOff);
+        unsigned long long* tile_off = (unsigned long long*)(scratch + kNaOffsOff);
+        unsigned long long* partials = (unsigned long long*)(scratch + kNaPartialsOff);
+        if (scan_partials_needed(ntiles) > kNaPartials) fail(OXB_EXECUTION, "scan partials exceed the static scratch");
+        int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+        note_launch(), filter_mask_kernel<<<grid, kThreads, 0, s->stream>>>(pred, n, mask, tile_counts, ntiles);
+        OXB_CUDA(cudaGetLastError());
+        scan_u32_to_u64_into(s, tile_counts, tile_off, ntiles, partials);
+        OXB_CUDA(cudaMemcpyAsync(&total, tile_off + ntiles, sizeof total, cudaMemcpyDeviceToHost, s->stream));
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    if (out_rows) *out_rows = (long long)total;
+    if ((long long)total > capacity)
+        fail(OXB_EXECUTION, "the selection has " + std::to_string(total) + " rows but the output buffers hold " +
+                                std::to_string(capacity));
+    if (total == 0 || a.nprojection == 0) return;
+
+    DevProjection proj{};
+    proj.ncols = a.nprojection;
+    for (int i = 0; i < a.nprojection; i++) {
+        const Column& src = in.cols[a.projection[i]];
+        unsigned int* dv = src.validity ? (unsigned int*)out_validity[i] : nullptr;
+        if (dv) OXB_CUDA(cudaMemsetAsync(dv, 0, ((total + 31) / 32) * 4, s->stream));
+        proj.cols[i] = DevProjCol{src.values, src.validity, out_values[i], dv, src.width()};
+    }
+    const unsigned int* mask = (const unsigned int*)(scratch + kNaMaskOff);
+    const unsigned long long* tile_off = (const unsigned long long*)(scratch + kNaOffsOff);
+    int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+    note_launch(), filter_gather_kernel<<<grid, kThreads, 0, s->stream>>>(mask, tile_off, n, ntiles, proj);
+    OXB_CUDA(cudaGetLastError());
+}
+
 }  // namespace oxb

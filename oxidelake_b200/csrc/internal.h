@@ -194,6 +194,11 @@ void check_status_word(uint32_t status, const char* what);
 // Exclusive scan of n u32 counts into n + 1 u64 offsets (offsets[n] = total).
 void scan_u32_to_u64(const StreamRef& s, const Backend& b, const unsigned int* counts,
                      unsigned long long* offsets, long long n);
+// The same scan with its block partials in caller memory
+// (scan_partials_needed(n) entries): it allocates nothing.
+long long scan_partials_needed(long long n);
+void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsigned long long* offsets, long long n,
+                          unsigned long long* partials);
 
 // Stable LSD radix sort of (key, value) pairs on bits [0, bits) of the key.
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
@@ -205,6 +210,9 @@ bool key_range(const StreamRef& s, const Backend& b, const Column& key, long lon
 
 // Operators.
 oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a);
+void filter_project_noalloc(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a,
+                            void* const* out_values, uint32_t* const* out_validity, long long capacity,
+                            long long* out_rows);
 oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b,
                                    const oxb_join_build_args& a);
 oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_join_probe_args& a);

@@ -223,6 +223,21 @@ void scan_u32_to_u64(const StreamRef& s, const Backend& b, const unsigned int* c
     OXB_CUDA(cudaGetLastError());
 }
 
+long long scan_partials_needed(long long n) { return n <= 0 ? 1 : (n + kScanChunk - 1) / kScanChunk + 1; }
+
+void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsigned long long* offsets, long long n,
+                          unsigned long long* partials) {
+    if (n <= 0) {
+        OXB_CUDA(cudaMemsetAsync(offsets, 0, sizeof(unsigned long long), s->stream));
+        return;
+    }
+    const long long blocks = (n + kScanChunk - 1) / kScanChunk;
+    note_launch(), scan_reduce_kernel<<<(unsigned)blocks, kScanThreads, 0, s->stream>>>(counts, n, partials);
+    note_launch(), scan_partials_kernel<<<1, 1024, 0, s->stream>>>(partials, blocks);
+    note_launch(), scan_apply_kernel<<<(unsigned)blocks, kScanThreads, 0, s->stream>>>(counts, n, partials, offsets);
+    OXB_CUDA(cudaGetLastError());
+}
+
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
                       unsigned int* values, long long n, int bits) {
     if (n <= 1 || bits <= 0) return;
