@@ -396,9 +396,13 @@ OXB_API uint64_t oxb_kernel_launches(void);
 OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
 /* Pins the aggregation kernels' variant instead of the tuned one: combine
  * -1 (automatic), 0 (per-row atomics), 1 (warp combining and caches), 2
- * (tile sort-reduce), 3 (columns streamed by bulk copies) or 4 (streamed
- * tile sort-reduce); rows_per_thread
- * 0 (automatic), 1 or 2. */
+ * (tile sort-reduce), 3 (columns streamed by bulk copies), 4 (streamed
+ * tile sort-reduce), 5 (join-aggregate only: the fused probe table, for a
+ * build-side group key with a small span; its dense form when the build
+ * keys fill at least a quarter of their range) or 6 (the fused probe table,
+ * hashed form); rows_per_thread 0 (automatic),
+ * 1, 2 or 4 (the row loops take 1 or 2, the fused kernel 2 or 4; other
+ * values round to the nearest the kernel has). */
 OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);
 
 /* GpuBackend::supports_predicate / supports_hash_join / supports_aggregate

@@ -1722,10 +1722,55 @@ __global__ void fuse_table_kernel(const __grid_constant__ JoinTableDev jt, const
 }
 
 struct FusedTab {
-    const FusedSlot* slots;
-    int aos;                  // 8-byte words per CTA slot (even)
-    int aos_idx[kMaxArrays];  // word of each array within a slot
+    const FusedSlot* slots;   // hashed form: one entry per join slot
+    const int* dense;         // dense form: one entry per key in [dense_lo, dense_lo + dense_n)
+    long long dense_lo;
+    unsigned long long dense_n;
 };
+
+// The fused kernel's CTA table, one array after another (no bank falls to a
+// fixed stride): the rows of each slot as u32 (a CTA folds fewer than 2^32
+// rows, which the host checks), then arrays 1.. as S u64 words each.
+__host__ __device__ inline size_t fused_counts_bytes(int S) { return ((size_t)S * 4 + 15) & ~(size_t)15; }
+size_t fused_smem_bytes(int S, int narrays) { return fused_counts_bytes(S) + (size_t)S * 8 * (narrays - 1); }
+
+// Dense form, for build keys that fill most of their range: entry
+// key - dense_lo holds the CTA slot of the key's group (>= 0), -1 when no
+// build row has the key, -2 when the key takes the slow path (repeated key,
+// NULL group, group outside the CTA table).  A 4-byte load from a table of
+// range x 4 bytes replaces the hashed probe.
+constexpr int kDenseNone = -1;
+constexpr int kDenseSlow = -2;
+
+__global__ void fuse_dense_kernel(const __grid_constant__ JoinTableDev jt, const __grid_constant__ AggKey gkey,
+                                  long long lo, int S, int* __restrict__ dense, long long dense_lo) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < jt.capacity;
+         s += (long long)gridDim.x * blockDim.x) {
+        const JoinSlot js = jt.slots[s];
+        if (js.key == kEmptyKey) continue;
+        int e = kDenseSlow;
+        if (js.count == 1) {
+            const unsigned int b = jt.first_row[s];
+            if (valid_at(gkey.validity, b)) {
+                const unsigned long long d = (unsigned long long)(load_int(gkey.values, gkey.type, b) - lo);
+                if (d < (unsigned long long)S) e = (int)d;
+            }
+        }
+        dense[(unsigned long long)js.key - (unsigned long long)dense_lo] = e;
+    }
+}
+
+// The join slot of a key placed in the table, -2 when it has none.
+__device__ __forceinline__ long long jt_find_slot(const JoinTableDev& t, long long key) {
+    unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (t.capacity - 1u));
+    for (unsigned int p = 0; p < t.capacity; p++) {
+        const long long k = t.slots[s].key;
+        if (k == key) return s;
+        if (k == kEmptyKey) return -2;
+        s = (s + 1u) & (t.capacity - 1u);
+    }
+    return -2;
+}
 
 // The slow path of one probe row: every match, folded into HBM.
 template <int MAXACC>
@@ -1754,21 +1799,17 @@ __device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const Jo
     (void)i;
 }
 
-template <int MAXACC, int RPT>
+template <int MAXACC, int RPT, bool DENSE>
 __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
     const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
     const __grid_constant__ FusedTab ft, long long n) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int S = P.smem_slots;
-    unsigned long long* tab = (unsigned long long*)smem;  // S * aos words, slot-major
-    for (int i = threadIdx.x; i < S * ft.aos; i += blockDim.x) {
-        const int w = i % ft.aos;
-        unsigned long long x = 0;
-        for (int a = 0; a < P.narrays; a++)
-            if (ft.aos_idx[a] == w) x = init_value(P.init[a]);
-        tab[i] = x;
-    }
+    unsigned int* rows = (unsigned int*)smem;
+    unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;  // array a at tab + a * S
+    for (int i = threadIdx.x; i < S; i += blockDim.x) rows[i] = 0;
+    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) tab[S + i] = init_value(P.init[1 + i / S]);
     __syncthreads();
     const unsigned long long keep = policy_evict_last();
     const unsigned int cap_mask = jt.capacity - 1u;
@@ -1787,6 +1828,18 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
             const long long key = pk_type == kInt64 ? __ldcs((const long long*)pk + i) : (long long)__ldcs((const int*)pk + i);
             if (key == kEmptyKey) {
                 if (jt.special_count) sidx[r] = -1;
+                continue;
+            }
+            if (DENSE) {
+                const unsigned long long d = (unsigned long long)key - (unsigned long long)ft.dense_lo;
+                if (d >= ft.dense_n) continue;
+                const int e = (int)ld_keep_u32(ft.dense + d, keep);
+                if (e >= 0) {
+                    sidx[r] = 0;
+                    cslot[r] = e;
+                } else if (e == kDenseSlow) {
+                    sidx[r] = jt_find_slot(jt, key);
+                }
                 continue;
             }
             unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & cap_mask);
@@ -1821,32 +1874,26 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
                 fused_slow_row<MAXACC>(P, gkey, jt, sidx[r], i, val);
                 continue;
             }
-            unsigned long long* t = tab + (long long)cslot[r] * ft.aos;
-            atomicAdd(&t[ft.aos_idx[0]], 1ull);
+            const int cs = cslot[r];
+            atomicAdd(&rows[cs], 1u);
 #pragma unroll
             for (int j = 0; j < MAXACC; j++) {
                 if (j >= P.nacc) break;
                 const DevAcc& a = P.acc[j];
-                unsigned long long* p = t + ft.aos_idx[a.arr];
+                unsigned long long* p = tab + a.arr * S + cs;
                 switch (a.kind) {
                     case kAccCount:
                     case kAccSumInt:
                         if (val[j]) atomicAdd(p, val[j]);
                         break;
                     case kAccSumF64: {
+                        // The atomic rounds old + x once; TwoSum recovers that
+                        // rounding error exactly, and it joins the compensation.
                         const double x = as_f64(val[j]);
-                        unsigned long long sv = p[0], cv = p[1];
-                        int tries = 0;
-                        for (; tries < (1 << 20); tries++) {
-                            double cs = as_f64(cv);
-                            const double ns = two_sum_into(as_f64(sv), x, &cs);
-                            unsigned long long os, oc;
-                            cas128_shared(smem_addr(p), sv, cv, as_u64(ns), as_u64(cs), &os, &oc);
-                            if (os == sv && oc == cv) break;
-                            sv = os;
-                            cv = oc;
-                        }
-                        if (tries == (1 << 20)) atomicOr(P.status, kStatusTimeout);
+                        const double old = atomicAdd((double*)p, x);
+                        double c = 0.0;
+                        two_sum_into(old, x, &c);
+                        if (c != 0.0) atomicAdd((double*)(p + S), c);
                         break;
                     }
                     case kAccMin:
@@ -1861,12 +1908,12 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
     }
     __syncthreads();
     for (int i = threadIdx.x; i < S; i += blockDim.x) {
-        const unsigned long long* t = tab + (long long)i * ft.aos;
-        if (t[ft.aos_idx[0]] == 0) continue;
+        if (rows[i] == 0) continue;
         const long long g = global_slot(P, true, P.direct_lo + i);
         if (g < 0) continue;
-        for (int a = 0; a < P.narrays; a++) {
-            const unsigned long long x = t[ft.aos_idx[a]];
+        atomicAdd(&P.arr[g], (unsigned long long)rows[i]);
+        for (int a = 1; a < P.narrays; a++) {
+            const unsigned long long x = tab[a * S + i];
             unsigned long long* d = P.arr + a * P.stride + g;
             switch (P.merge[a]) {
                 case kMergeAddU64:
@@ -2182,6 +2229,8 @@ struct AggVariant {
     bool tile;    // the tile sort-reduce kernels (combine/rpt unused)
     bool stream = false;  // the streamed kernels (combine/rpt unused)
     bool stile = false;   // the streamed tile sort-reduce kernels
+    bool fused = false;   // the fused probe-table join kernel (rpt used)
+    bool dense = false;   // ... with the dense lookup table
 };
 
 // The streamed kernels' plan: the probe-side columns (deduplicated) with
@@ -2307,7 +2356,22 @@ StreamJoinKernel stream_join_kernel_for(int maxacc) {
     return agg_stream_join_kernel<kMaxAccs>;
 }
 
+using FusedKernel = void (*)(const AggProgram, const DevPredicate, const AggKey, const void*, const uint8_t*, int,
+                             const JoinTableDev, const FusedTab, long long);
+
+FusedKernel fused_kernel_for(const AggVariant& v) {
+#define OXB_PICK(M, R, D) \
+    if (v.maxacc == M && v.rpt == R && v.dense == D) return agg_fused_join_kernel<M, R, D>;
+    OXB_PICK(2, 2, false) OXB_PICK(2, 4, false) OXB_PICK(4, 2, false) OXB_PICK(4, 4, false)
+    OXB_PICK(2, 2, true) OXB_PICK(2, 4, true) OXB_PICK(4, 2, true) OXB_PICK(4, 4, true)
+#undef OXB_PICK
+    fail(OXB_EXECUTION, "no fused join kernel for this variant");
+}
+
 std::string variant_name(const char* base, const AggVariant& v) {
+    if (v.fused)
+        return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") +
+               std::to_string(v.rpt) + ">";
     if (v.stile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream-tile>";
     if (v.stream) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream>";
     if (v.tile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",tile>";
@@ -2324,7 +2388,7 @@ std::map<std::string, AggVariant> g_tuned;
 template <typename Launch>
 oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, const AggKey& key_for_sample,
                          long long sample_rows, long long max_groups, const char* kernel_name, const StreamPlan* SP,
-                         Launch&& launch) {
+                         int fusable, Launch&& launch) {
     AggProgram& P = plan.P;
     const int maxacc = maxacc_for(P.nacc);
     P.scratch_accs = maxacc <= 4 ? maxacc : 0;
@@ -2432,8 +2496,20 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         }
         sp.bytes = stream_smem_bytes(sp.S, SP->stage_bytes, SP->aos);
     }
+    // The fused join kernel: a direct-mapped CTA table over the sampled span
+    // of the (build-side) group key, small enough for full occupancy.
+    SmemPlan fp;
+    if (fusable && maxacc <= 4 && span < 4096ull) {
+        const size_t bytes = fused_smem_bytes((int)span + 1, P.narrays);
+        if (bytes <= 48 * 1024) {
+            fp.S = (int)span + 1;
+            fp.direct = 1;
+            fp.direct_lo = span_lo;
+            fp.bytes = bytes;
+        }
+    }
     auto configure = [&](const AggVariant& v) {
-        const SmemPlan& p = v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp));
+        const SmemPlan& p = v.fused ? fp : (v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp)));
         P.smem_slots = p.S;
         P.wslots = p.Sw;
         P.direct = p.direct;
@@ -2448,6 +2524,13 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     // Warp caches need combining; without a CTA table the atomic-only path
     // would send every row to HBM, so it is no candidate then either.
     std::vector<AggVariant> candidates;
+    for (int d = fusable == 2 ? 1 : 0; d >= 0 && fp.S > 0; d--)
+        for (int r = 2; r <= 4; r += 2) {
+            AggVariant f{maxacc, false, r, false};
+            f.fused = true;
+            f.dense = d == 1;
+            candidates.push_back(f);
+        }
     if (stp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, false, true});
     if (sp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, true});
     if (tp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, true});
@@ -2460,17 +2543,27 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     while ((1u << cap_class) < cap) cap_class++;
     const std::string shape = std::string(kernel_name) + "/" + std::to_string(maxacc) + "/" +
                               std::to_string(cp.wdirect) + std::to_string(cp.direct) + std::to_string(tp.direct) + "/" +
-                              std::to_string(sampled_distinct * 8 <= 8192) + "/" + std::to_string(cap_class);
+                              std::to_string(sampled_distinct * 8 <= 8192) + "/" + std::to_string(cap_class) + "/" +
+                              std::to_string(fp.S > 0);
     AggVariant chosen{maxacc, maxacc <= 4, 2, tp.S > 0 && sp.S == 0, sp.S > 0 && stp.S == 0, stp.S > 0};
+    if (fp.S > 0) {
+        chosen = AggVariant{maxacc, false, 2, false};
+        chosen.fused = true;
+        chosen.dense = fusable == 2;
+    }
     bool tune = false;
     if (b.force_combine >= 0 || b.force_rpt > 0) {
         if (b.force_combine >= 0) {
+            chosen.fused = (b.force_combine == 5 || b.force_combine == 6) && fp.S > 0;
+            chosen.dense = b.force_combine == 5 && fusable == 2;
             chosen.stile = b.force_combine == 4 && stp.S > 0;
             chosen.stream = b.force_combine == 3 && sp.S > 0;
             chosen.tile = b.force_combine == 2 && tp.S > 0;
             chosen.combine = b.force_combine == 1 && maxacc <= 4;
         }
         if (b.force_rpt > 0) chosen.rpt = b.force_rpt;
+        if (chosen.fused) chosen.rpt = chosen.rpt <= 2 ? 2 : 4;
+        else if (chosen.rpt > 2) chosen.rpt = 2;
     } else {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tuned.find(shape);
@@ -2657,7 +2750,7 @@ oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_a
     AggKey k{key.values, key.validity, key.type, 0};
     StreamPlan SP;
     const bool streamable = plan_stream(plan.P, pred, key.values, key.validity, key.type, n, &SP);
-    return run_aggregate(s, b, plan, k, n, n, "agg_rows_kernel", streamable ? &SP : nullptr,
+    return run_aggregate(s, b, plan, k, n, n, "agg_rows_kernel", streamable ? &SP : nullptr, 0,
                          [&](AggProgram& P, size_t smem, const AggVariant& v) {
         if (n == 0) return;
         if (v.stile) {
@@ -2722,9 +2815,44 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
     const JoinTableDev jt = a.table->t;
     StreamPlan SP;
     const bool streamable = plan_stream(plan.P, pred, pk.values, pk.validity, pk.type, n, &SP);
+    // The fused probe-table kernel takes a build-side group key and
+    // probe-side aggregate inputs.
+    // Its CTA row counts are u32: with at least one CTA per SM, fewer than
+    // 2^38 probe rows keep every CTA under 2^32.
+    bool fusable = a.group_side == 1 && n < (1ll << 38);
+    for (int j = 0; j < plan.P.nacc; j++) fusable = fusable && plan.P.acc[j].side == 0;
+    // The dense lookup table when the build keys fill at least a quarter of
+    // their range (and it stays under 256 MB).
+    const unsigned long long key_span = (unsigned long long)jt.key_hi - (unsigned long long)jt.key_lo;
+    const bool dense = jt.key_lo <= jt.key_hi && key_span < (1ull << 26) &&
+                       (long long)key_span < 4 * jt.ndistinct + 4096;
     return run_aggregate(s, b, plan, sample_key, group_rows, group_rows, "agg_join_kernel", streamable ? &SP : nullptr,
-                         [&](AggProgram& P, size_t smem, const AggVariant& v) {
+                         fusable ? (dense ? 2 : 1) : 0, [&](AggProgram& P, size_t smem, const AggVariant& v) {
                              if (n == 0) return;
+                             if (v.fused) {
+                                 FusedTab ft{};
+                                 AllocRef fs;
+                                 const int grid = grid_for(b, jt.capacity, 256, 8);
+                                 if (v.dense) {
+                                     ft.dense_lo = jt.key_lo;
+                                     ft.dense_n = key_span + 1;
+                                     fs = dev_alloc(s, (size_t)ft.dense_n * 4, false);
+                                     OXB_CUDA(cudaMemsetAsync(fs->ptr, 0xff, (size_t)ft.dense_n * 4, s->stream));
+                                     ft.dense = (const int*)fs->ptr;
+                                     note_launch(), fuse_dense_kernel<<<grid, 256, 0, s->stream>>>(
+                                         jt, k, P.direct_lo, P.smem_slots, (int*)fs->ptr, ft.dense_lo);
+                                 } else {
+                                     fs = dev_alloc(s, (size_t)jt.capacity * sizeof(FusedSlot), false);
+                                     ft.slots = (const FusedSlot*)fs->ptr;
+                                     note_launch(), fuse_table_kernel<<<grid, 256, 0, s->stream>>>(
+                                         jt, k, P.direct_lo, P.smem_slots, (FusedSlot*)fs->ptr);
+                                 }
+                                 FusedKernel kern = fused_kernel_for(v);
+                                 set_smem(kern, smem);
+                                 note_launch(), kern<<<resident_grid(b, kern, smem, (n + v.rpt - 1) / v.rpt), kFusedThreads,
+                                                       smem, s->stream>>>(P, pred, k, pk.values, pk.validity, pk.type, jt, ft, n);
+                                 return;
+                             }
                              if (v.stile) {
                                  StileKernel kern = stile_kernel_for(v.maxacc, true);
                                  set_smem(kern, smem);

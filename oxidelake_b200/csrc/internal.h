@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <cstdint>
@@ -157,6 +158,9 @@ struct JoinTableDev {
     unsigned int special_start = 0;
     unsigned int special_count = 0;
     int key_type = kInt64;
+    // Smallest and largest key placed in the slots (key_lo > key_hi: none).
+    long long key_lo = 0;
+    long long key_hi = -1;
 };
 
 }  // namespace oxb

@@ -269,16 +269,26 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
             OXB_CUDA(cudaMemcpyAsync(rstart.get(), ix.starts, nruns * 4, cudaMemcpyHostToDevice, s->stream));
             OXB_CUDA(cudaMemcpyAsync(rcount.get(), ix.counts, nruns * 4, cudaMemcpyHostToDevice, s->stream));
             // The side slot is filled on the host for the kEmptyKey run.
-            for (long long r = 0; r < nruns; r++)
+            for (long long r = 0; r < nruns; r++) {
                 if (ix.keys[r] == kEmptyKey) {
                     t.special_start = ix.starts[r];
                     t.special_count = ix.counts[r];
+                    continue;
                 }
+                if (t.key_lo > t.key_hi) t.key_lo = t.key_hi = ix.keys[r];
+                t.key_lo = std::min(t.key_lo, (long long)ix.keys[r]);
+                t.key_hi = std::max(t.key_hi, (long long)ix.keys[r]);
+            }
         }
     } else {
         // Device build: stable sort of (key, row) by key keeps build order.
         long long lo = 0, hi = 0, nvalid = 0;
         bool any = key_range(s, b, key, n, &lo, &hi, &nvalid);
+        if (any) {
+            // kEmptyKey lives in the side slot: the placed range starts above it.
+            t.key_lo = lo == kEmptyKey ? lo + 1 : lo;
+            t.key_hi = hi;
+        }
         Scratch<unsigned long long> ukeys;
         Scratch<unsigned int> srows;
         if (any) {
@@ -320,12 +330,17 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
                                                                                   rcount.get());
             OXB_CUDA(cudaGetLastError());
             if (lo == kEmptyKey) {
-                // The smallest key sorts first: run 0.
+                // The smallest key sorts first: run 0; the smallest placed key
+                // is run 1's.
                 unsigned int c = 0;
+                long long next = 0;
                 OXB_CUDA(cudaMemcpyAsync(&c, rcount.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+                if (nruns > 1)
+                    OXB_CUDA(cudaMemcpyAsync(&next, rkeys.get() + 1, 8, cudaMemcpyDeviceToHost, s->stream));
                 OXB_CUDA(cudaStreamSynchronize(s->stream));
                 t.special_start = 0;
                 t.special_count = c;
+                if (nruns > 1) t.key_lo = next;
             }
         }
     }

@@ -5,7 +5,7 @@ import pyarrow as pa
 import pytest
 
 import oracle
-from compare import assert_batches_equal
+from compare import abs_columns, assert_batches_equal
 from datagen import config2
 from oxidelake_b200.params import AggregateFunction as F
 from oxidelake_b200.params import Comparison as Cmp
@@ -57,7 +57,7 @@ def test_duplicates_nulls_and_probe_side_groups(backend, stream):
             assert_batches_equal(got, want, float_sum_cols=(1,))
 
 
-@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("rpt", [1, 2])
 def test_every_kernel_variant(backend, stream, combine, rpt):
     """Each compiled variant of the row-loop kernels (the autotuner's
@@ -86,7 +86,60 @@ def test_every_kernel_variant(backend, stream, combine, rpt):
         for sp in (spec, AggregateSpec(0, [(F.Sum, 1), (F.CountStar, 0)])):
             got = backend.download(stream, backend.aggregate(stream, dev, sp))
             want = oracle.aggregate(batch, 0, [(int(f), c) for f, c in sp.aggregates])
+            scale = oracle.aggregate(abs_columns(batch, {1}), 0, [(int(f), c) for f, c in sp.aggregates])
             sums = [1 + j for j, (f, c) in enumerate(sp.aggregates) if f in (F.Sum, F.Avg) and c == 1]
-            assert_batches_equal(got, want, float_sum_cols=sums)
+            assert_batches_equal(got, want, float_sum_cols=sums, scale=scale)
     finally:
         backend.set_agg_variant(-1, 0)
+
+
+@pytest.mark.parametrize("rpt", [2, 4])
+@pytest.mark.parametrize("form", [5, 6], ids=["dense", "hashed"])
+def test_fused_probe_table_edges(backend, stream, rpt, form):
+    """The fused probe-table kernel (a build-side group key, probe-side
+    inputs) on the cases its fast path hands to the slow one: build keys
+    that repeat, NULL group keys, the INT64_MIN key on both sides, and group
+    keys outside the sampled span (the group-key sample reads build rows
+    0, 4, 8, ... of these 32768, so rows 1 mod 4 stay unsampled)."""
+    rng = np.random.default_rng(40 + rpt)
+    nb, npr = 32_768, 500_000
+    key = rng.permutation(nb).astype(np.int64)
+    key[:300] = key[300:600]  # 300 keys appear twice
+    key[600] = np.iinfo(np.int64).min
+    attr = rng.integers(0, 40, nb).astype(np.int32)
+    outliers = np.array([701, 705, 709, 713, 717])
+    attr[outliers] = [2_000_000_000, -2_000_000_000, 1_000_000, 77_777, -5]
+    attr_null = rng.random(nb) < 0.03
+    attr_null[outliers] = False
+    build = pa.RecordBatch.from_arrays(
+        [pa.array(key, pa.int64(), mask=rng.random(nb) < 0.01), pa.array(attr, mask=attr_null)],
+        names=["key", "attr"],
+    )
+    fk = rng.integers(0, nb + nb // 10, npr).astype(np.int64)
+    fk[rng.random(npr) < 0.01] = np.iinfo(np.int64).min
+    hot = rng.random(npr) < 0.2
+    fk[hot] = key[outliers[rng.integers(0, 5, hot.sum())]]
+    probe = pa.RecordBatch.from_arrays(
+        [
+            pa.array(fk, pa.int64(), mask=rng.random(npr) < 0.02),
+            pa.array(rng.uniform(-100, 100, npr), mask=rng.random(npr) < 0.03),
+            pa.array(rng.integers(1, 51, npr).astype(np.int32), mask=rng.random(npr) < 0.01),
+        ],
+        names=["fk", "payload", "qty"],
+    )
+    pred = compare(2, Cmp.Gt, Literal.int32(10))
+    aggs = [(F.Sum, 0, 1), (F.Sum, 0, 2), (F.CountStar, 0, 0), (F.Avg, 0, 1), (F.Min, 0, 2), (F.Max, 0, 1)]
+    backend.set_agg_variant(form, rpt)
+    backend.set_kernel_timing(True)
+    try:
+        for agg_set, fused in ((aggs[:4], True), (aggs, False)):
+            got = run(backend, stream, build, probe, pred, (1, 1), agg_set)
+            name = backend.last_kernel_time()[0]
+            assert ("fused" in name) == fused and ("fused-dense" in name) == (fused and form == 5), name
+            spec = [(int(f), s, c) for f, s, c in agg_set]
+            want = oracle.join_aggregate(probe, build, 0, 0, leaves(pred), (1, 1), spec)
+            scale = oracle.join_aggregate(abs_columns(probe, {1}), build, 0, 0, leaves(pred), (1, 1), spec)
+            assert_batches_equal(got, want, float_sum_cols=(1, 4), scale=scale)
+    finally:
+        backend.set_agg_variant(-1, 0)
+        backend.set_kernel_timing(False)
