@@ -399,10 +399,11 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * (tile sort-reduce), 3 (columns streamed by bulk copies), 4 (streamed
  * tile sort-reduce), 5 (join-aggregate only: the fused probe table, for a
  * build-side group key with a small span; its dense form when the build
- * keys fill at least a quarter of their range) or 6 (the fused probe table,
- * hashed form); rows_per_thread 0 (automatic),
- * 1, 2 or 4 (the row loops take 1 or 2, the fused kernel 2 or 4; other
- * values round to the nearest the kernel has). */
+ * keys fill at least a quarter of their range), 6 (the fused probe table,
+ * hashed form), 7 or 8 (5 or 6 interpreted a vector of rows per thread at
+ * a time); rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
+ * 1 or 2, the fused kernels 2 or 4, the vector ones 4 or 8; other values
+ * round to the nearest the kernel has). */
 OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);
 
 /* GpuBackend::supports_predicate / supports_hash_join / supports_aggregate

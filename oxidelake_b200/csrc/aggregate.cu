@@ -1799,6 +1799,49 @@ __device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const Jo
     (void)i;
 }
 
+// Adds a fused kernel's CTA table into the HBM table: each occupied slot's
+// rows and arrays, Float64 sums with their compensation.
+__device__ void fused_flush(const AggProgram& P, const unsigned int* rows, const unsigned long long* tab, int S) {
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+        if (rows[i] == 0) continue;
+        const long long g = global_slot(P, true, P.direct_lo + i);
+        if (g < 0) continue;
+        atomicAdd(&P.arr[g], (unsigned long long)rows[i]);
+        for (int a = 1; a < P.narrays; a++) {
+            const unsigned long long x = tab[a * S + i];
+            unsigned long long* d = P.arr + a * P.stride + g;
+            switch (P.merge[a]) {
+                case kMergeAddU64:
+                    if (x) atomicAdd(d, x);
+                    break;
+                case kMergeAddF64Comp:
+                    add_f64_comp((double*)d, (double*)(d + P.stride), as_f64(x));
+                    break;
+                case kMergeAddF64:
+                    if (as_f64(x) != 0.0) atomicAdd((double*)d, as_f64(x));
+                    break;
+                case kMergeMin:
+                    if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)d, (long long)x);
+                    break;
+                default:
+                    if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)d, (long long)x);
+                    break;
+            }
+        }
+    }
+}
+
+// The slow path of one probe row, out of line: its contributions, then
+// every match folded into HBM.
+__device__ __noinline__ void fused_slow(const AggProgram& P, const AggKey& gkey, const JoinTableDev& jt,
+                                        long long s_or_special, long long i) {
+    unsigned long long val[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (j < P.nacc) val[j] = contribution(P.acc[j], i, 0);
+    fused_slow_row<4>(P, gkey, jt, s_or_special, i, val);
+}
+
 template <int MAXACC, int RPT, bool DENSE>
 __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
@@ -1907,33 +1950,168 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < S; i += blockDim.x) {
-        if (rows[i] == 0) continue;
-        const long long g = global_slot(P, true, P.direct_lo + i);
-        if (g < 0) continue;
-        atomicAdd(&P.arr[g], (unsigned long long)rows[i]);
-        for (int a = 1; a < P.narrays; a++) {
-            const unsigned long long x = tab[a * S + i];
-            unsigned long long* d = P.arr + a * P.stride + g;
-            switch (P.merge[a]) {
-                case kMergeAddU64:
-                    if (x) atomicAdd(d, x);
+    fused_flush(P, rows, tab, S);
+}
+
+// The fused join-aggregate, interpreted a vector of rows at a time: each
+// thread takes RPT rows; the predicate's leaves, the key, the lookups and
+// then each accumulator are handled for all RPT rows together, so a type or
+// kind is dispatched once per RPT rows and each column's loads go out
+// together.  The CTA table and its flush are agg_fused_join_kernel's.
+template <int RPT, bool DENSE>
+__global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
+    const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
+    const __grid_constant__ FusedTab ft, long long n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int S = P.smem_slots;
+    unsigned int* rows = (unsigned int*)smem;
+    unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;  // array a at tab + a * S
+    for (int i = threadIdx.x; i < S; i += blockDim.x) rows[i] = 0;
+    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) tab[S + i] = init_value(P.init[1 + i / S]);
+    __syncthreads();
+    const unsigned long long keep = policy_evict_last();
+    const long long stride = blockDim.x;
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long tile = blockIdx.x * (long long)blockDim.x * RPT; tile < n; tile += step) {
+        const long long base = tile + threadIdx.x;  // row r: base + r * stride
+        unsigned live = 0;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if (base + r * stride < n) live |= 1u << r;
+        live = predicate_mask<RPT>(pred, base, stride, live);
+        if (pkv) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                if (((live >> r) & 1u) && !valid_at(pkv, base + r * stride)) live &= ~(1u << r);
+        }
+        long long key[RPT];
+        if (pk_type == kInt64) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++) key[r] = (live >> r) & 1u ? __ldcs((const long long*)pk + base + r * stride) : 0;
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                key[r] = (live >> r) & 1u ? (long long)__ldcs((const int*)pk + base + r * stride) : 0;
+        }
+        // Lookups: cs[r] is the CTA slot of a fast row; slow rows fold now.
+        int cs[RPT];
+        unsigned fast = 0;
+        if (DENSE) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                cs[r] = kDenseNone;
+                const unsigned long long d = (unsigned long long)key[r] - (unsigned long long)ft.dense_lo;
+                if (((live >> r) & 1u) && d < ft.dense_n) cs[r] = (int)ld_keep_u32(ft.dense + d, keep);
+            }
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                if (!((live >> r) & 1u)) continue;
+                if (cs[r] >= 0) {
+                    fast |= 1u << r;
+                } else if (key[r] == kEmptyKey) {
+                    if (jt.special_count) fused_slow(P, gkey, jt, -1, base + r * stride);
+                } else if (cs[r] == kDenseSlow) {
+                    fused_slow(P, gkey, jt, jt_find_slot(jt, key[r]), base + r * stride);
+                }
+            }
+        } else {
+            const unsigned int cap_mask = jt.capacity - 1u;
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                cs[r] = -1;
+                if (!((live >> r) & 1u)) continue;
+                if (key[r] == kEmptyKey) {
+                    if (jt.special_count) fused_slow(P, gkey, jt, -1, base + r * stride);
+                    continue;
+                }
+                unsigned int sl = (unsigned int)(fmix64((unsigned long long)key[r]) & cap_mask);
+                for (unsigned int q = 0; q <= cap_mask; q++) {
+                    const int4 e = ld_keep_v4(&ft.slots[sl], keep);
+                    const long long k = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
+                    if (k == key[r]) {
+                        if ((unsigned int)e.w == 1u && e.z >= 0) {
+                            cs[r] = e.z;
+                            fast |= 1u << r;
+                        } else {
+                            fused_slow(P, gkey, jt, sl, base + r * stride);
+                        }
+                        break;
+                    }
+                    if (k == kEmptyKey) break;
+                    sl = (sl + 1u) & cap_mask;
+                }
+            }
+        }
+        if (!fast) continue;
+#pragma unroll
+        for (int r = 0; r < RPT; r++)
+            if ((fast >> r) & 1u) atomicAdd(&rows[cs[r]], 1u);
+        for (int j = 0; j < P.nacc; j++) {
+            const DevAcc& a = P.acc[j];
+            unsigned long long* col = tab + a.arr * S;
+            unsigned vm = fast;
+            if (a.validity) {
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    if (((vm >> r) & 1u) && !valid_at(a.validity, base + r * stride)) vm &= ~(1u << r);
+            }
+            if (a.kind == kAccCount) {
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    if ((vm >> r) & 1u) atomicAdd(&col[cs[r]], 1ull);
+                continue;
+            }
+            long long raw[RPT];
+            if (a.in_type == kInt32) {
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    raw[r] = (vm >> r) & 1u ? (long long)__ldcs((const int*)a.values + base + r * stride) : 0;
+            } else {
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    raw[r] = (vm >> r) & 1u ? __ldcs((const long long*)a.values + base + r * stride) : 0;
+            }
+            switch (a.kind) {
+                case kAccSumInt:
+#pragma unroll
+                    for (int r = 0; r < RPT; r++)
+                        if ((vm >> r) & 1u) atomicAdd(&col[cs[r]], (unsigned long long)raw[r]);
                     break;
-                case kMergeAddF64Comp:
-                    add_f64_comp((double*)d, (double*)(d + P.stride), as_f64(x));
+                case kAccSumF64:
+#pragma unroll
+                    for (int r = 0; r < RPT; r++) {
+                        if (!((vm >> r) & 1u)) continue;
+                        // The atomic rounds old + x once; TwoSum recovers that
+                        // rounding error exactly, and it joins the compensation.
+                        const double x = a.in_type == kFloat64 ? __longlong_as_double(raw[r]) : (double)raw[r];
+                        const double old = atomicAdd((double*)&col[cs[r]], x);
+                        double c = 0.0;
+                        two_sum_into(old, x, &c);
+                        if (c != 0.0) atomicAdd((double*)&col[S + cs[r]], c);
+                    }
                     break;
-                case kMergeAddF64:
-                    if (as_f64(x) != 0.0) atomicAdd((double*)d, as_f64(x));
-                    break;
-                case kMergeMin:
-                    if ((long long)x != 0x7fffffffffffffffll) atomicMin((long long*)d, (long long)x);
+                case kAccMin:
+#pragma unroll
+                    for (int r = 0; r < RPT; r++) {
+                        if (!((vm >> r) & 1u)) continue;
+                        const long long v = a.in_type == kFloat64 ? total_order_key(__longlong_as_double(raw[r])) : raw[r];
+                        atomicMin((long long*)&col[cs[r]], v);
+                    }
                     break;
                 default:
-                    if ((long long)x != (long long)0x8000000000000000ull) atomicMax((long long*)d, (long long)x);
+#pragma unroll
+                    for (int r = 0; r < RPT; r++) {
+                        if (!((vm >> r) & 1u)) continue;
+                        const long long v = a.in_type == kFloat64 ? total_order_key(__longlong_as_double(raw[r])) : raw[r];
+                        atomicMax((long long*)&col[cs[r]], v);
+                    }
                     break;
             }
         }
     }
+    __syncthreads();
+    fused_flush(P, rows, tab, S);
 }
 
 __global__ void agg_init_kernel(const __grid_constant__ AggProgram P) {
@@ -2231,6 +2409,7 @@ struct AggVariant {
     bool stile = false;   // the streamed tile sort-reduce kernels
     bool fused = false;   // the fused probe-table join kernel (rpt used)
     bool dense = false;   // ... with the dense lookup table
+    bool vec = false;     // ... interpreted a vector of rows at a time (rpt 4 or 8)
 };
 
 // The streamed kernels' plan: the probe-side columns (deduplicated) with
@@ -2360,6 +2539,10 @@ using FusedKernel = void (*)(const AggProgram, const DevPredicate, const AggKey,
                              const JoinTableDev, const FusedTab, long long);
 
 FusedKernel fused_kernel_for(const AggVariant& v) {
+    if (v.vec) {
+        if (v.dense) return v.rpt == 4 ? agg_fusedv_join_kernel<4, true> : agg_fusedv_join_kernel<8, true>;
+        return v.rpt == 4 ? agg_fusedv_join_kernel<4, false> : agg_fusedv_join_kernel<8, false>;
+    }
 #define OXB_PICK(M, R, D) \
     if (v.maxacc == M && v.rpt == R && v.dense == D) return agg_fused_join_kernel<M, R, D>;
     OXB_PICK(2, 2, false) OXB_PICK(2, 4, false) OXB_PICK(4, 2, false) OXB_PICK(4, 4, false)
@@ -2371,7 +2554,7 @@ FusedKernel fused_kernel_for(const AggVariant& v) {
 std::string variant_name(const char* base, const AggVariant& v) {
     if (v.fused)
         return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") +
-               std::to_string(v.rpt) + ">";
+               (v.vec ? "vec," : "") + std::to_string(v.rpt) + ">";
     if (v.stile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream-tile>";
     if (v.stream) return std::string(base) + "<" + std::to_string(v.maxacc) + ",stream>";
     if (v.tile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",tile>";
@@ -2525,12 +2708,15 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     // would send every row to HBM, so it is no candidate then either.
     std::vector<AggVariant> candidates;
     for (int d = fusable == 2 ? 1 : 0; d >= 0 && fp.S > 0; d--)
-        for (int r = 2; r <= 4; r += 2) {
-            AggVariant f{maxacc, false, r, false};
-            f.fused = true;
-            f.dense = d == 1;
-            candidates.push_back(f);
-        }
+        for (int r = 2; r <= 8; r *= 2)
+            for (int vec = 0; vec < 2; vec++) {
+                if ((vec == 0 && r == 8) || (vec == 1 && r == 2)) continue;
+                AggVariant f{maxacc, false, r, false};
+                f.fused = true;
+                f.vec = vec == 1;
+                f.dense = d == 1;
+                candidates.push_back(f);
+            }
     if (stp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, false, true});
     if (sp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, true});
     if (tp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, true});
@@ -2554,15 +2740,17 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     bool tune = false;
     if (b.force_combine >= 0 || b.force_rpt > 0) {
         if (b.force_combine >= 0) {
-            chosen.fused = (b.force_combine == 5 || b.force_combine == 6) && fp.S > 0;
-            chosen.dense = b.force_combine == 5 && fusable == 2;
+            chosen.fused = b.force_combine >= 5 && b.force_combine <= 8 && fp.S > 0;
+            chosen.vec = b.force_combine >= 7;
+            chosen.dense = (b.force_combine == 5 || b.force_combine == 7) && fusable == 2;
             chosen.stile = b.force_combine == 4 && stp.S > 0;
             chosen.stream = b.force_combine == 3 && sp.S > 0;
             chosen.tile = b.force_combine == 2 && tp.S > 0;
             chosen.combine = b.force_combine == 1 && maxacc <= 4;
         }
         if (b.force_rpt > 0) chosen.rpt = b.force_rpt;
-        if (chosen.fused) chosen.rpt = chosen.rpt <= 2 ? 2 : 4;
+        if (chosen.fused && chosen.vec) chosen.rpt = chosen.rpt <= 4 ? 4 : 8;
+        else if (chosen.fused) chosen.rpt = chosen.rpt <= 2 ? 2 : 4;
         else if (chosen.rpt > 2) chosen.rpt = 2;
     } else {
         std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -104,6 +104,63 @@ __device__ __forceinline__ bool predicate_holds(const DevPredicate& p, long long
     return true;
 }
 
+// The predicate over RPT rows at once: bit r of the result is set when row
+// base + r * stride (bit r of `live`) satisfies every leaf.  A leaf's type
+// and comparison are dispatched once for the RPT rows, whose loads are
+// issued together.
+template <int RPT>
+__device__ __forceinline__ unsigned predicate_mask(const DevPredicate& p, long long base, long long stride,
+                                                   unsigned live) {
+    for (int l = 0; l < p.nleaves && live; l++) {
+        const DevLeaf& lf = p.leaves[l];
+        long long a[RPT];
+        if (lf.type == kFloat64) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                a[r] = (live >> r) & 1u ? filter_order_key(__ldcs((const double*)lf.values + base + r * stride)) : 0;
+        } else if (lf.type == kInt64) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                a[r] = (live >> r) & 1u ? __ldcs((const long long*)lf.values + base + r * stride) : 0;
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                a[r] = (live >> r) & 1u ? (long long)__ldcs((const int*)lf.values + base + r * stride) : 0;
+        }
+        const long long lit = lf.lit;
+        unsigned m = 0;
+        switch (lf.op) {
+            case 0:
+#pragma unroll
+                for (int r = 0; r < RPT; r++) m |= (unsigned)(a[r] == lit) << r;
+                break;
+            case 1:
+#pragma unroll
+                for (int r = 0; r < RPT; r++) m |= (unsigned)(a[r] < lit) << r;
+                break;
+            case 2:
+#pragma unroll
+                for (int r = 0; r < RPT; r++) m |= (unsigned)(a[r] <= lit) << r;
+                break;
+            case 3:
+#pragma unroll
+                for (int r = 0; r < RPT; r++) m |= (unsigned)(a[r] > lit) << r;
+                break;
+            default:
+#pragma unroll
+                for (int r = 0; r < RPT; r++) m |= (unsigned)(a[r] >= lit) << r;
+                break;
+        }
+        live &= m;
+        if (lf.validity) {
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                if (((live >> r) & 1u) && !valid_at(lf.validity, base + r * stride)) live &= ~(1u << r);
+        }
+    }
+    return live;
+}
+
 __device__ __forceinline__ long long load_key(const void* values, int type, long long row) {
     return type == kInt64 ? __ldg((const long long*)values + row)
                           : (long long)__ldg((const int*)values + row);

@@ -57,7 +57,7 @@ def test_duplicates_nulls_and_probe_side_groups(backend, stream):
             assert_batches_equal(got, want, float_sum_cols=(1,))
 
 
-@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("rpt", [1, 2])
 def test_every_kernel_variant(backend, stream, combine, rpt):
     """Each compiled variant of the row-loop kernels (the autotuner's
@@ -93,8 +93,8 @@ def test_every_kernel_variant(backend, stream, combine, rpt):
         backend.set_agg_variant(-1, 0)
 
 
-@pytest.mark.parametrize("rpt", [2, 4])
-@pytest.mark.parametrize("form", [5, 6], ids=["dense", "hashed"])
+@pytest.mark.parametrize("rpt", [2, 4, 8])
+@pytest.mark.parametrize("form", [5, 6, 7, 8], ids=["dense", "hashed", "dense-vec", "hashed-vec"])
 def test_fused_probe_table_edges(backend, stream, rpt, form):
     """The fused probe-table kernel (a build-side group key, probe-side
     inputs) on the cases its fast path hands to the slow one: build keys
@@ -135,7 +135,8 @@ def test_fused_probe_table_edges(backend, stream, rpt, form):
         for agg_set, fused in ((aggs[:4], True), (aggs, False)):
             got = run(backend, stream, build, probe, pred, (1, 1), agg_set)
             name = backend.last_kernel_time()[0]
-            assert ("fused" in name) == fused and ("fused-dense" in name) == (fused and form == 5), name
+            assert ("fused" in name) == fused and ("fused-dense" in name) == (fused and form in (5, 7)), name
+            assert ("vec" in name) == (fused and form in (7, 8)), name
             spec = [(int(f), s, c) for f, s, c in agg_set]
             want = oracle.join_aggregate(probe, build, 0, 0, leaves(pred), (1, 1), spec)
             scale = oracle.join_aggregate(abs_columns(probe, {1}), build, 0, 0, leaves(pred), (1, 1), spec)
