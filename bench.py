@@ -20,7 +20,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -67,59 +66,76 @@ def profiled_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clocks and clock-event (throttle) reasons read from NVML every 2 ms
+    by a thread while the timed region runs (read-only queries; no setting of
+    the GPU is touched)."""
 
-    Q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    REASONS = {
+        "hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+        "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+        "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+        "sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
+        "hw_power_brake_slowdown": "nvmlClocksEventReasonHwPowerBrakeSlowdown",
+    }
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []  # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
+        self.handle = None
+        self.stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL,
-                text=True,
-            )
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self.nv = nv
+            self.handle = nv.nvmlDeviceGetHandleByUUID(uuid)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+        except Exception as e:  # NVML missing: no clock record
+            self.error = repr(e)
+            self.handle = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                why = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((float(mhz), int(why)))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
+        if not self.samples:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = set()
+        for _, why in self.samples:
+            for name, const in self.REASONS.items():
+                if why & getattr(self.nv, const, 0):
+                    reasons.add(name)
+        return {
+            "sm_mhz": float(np.median([m for m, _ in self.samples])),
+            "sm_max_mhz": self.max_mhz,
+            "reasons": sorted(reasons),
+            "samples": len(self.samples),
+            "source": "NVML, every 2 ms during the timed steps",
+        }
 
 
 def gen_data(rank: int, build_rows: int, probe_rows: int):
@@ -220,7 +236,7 @@ def cpu_baseline(build, probe, target_s: float):
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
@@ -303,6 +319,7 @@ def main() -> int:
     torch.cuda.synchronize()
 
     kernel_ms = []
+    kernel_name = None
     launches0 = backend.kernel_launches()
     with ClockSampler(local) as clocks:
         barrier()
@@ -311,7 +328,8 @@ def main() -> int:
         e0.record(tstream)
         for _ in range(args.steps):
             res = step()
-            kernel_ms.append(backend.last_kernel_time()[1])
+            kernel_name, kms_step = backend.last_kernel_time()
+            kernel_ms.append(kms_step)
         e1.record(tstream)
         torch.cuda.synchronize()
         barrier()
@@ -385,14 +403,15 @@ def main() -> int:
             },
             "roofline": {
                 "bound": "hbm",
-                "kernel": "agg_join_kernel",
+                "kernel": kernel_name,
+                "timed": "the query's probe-table pre-pass and fused probe/filter/aggregate kernel, CUDA events on its stream",
                 "achieved": round(achieved, 1) if achieved else None,
                 "peak": peak,
                 "peak_kind": peak_kind,
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None,
                 "kernel_ms": round(kms, 4) if kms else None,
-                "traffic": profiled_traffic("agg_join_kernel"),
+                "traffic": profiled_traffic("agg_fused_join_kernel"),
                 "algorithmic_bytes_per_launch": kernel_bytes,
             },
             "e2e": {
