@@ -337,6 +337,48 @@ typedef struct oxb_aggregate_args {
 OXB_API oxb_status oxb_aggregate(oxb_backend* backend, oxb_stream* stream,
                          const oxb_aggregate_args* args, oxb_batch** out);
 
+/* ORDER BY l2|cosine(vector, query) LIMIT k over the rows a WHERE keeps, for
+ * a batch of queries: the reference's GpuVectorDistanceExec followed by its
+ * CPU SortExec(fetch = k) (compute/src/exec/vector.rs:29-249,
+ * cpu/kernels.rs:841-927), fused.  Rows with a NULL vector are left out; the
+ * order is (distance in IEEE totalOrder, row id); when fewer than k rows
+ * qualify, the rest of the row is id -1 and distance NaN.  Returned
+ * distances are the reference's FP32 values bit for bit.
+ *
+ * oxb_vector_index_build keeps a BF16 copy of the vector column (and each
+ * row's norm) resident for the tensor-core scan; the index refers to the
+ * batch's FP32 vectors, so the batch outlives it.  Up to 2^32 - 1 rows. */
+OXB_API oxb_status oxb_vector_index_build(oxb_backend* backend, oxb_stream* stream, const oxb_batch* input,
+                                          int32_t column, oxb_vector_index** out);
+OXB_API void oxb_vector_index_free(oxb_vector_index* index);
+
+typedef struct oxb_vector_topk_args {
+    const oxb_vector_index* index;
+    const oxb_batch* input;  /* the batch the index was built over (WHERE columns) */
+    const oxb_leaf* leaves;  /* WHERE over `input`, NULL/0 = every row */
+    int32_t nleaves;
+    int32_t nqueries;
+    const float* queries;    /* host, nqueries x dim FP32 */
+    int32_t dim;
+    int32_t k;               /* 1..4096 */
+    int32_t metric;          /* oxb_metric */
+    int32_t overfetch;       /* re-ranked candidates per query = overfetch * k (0: 4) */
+    int32_t exact;           /* 1: skip the BF16 scan, the exact FP32 path for every query */
+    int32_t reserved;
+} oxb_vector_topk_args;
+
+typedef struct oxb_vector_topk_stats {
+    int64_t reranked;          /* candidates re-ranked in FP32 */
+    int64_t exact_queries;     /* queries the exact path answered */
+    double max_score_error;    /* largest |BF16 score - FP64 score| among re-ranked candidates */
+    double mean_score_error;
+} oxb_vector_topk_stats;
+
+/* out_ids: nqueries x k int64 (host), out_dist: nqueries x k float (host);
+ * stats may be NULL.  Synchronizes `stream`. */
+OXB_API oxb_status oxb_vector_topk(oxb_backend* backend, oxb_stream* stream, const oxb_vector_topk_args* args,
+                                   int64_t* out_ids, float* out_dist, oxb_vector_topk_stats* stats);
+
 /* VectorDistanceArgs, args.rs:72-84 -> GpuBackend::vector_distance
  * (backend.rs:173): the input columns plus a Float32 distance column with
  * the vector column's validity.  Distances follow cpu/kernels.rs:909-927

@@ -125,6 +125,32 @@ class AggregateArgs(C.Structure):
     ]
 
 
+class VectorTopkArgs(C.Structure):
+    _fields_ = [
+        ("index", C.c_void_p),
+        ("input", C.c_void_p),
+        ("leaves", C.c_void_p),
+        ("nleaves", C.c_int32),
+        ("nqueries", C.c_int32),
+        ("queries", C.c_void_p),
+        ("dim", C.c_int32),
+        ("k", C.c_int32),
+        ("metric", C.c_int32),
+        ("overfetch", C.c_int32),
+        ("exact", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class VectorTopkStats(C.Structure):
+    _fields_ = [
+        ("reranked", C.c_int64),
+        ("exact_queries", C.c_int64),
+        ("max_score_error", C.c_double),
+        ("mean_score_error", C.c_double),
+    ]
+
+
 class VectorDistanceArgs(C.Structure):
     _fields_ = [
         ("input", C.c_void_p),
@@ -207,6 +233,9 @@ PROTOTYPES = {
     "oxb_aggregate": (_S, [_P, _P, C.POINTER(AggregateArgs), _PP]),
     "oxb_join_aggregate": (_S, [_P, _P, C.POINTER(JoinAggregateArgs), _PP]),
     "oxb_vector_distance": (_S, [_P, _P, C.POINTER(VectorDistanceArgs), _PP]),
+    "oxb_vector_index_build": (_S, [_P, _P, _P, C.c_int32, _PP]),
+    "oxb_vector_index_free": (None, [_P]),
+    "oxb_vector_topk": (_S, [_P, _P, C.POINTER(VectorTopkArgs), _P, _P, C.POINTER(VectorTopkStats)]),
     "oxb_set_kernel_timing": (_S, [_P, C.c_int32]),
     "oxb_last_kernel_time": (_S, [_P, C.c_char_p, C.c_int32, C.POINTER(C.c_float)]),
     "oxb_kernel_launches": (C.c_uint64, []),

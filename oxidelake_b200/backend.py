@@ -133,6 +133,19 @@ class DeviceJoinTable:
             _L().oxb_join_table_free(h)
 
 
+class VectorIndex:
+    """The BF16 copy of a vector column that vector_topk scans."""
+
+    def __init__(self, handle: int, input: "DeviceBatch"):
+        self.handle = handle
+        self._input = input
+
+    def __del__(self):
+        h, self.handle = getattr(self, "handle", None), None
+        if h:
+            _L().oxb_vector_index_free(h)
+
+
 class DeviceJoinMatches:
     """handles.rs:303: one probe batch's matches."""
 
@@ -500,6 +513,50 @@ class CudaBackend:
         return DeviceBatch(h.value, schema)
 
     # --- instrumentation ----------------------------------------------------------
+    def vector_index(self, stream: DeviceStream, input: DeviceBatch, column: int) -> "VectorIndex":
+        """A resident BF16 copy of a vector column for vector_topk (the batch
+        must outlive it)."""
+        h = C.c_void_p()
+        _abi.check(_L().oxb_vector_index_build(self.handle, stream.handle, input.handle, column, C.byref(h)))
+        return VectorIndex(h.value, input)
+
+    def vector_topk(
+        self,
+        stream: DeviceStream,
+        index: "VectorIndex",
+        input: DeviceBatch,
+        predicate: Optional[Predicate],
+        queries,
+        k: int,
+        metric: DistanceMetric,
+        overfetch: int = 0,
+        exact: bool = False,
+    ):
+        """ORDER BY distance, row LIMIT k per query over the rows `predicate`
+        keeps: (ids int64 [Q, k], dist float32 [Q, k], stats dict)."""
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32))
+        if q.ndim != 2:
+            raise Plan("queries must be a 2-D array")
+        lv, nl = _leaf_array(predicate)
+        nq, dim = q.shape
+        a = _abi.VectorTopkArgs(
+            index.handle, input.handle, C.cast(lv, C.c_void_p) if lv is not None else None, nl, nq,
+            q.ctypes.data, dim, k, int(metric), overfetch, 1 if exact else 0, 0,
+        )
+        ids = np.empty((max(nq, 1), k), np.int64)
+        dist = np.empty((max(nq, 1), k), np.float32)
+        st = _abi.VectorTopkStats()
+        _abi.check(
+            _L().oxb_vector_topk(self.handle, stream.handle, C.byref(a), ids.ctypes.data, dist.ctypes.data, C.byref(st))
+        )
+        stats = {
+            "reranked": st.reranked,
+            "exact_queries": st.exact_queries,
+            "max_score_error": st.max_score_error,
+            "mean_score_error": st.mean_score_error,
+        }
+        return ids[:nq], dist[:nq], stats
+
     def set_kernel_timing(self, enabled: bool) -> None:
         _abi.check(_L().oxb_set_kernel_timing(self.handle, 1 if enabled else 0))
 

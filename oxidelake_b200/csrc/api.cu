@@ -495,6 +495,26 @@ oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream, const o
     OXB_CATCH
 }
 
+oxb_status oxb_vector_index_build(oxb_backend* backend, oxb_stream* stream, const oxb_batch* input, int32_t column,
+                                  oxb_vector_index** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!input || !out) fail(OXB_PLAN, "null argument");
+    *out = vector_index_build(stream_of(stream), backend->b, *input, column);
+    OXB_CATCH
+}
+
+void oxb_vector_index_free(oxb_vector_index* index) { delete index; }
+
+oxb_status oxb_vector_topk(oxb_backend* backend, oxb_stream* stream, const oxb_vector_topk_args* args,
+                           int64_t* out_ids, float* out_dist, oxb_vector_topk_stats* stats) {
+    OXB_TRY
+    use_device(backend);
+    if (!args) fail(OXB_PLAN, "null argument");
+    vector_topk(stream_of(stream), backend->b, *args, out_ids, out_dist, stats);
+    OXB_CATCH
+}
+
 int32_t oxb_supports_predicate(const oxb_backend* backend, const oxb_leaf* leaves, int32_t nleaves) {
     (void)backend;
     if (nleaves < 0 || nleaves > OXB_MAX_PREDICATE_LEAVES) return 0;

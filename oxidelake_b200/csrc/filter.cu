@@ -244,6 +244,21 @@ oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter
     return out.release();
 }
 
+// The rows a predicate keeps as a bitmap of u32 words (bit r of word w: row
+// 32w + r), for operators that apply a WHERE inside their own kernels.
+AllocRef predicate_bits(const StreamRef& s, const Backend& b, const DevPredicate& pred, long long n) {
+    const long long ntiles = (n + kTileRows - 1) / kTileRows;
+    AllocRef mask = dev_alloc(s, (size_t)(ntiles * kWords + 1) * 4, true);
+    if (n > 0) {
+        Scratch<unsigned int> tile_counts(s, ntiles);
+        int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+        note_launch(), filter_mask_kernel<<<grid, kThreads, 0, s->stream>>>(pred, n, (unsigned int*)mask->ptr,
+                                                                          tile_counts.get(), ntiles);
+        OXB_CUDA(cudaGetLastError());
+    }
+    return mask;
+}
+
 // ---- filter + projection into caller buffers, with static scratch ----------
 //
 // The same three steps as filter_project, but nothing is allocated: the

@@ -3,6 +3,7 @@
 // layer (api.cu) dispatches to.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -165,6 +166,17 @@ struct JoinTableDev {
 
 }  // namespace oxb
 
+// A vector column prepared for the tensor-core top-k scan (topk.cu).
+struct oxb_vector_index {
+    oxb::Column vec;  // the FP32 vectors (shares the batch's memory)
+    long long n = 0;
+    int dim = 0;
+    int dp = 0;  // dim rounded up to 64
+    oxb::AllocRef bf16, norm2, inv;
+    float xmax = 0.0f;  // largest row norm
+    CUtensorMap xmap;
+};
+
 struct oxb_join_table {
     oxb::JoinTableDev t;
     oxb::AllocRef slots_mem, rows_mem;
@@ -214,6 +226,10 @@ bool key_range(const StreamRef& s, const Backend& b, const Column& key, long lon
 
 // Operators.
 oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a);
+AllocRef predicate_bits(const StreamRef& s, const Backend& b, const DevPredicate& pred, long long n);
+oxb_vector_index* vector_index_build(const StreamRef& s, const Backend& b, const oxb_batch& in, int column);
+void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_args& a, int64_t* out_ids,
+                 float* out_dist, oxb_vector_topk_stats* stats);
 void filter_project_noalloc(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a,
                             void* const* out_values, uint32_t* const* out_validity, long long capacity,
                             long long* out_rows);
