@@ -74,7 +74,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         msg = "\n".join(f"--- {s.name}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     if jobs or force or not LIB.exists():
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcuda"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objects)]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

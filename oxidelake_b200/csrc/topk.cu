@@ -36,13 +36,17 @@ namespace {
 constexpr int kQTile = 128;   // queries per CTA: the TMEM lanes
 constexpr int kRTile = 256;   // rows per tile: the MMA's N
 constexpr int kKBlock = 64;   // BF16 per k-block: one 128-byte swizzle span
-constexpr int kStages = 4;
+constexpr int kMaxStages = 4;
 constexpr int kABytes = kQTile * kKBlock * 2;  // 16 KB
 constexpr int kBBytes = kRTile * kKBlock * 2;  // 32 KB
 constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kScanThreads = 256;  // warp 0 TMA, warp 1 MMA, warps 4-7 epilogue
 constexpr int kTmemCols = 2 * kRTile;
-constexpr size_t kScanSmem = (size_t)kStages * kStageBytes + 1024 + 256;
+// Shared memory of the scan: the stage ring, the candidate buffers of the
+// 128 queries (C keys each, interleaved by query), the barriers.
+constexpr size_t scan_smem(int stages, int C) {
+    return (size_t)stages * kStageBytes + (size_t)C * kQTile * 8 + 1024 + 256;
+}
 constexpr int kPoolMax = 16384;  // merged candidates per query
 constexpr int kExactMax = 8192;  // re-ranked candidates per query
 constexpr int kFinalThreads = 256;
@@ -128,22 +132,23 @@ __host__ __device__ __forceinline__ unsigned f32_unorder(unsigned o) {
     return (o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o;
 }
 
-// Rearranges a[0, m) so a[0, L) are its L smallest keys (distinct keys);
-// returns the largest of them.
-__device__ unsigned long long select_smallest(unsigned long long* a, int m, int L) {
+// Rearranges the keys a[0], a[st], ..., a[(m - 1) st] so the first L are the
+// L smallest (keys are distinct); returns the largest of them.
+__device__ unsigned long long select_smallest(unsigned long long* base, int m, int L, int st) {
+    auto a = [&](int i) -> unsigned long long& { return base[(size_t)i * st]; };
     int lo = 0, hi = m - 1;
     const int kth = L - 1;
     while (lo < hi) {
-        unsigned long long x = a[lo], y = a[(lo + hi) >> 1], z = a[hi];
+        unsigned long long x = a(lo), y = a((lo + hi) >> 1), z = a(hi);
         unsigned long long pivot = x < y ? (y < z ? y : (x < z ? z : x)) : (x < z ? x : (y < z ? z : y));
         int i = lo, j = hi;
         while (i <= j) {
-            while (a[i] < pivot) i++;
-            while (a[j] > pivot) j--;
+            while (a(i) < pivot) i++;
+            while (a(j) > pivot) j--;
             if (i <= j) {
-                unsigned long long t = a[i];
-                a[i] = a[j];
-                a[j] = t;
+                unsigned long long t = a(i);
+                a(i) = a(j);
+                a(j) = t;
                 i++;
                 j--;
             }
@@ -153,7 +158,7 @@ __device__ unsigned long long select_smallest(unsigned long long* a, int m, int 
         else break;
     }
     unsigned long long mx = 0;
-    for (int i = 0; i < L; i++) mx = a[i] > mx ? a[i] : mx;
+    for (int i = 0; i < L; i++) mx = a(i) > mx ? a(i) : mx;
     return mx;
 }
 
@@ -163,13 +168,14 @@ struct ScanParams {
     int groups;   // padded queries / 128
     int nq;
     int metric;
-    int L;    // candidates kept per (CTA, query)
-    int cap;  // buffer length, 2L
+    int L;       // candidates kept per (CTA, query)
+    int C;       // shared-memory buffer per query, >= L + 32
+    int stages;  // stage ring depth
     const unsigned* sel;        // rows the WHERE keeps (bit per row), null = all
     const uint8_t* valid;       // vector validity, null = all
     const float* norm2;         // per row ||x||^2
     const float* inv;           // per row 1 / ||x||
-    unsigned long long* lists;  // [grid * 128][cap]
+    unsigned long long* lists;  // [grid * 128][L]
     unsigned* counts;           // [grid * 128]
     unsigned long long* bounds; // [grid * 128]: every row missing from the list has a larger key
     unsigned* status;
@@ -180,12 +186,14 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                                                                     const __grid_constant__ ScanParams p) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
-    unsigned long long* bars = (unsigned long long*)(smem + (size_t)kStages * kStageBytes);
+    const int stages = p.stages;
+    unsigned long long* cands = (unsigned long long*)(smem + (size_t)stages * kStageBytes);
+    unsigned long long* bars = cands + (size_t)p.C * kQTile;
     unsigned long long* full = bars;
-    unsigned long long* empty = bars + kStages;
-    unsigned long long* tfull = bars + 2 * kStages;
-    unsigned long long* tempty = bars + 2 * kStages + 2;
-    unsigned* tmem_slot = (unsigned*)(bars + 2 * kStages + 4);
+    unsigned long long* empty = bars + kMaxStages;
+    unsigned long long* tfull = bars + 2 * kMaxStages;
+    unsigned long long* tempty = bars + 2 * kMaxStages + 2;
+    unsigned* tmem_slot = (unsigned*)(bars + 2 * kMaxStages + 4);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x % p.groups;
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
     const long long ntiles = (p.n + kRTile - 1) / kRTile;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < stages; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -224,7 +232,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                     mbar_arrive_expect_tx(&full[s], kStageBytes);
                     tma_load_2d(st, &qmap, kb * kKBlock, g * kQTile, &full[s]);
                     tma_load_2d(st + kABytes, &xmap, kb * kKBlock, (int)(t * kRTile), &full[s]);
-                    if (++s == kStages) {
+                    if (++s == stages) {
                         s = 0;
                         ph ^= 1u;
                     }
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                     for (int k = 0; k < kKBlock / 16; k++)  // 32 bytes of K per instruction
                         umma_bf16(d, ad + 2ull * k, bd + 2ull * k, (kb | k) != 0);
                     umma_commit(&empty[s]);
-                    if (++s == kStages) {
+                    if (++s == stages) {
                         s = 0;
                         ph ^= 1u;
                     }
@@ -275,7 +283,8 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
         const int ql = qw * 32 + lane;
         const int q = g * kQTile + ql;
         const bool active = q < p.nq;
-        unsigned long long* list = p.lists + ((size_t)blockIdx.x * kQTile + ql) * p.cap;
+        // This query's keys: entry i at sb[i * 128] (lanes side by side).
+        unsigned long long* sb = cands + ql;
         unsigned long long thr = kNoKey;
         int cnt = 0;
         bool dropped = false;
@@ -291,6 +300,13 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                 unsigned r[32];
                 __syncwarp();
                 tmem_ld32(tmem + ((unsigned)(qw * 32) << 16) + (unsigned)(buf * kRTile + c * 32), r);
+                // Room for 32 more keys in every buffer: when one is nearly
+                // full, the warp's lanes compact theirs together.
+                if (__any_sync(0xffffffffu, cnt > p.C - 32) && cnt > p.L) {
+                    thr = select_smallest(sb, cnt, p.L, kQTile);
+                    cnt = p.L;
+                    dropped = true;
+                }
                 const long long row0 = t * kRTile + c * 32;
                 if (!active || row0 >= p.n) continue;
                 unsigned sel = p.sel ? __ldg(p.sel + (row0 >> 5)) : ~0u;
@@ -312,13 +328,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                     const float sc = p.metric == 0 ? fmaf(-2.0f, dot, __ldg(nrm + j)) : -dot * __ldg(nrm + j);
                     const unsigned o = sc == sc ? f32_order(__float_as_uint(sc)) : 0xFFFFFFFFu;
                     const unsigned long long key = ((unsigned long long)o << 32) | (unsigned)(row0 + j);
-                    if (key >= thr) continue;
-                    list[cnt++] = key;
-                    if (cnt == p.cap) {
-                        thr = select_smallest(list, cnt, p.L);
-                        cnt = p.L;
-                        dropped = true;
-                    }
+                    if (key < thr) sb[(size_t)(cnt++) * kQTile] = key;
                 }
             }
             tc_fence_before();
@@ -329,11 +339,14 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
             }
         }
         if (cnt > p.L) {
-            thr = select_smallest(list, cnt, p.L);
+            thr = select_smallest(sb, cnt, p.L, kQTile);
             cnt = p.L;
             dropped = true;
         }
-        p.counts[(size_t)blockIdx.x * kQTile + ql] = active ? (unsigned)cnt : 0u;
+        if (!active) cnt = 0;
+        unsigned long long* out = p.lists + ((size_t)blockIdx.x * kQTile + ql) * p.L;
+        for (int i = 0; i < cnt; i++) out[i] = sb[(size_t)i * kQTile];
+        p.counts[(size_t)blockIdx.x * kQTile + ql] = (unsigned)cnt;
         p.bounds[(size_t)blockIdx.x * kQTile + ql] = dropped ? thr : kNoKey;
     }
     tc_fence_before();
@@ -345,16 +358,17 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
     }
 }
 
-// The reference's FP32 distance of one row (cpu/kernels.rs:909-927): folded
-// in index order from -0.0, one correctly rounded operation per step.
-__device__ float exact_distance(const float* x, const float* q, int dim, int metric, float qnorm) {
+// The bits of the reference's FP32 distance of one row
+// (cpu/kernels.rs:909-927): folded in index order from -0.0, one correctly
+// rounded operation per step; a zero norm gives the NaN 0x7fc00000.
+__device__ unsigned exact_distance_bits(const float* x, const float* q, int dim, int metric, float qnorm) {
     if (metric == 0) {
         float s = -0.0f;
         for (int i = 0; i < dim; i++) {
             const float d = __fsub_rn(__ldg(x + i), q[i]);
             s = __fadd_rn(s, __fmul_rn(d, d));
         }
-        return __fsqrt_rn(s);
+        return __float_as_uint(__fsqrt_rn(s));
     }
     float s0 = -0.0f, s1 = -0.0f;
     for (int i = 0; i < dim; i++) {
@@ -363,8 +377,8 @@ __device__ float exact_distance(const float* x, const float* q, int dim, int met
         s1 = __fadd_rn(s1, __fmul_rn(a, a));
     }
     const float na = __fsqrt_rn(s1);
-    if (na == 0.0f || qnorm == 0.0f) return __int_as_float(0x7fc00000);
-    return __fsub_rn(1.0f, __fdiv_rn(s0, __fmul_rn(na, qnorm)));
+    if (na == 0.0f || qnorm == 0.0f) return 0x7fc00000u;
+    return __float_as_uint(__fsub_rn(1.0f, __fdiv_rn(s0, __fmul_rn(na, qnorm))));
 }
 
 // Ascending bitonic sort of a[0, m), m a power of two, by the whole block.
@@ -470,8 +484,8 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
         for (int i = done + threadIdx.x; i < R; i += blockDim.x) {
             const unsigned row = (unsigned)(pool[i] & 0xFFFFFFFFu);
             const float* x = p.table + (size_t)row * p.dim;
-            const float d = exact_distance(x, qv, p.dim, p.metric, qn);
-            ex[i] = ((unsigned long long)f32_order(__float_as_uint(d)) << 32) | row;
+            const unsigned d = exact_distance_bits(x, qv, p.dim, p.metric, qn);
+            ex[i] = ((unsigned long long)f32_order(d) << 32) | row;
             // The BF16 score against the FP64 one, for the report.
             double dot = 0.0, xx = 0.0;
             for (int t = 0; t < p.dim; t++) {
@@ -527,8 +541,7 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
         for (int j = threadIdx.x; j < p.k; j += blockDim.x) {
             const unsigned long long e = j < R ? ex[j] : kNoKey;
             p.ids[(size_t)q * p.k + j] = e == kNoKey ? -1 : (long long)(e & 0xFFFFFFFFu);
-            p.dist[(size_t)q * p.k + j] =
-                e == kNoKey ? __int_as_float(0x7fc00000) : __uint_as_float(f32_unorder((unsigned)(e >> 32)));
+            ((unsigned*)p.dist)[(size_t)q * p.k + j] = e == kNoKey ? 0x7fc00000u : f32_unorder((unsigned)(e >> 32));
         }
     }
     if (ecount) {
@@ -545,8 +558,9 @@ __global__ void topk_exact_keys_kernel(const float* __restrict__ d, const unsign
                                        unsigned long long* __restrict__ keys) {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
         const bool ok = (!sel || ((__ldg(sel + (r >> 5)) >> (r & 31)) & 1u)) && valid_at(valid, r);
-        keys[r] = ok ? ((unsigned long long)f32_order(__float_as_uint(__ldg(d + r))) << 32) | (unsigned long long)r
-                     : kNoKey;
+        // The distance's bits, loaded as an integer: a NaN keeps its bits.
+        const unsigned bits = __ldg((const unsigned*)d + r);
+        keys[r] = ok ? ((unsigned long long)f32_order(bits) << 32) | (unsigned long long)r : kNoKey;
     }
 }
 
@@ -555,7 +569,7 @@ __global__ void topk_exact_out_kernel(const unsigned long long* __restrict__ key
     for (int j = threadIdx.x; j < k; j += blockDim.x) {
         const unsigned long long e = j < n ? keys[j] : kNoKey;
         ids[j] = e == kNoKey ? -1 : (long long)(e & 0xFFFFFFFFu);
-        dist[j] = e == kNoKey ? __int_as_float(0x7fc00000) : __uint_as_float(f32_unorder((unsigned)(e >> 32)));
+        ((unsigned*)dist)[j] = e == kNoKey ? 0x7fc00000u : f32_unorder((unsigned)(e >> 32));
     }
 }
 
@@ -598,12 +612,32 @@ __global__ void query_prep_kernel(const float* __restrict__ q, int nq, int dim, 
     }
 }
 
+// cuTensorMapEncodeTiled, found through the runtime so the library itself
+// does not link the driver library.
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+    static std::mutex mu;
+    static EncodeTiled fn = nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        OXB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(OXB_DEVICE, "cuTensorMapEncodeTiled is not available");
+        fn = (EncodeTiled)p;
+    }
+    return fn;
+}
+
 void encode_bf16_map(CUtensorMap* map, const void* base, long long rows, int dp, int box_rows) {
     cuuint64_t dims[2] = {(cuuint64_t)dp, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)dp * 2};
     cuuint32_t box[2] = {(cuuint32_t)kKBlock, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+    CUresult r = encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
                                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -687,11 +721,25 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     int cpg = b.sms / groups;
     if (cpg < 1) cpg = 1;
     const int grid = cpg * groups;
-    int L = std::min(over * k, kPoolMax / cpg);
-    const bool fast = !a.exact && n > 0 && L >= k;
+    // Candidates kept per (CTA, query) and the shared memory they take: the
+    // deepest stage ring (2..4) that leaves room for buffers of C keys.
+    int L = std::max(1, std::min(over * k, kPoolMax / cpg));
+    int C = 0, stages = 0;
+    for (; L >= 1; L = L * 3 / 4) {
+        for (int c : {std::max(2 * L, L + 32), L + 32}) {
+            for (stages = kMaxStages; stages >= 2 && scan_smem(stages, c) > b.smem_optin; stages--) {
+            }
+            if (stages >= 2) {
+                C = c;
+                break;
+            }
+        }
+        if (C) break;
+    }
+    const bool fast = !a.exact && n > 0 && C > 0;
     std::vector<int> host_fb(nq, 1);
     if (fast) {
-        const int cap = 2 * L;
+        const int cap = L;
         Scratch<unsigned long long> lists(s, (size_t)grid * kQTile * cap);
         Scratch<unsigned> counts(s, (size_t)grid * kQTile);
         Scratch<unsigned long long> bounds(s, (size_t)grid * kQTile);
@@ -705,7 +753,8 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.nq = nq;
         sp.metric = a.metric;
         sp.L = L;
-        sp.cap = cap;
+        sp.C = C;
+        sp.stages = stages;
         sp.sel = selp;
         sp.valid = ix.vec.validity;
         sp.norm2 = (const float*)ix.norm2->ptr;
@@ -714,11 +763,12 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.counts = counts.get();
         sp.bounds = bounds.get();
         sp.status = status.get();
-        OXB_CUDA(cudaFuncSetAttribute(topk_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScanSmem));
+        const size_t smem = scan_smem(stages, C);
+        OXB_CUDA(cudaFuncSetAttribute(topk_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         {
             KernelTimer timer(b, s, "topk_scan_kernel");
             timer.begin();
-            note_launch(), topk_scan_kernel<<<grid, kScanThreads, kScanSmem, s->stream>>>(qmap, ix.xmap, sp);
+            note_launch(), topk_scan_kernel<<<grid, kScanThreads, smem, s->stream>>>(qmap, ix.xmap, sp);
             timer.end();
             OXB_CUDA(cudaGetLastError());
         }
