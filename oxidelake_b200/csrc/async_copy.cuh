@@ -44,10 +44,12 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Waits for the barrier phase with the given parity to complete; false when
 // the bounded wait gave up.
+// try_wait itself suspends the thread for a while, so a pipeline's waits
+// spin on it; only a wait that has gone on for many polls backs off.
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
     for (long long i = 0; i < kWaitLimit; i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
+        if (i > (1 << 14)) __nanosleep(32);
     }
     return false;
 }

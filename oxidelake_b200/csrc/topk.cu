@@ -43,9 +43,11 @@ constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kScanThreads = 256;  // warp 0 TMA, warp 1 MMA, warps 4-7 epilogue
 constexpr int kTmemCols = 2 * kRTile;
 // Shared memory of the scan: the stage ring, the candidate buffers of the
-// 128 queries (C keys each, interleaved by query), the barriers.
+// 128 queries (C keys each, interleaved by query), two tiles' row norms and
+// selection words for the epilogue, the barriers, and alignment slack.
+constexpr size_t kTileAux = (size_t)kRTile * 4 + (kRTile / 32) * 4;  // norms + selection words
 constexpr size_t scan_smem(int stages, int C) {
-    return (size_t)stages * kStageBytes + (size_t)C * kQTile * 8 + 1024 + 256;
+    return (size_t)stages * kStageBytes + (size_t)C * kQTile * 8 + 2 * kTileAux + 128 + 1024;
 }
 constexpr int kPoolMax = 16384;  // merged candidates per query
 constexpr int kExactMax = 8192;  // re-ranked candidates per query
@@ -188,7 +190,9 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
     unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
     const int stages = p.stages;
     unsigned long long* cands = (unsigned long long*)(smem + (size_t)stages * kStageBytes);
-    unsigned long long* bars = cands + (size_t)p.C * kQTile;
+    float* tnorm = (float*)(cands + (size_t)p.C * kQTile);     // [2][256]
+    unsigned* tsel = (unsigned*)(tnorm + 2 * kRTile);            // [2][8]
+    unsigned long long* bars = (unsigned long long*)(tsel + 2 * (kRTile / 32));
     unsigned long long* full = bars;
     unsigned long long* empty = bars + kMaxStages;
     unsigned long long* tfull = bars + 2 * kMaxStages;
@@ -290,12 +294,57 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
         bool dropped = false;
         int buf = 0;
         unsigned tph = 0;
-        for (long long t = ci; t < ntiles; t += cpg) {
-            if (!mbar_wait(&tfull[buf], tph)) {
-                atomicOr(p.status, kStatusTimeout);
+        const float* nsrc = p.metric == 0 ? p.norm2 : p.inv;
+        int par = 0;
+        for (long long t = ci; t < ntiles; t += cpg, par ^= 1) {
+            // The four epilogue warps stage this tile's row norms and
+            // selection words (WHERE, validity, rows past n) once for all
+            // 128 queries; two buffers, so a warp one tile ahead cannot
+            // overwrite what a slower one still reads.
+            {
+                float* tn = tnorm + par * kRTile;
+                for (int h = 0; h < kRTile / kQTile; h++) {
+                    const long long r = t * kRTile + h * kQTile + ql;
+                    tn[h * kQTile + ql] = r < p.n ? __ldg(nsrc + r) : 0.0f;
+                }
+                if (ql < kRTile / 32) {
+                    const long long row0 = t * kRTile + ql * 32;
+                    unsigned sel = 0;
+                    if (row0 < p.n) {
+                        sel = p.sel ? __ldg(p.sel + (row0 >> 5)) : ~0u;
+                        if (p.valid) {
+                            // The bitmap's bytes for these 32 rows, none past its end.
+                            const long long b0 = row0 >> 3, nbytes = (p.n + 7) >> 3;
+                            unsigned v = 0;
+#pragma unroll
+                            for (int bi = 0; bi < 4; bi++)
+                                if (b0 + bi < nbytes) v |= (unsigned)__ldg(p.valid + b0 + bi) << (8 * bi);
+                            sel &= v;
+                        }
+                        if (row0 + 32 > p.n) sel &= (1u << (p.n - row0)) - 1u;
+                    }
+                    tsel[par * (kRTile / 32) + ql] = sel;
+                }
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+            }
+            // Every epilogue thread leaves together if any wait gave up, so
+            // none is left at the next named barrier.
+            const bool ok = mbar_wait(&tfull[buf], tph);
+            unsigned any_fail;
+            asm volatile(
+                "{\n\t.reg .pred p, q;\n\t"
+                "setp.eq.u32 p, %1, 0;\n\t"
+                "bar.red.or.pred q, 2, 128, p;\n\t"
+                "selp.u32 %0, 1, 0, q;\n\t}"
+                : "=r"(any_fail)
+                : "r"((unsigned)ok)
+                : "memory");
+            if (any_fail) {
+                if (!ok) atomicOr(p.status, kStatusTimeout);
                 break;
             }
             tc_fence_after();
+            const float* tn = tnorm + par * kRTile;
             for (int c = 0; c < kRTile / 32; c++) {
                 unsigned r[32];
                 __syncwarp();
@@ -307,28 +356,17 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                     cnt = p.L;
                     dropped = true;
                 }
-                const long long row0 = t * kRTile + c * 32;
-                if (!active || row0 >= p.n) continue;
-                unsigned sel = p.sel ? __ldg(p.sel + (row0 >> 5)) : ~0u;
-                if (p.valid) {
-                    // The bitmap's bytes for these 32 rows, none past its end.
-                    const long long b0 = row0 >> 3, nbytes = (p.n + 7) >> 3;
-                    unsigned v = 0;
-#pragma unroll
-                    for (int bi = 0; bi < 4; bi++)
-                        if (b0 + bi < nbytes) v |= (unsigned)__ldg(p.valid + b0 + bi) << (8 * bi);
-                    sel &= v;
-                }
-                if (row0 + 32 > p.n) sel &= (1u << (p.n - row0)) - 1u;
-                const float* nrm = (p.metric == 0 ? p.norm2 : p.inv) + row0;
+                const unsigned sel = tsel[par * (kRTile / 32) + c];
+                if (!active || !sel) continue;
+                const unsigned row0 = (unsigned)(t * kRTile + c * 32);
 #pragma unroll
                 for (int j = 0; j < 32; j++) {
-                    if (!((sel >> j) & 1u)) continue;
                     const float dot = __uint_as_float(r[j]);
-                    const float sc = p.metric == 0 ? fmaf(-2.0f, dot, __ldg(nrm + j)) : -dot * __ldg(nrm + j);
+                    const float nr = tn[c * 32 + j];
+                    const float sc = p.metric == 0 ? fmaf(-2.0f, dot, nr) : -dot * nr;
                     const unsigned o = sc == sc ? f32_order(__float_as_uint(sc)) : 0xFFFFFFFFu;
-                    const unsigned long long key = ((unsigned long long)o << 32) | (unsigned)(row0 + j);
-                    if (key < thr) sb[(size_t)(cnt++) * kQTile] = key;
+                    const unsigned long long key = ((unsigned long long)o << 32) | (row0 + j);
+                    if (((sel >> j) & 1u) && key < thr) sb[(size_t)(cnt++) * kQTile] = key;
                 }
             }
             tc_fence_before();
@@ -721,16 +759,19 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     int cpg = b.sms / groups;
     if (cpg < 1) cpg = 1;
     const int grid = cpg * groups;
-    // Candidates kept per (CTA, query) and the shared memory they take: the
-    // deepest stage ring (2..4) that leaves room for buffers of C keys.
-    int L = std::max(1, std::min(over * k, kPoolMax / cpg));
+    // Candidates kept per (CTA, query): enough that each CTA's bound sits far
+    // below the k-th distance (the over-fetch of 4k is taken from the merged
+    // lists), and buffers with room for them plus a 32-key chunk plus slack,
+    // so a compaction frees many slots; the deepest stage ring that fits.
+    int L = std::max(1, std::min({std::max(2 * k, k + 16), over * k, kPoolMax / cpg}));
     int C = 0, stages = 0;
-    for (; L >= 1; L = L * 3 / 4) {
-        for (int c : {std::max(2 * L, L + 32), L + 32}) {
-            for (stages = kMaxStages; stages >= 2 && scan_smem(stages, c) > b.smem_optin; stages--) {
-            }
-            if (stages >= 2) {
-                C = c;
+    for (; L >= 1 && !C; L = L * 3 / 4) {
+        for (stages = kMaxStages; stages >= 2; stages--) {
+            const size_t fixed = scan_smem(stages, 0);
+            if (fixed >= b.smem_optin) continue;
+            const int cmax = (int)((b.smem_optin - fixed) / ((size_t)kQTile * 8));
+            if (cmax >= L + 32 + std::min(L, 16)) {
+                C = std::min(cmax, 2 * L + 32);
                 break;
             }
         }
