@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
         // This query's keys: entry i at sb[i * 128] (lanes side by side).
         unsigned long long* sb = cands + ql;
         unsigned long long thr = kNoKey;
+        float thr_f = INFINITY;  // the score part of thr (+inf while the list has room)
         int cnt = 0;
         bool dropped = false;
         int buf = 0;
@@ -353,20 +354,40 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                 // full, the warp's lanes compact theirs together.
                 if (__any_sync(0xffffffffu, cnt > p.C - 32) && cnt > p.L) {
                     thr = select_smallest(sb, cnt, p.L, kQTile);
+                    thr_f = __uint_as_float(f32_unorder((unsigned)(thr >> 32)));
                     cnt = p.L;
                     dropped = true;
                 }
                 const unsigned sel = tsel[par * (kRTile / 32) + c];
                 if (!active || !sel) continue;
                 const unsigned row0 = (unsigned)(t * kRTile + c * 32);
+                // Scores (a NaN counts as +inf, after every finite score) and
+                // their minimum over the selected rows; only a chunk whose
+                // minimum reaches the threshold is looked at row by row.
+                float sc[32];
+                float mn = INFINITY;
+                const float4* tn4 = (const float4*)(tn + c * 32);
+#pragma unroll
+                for (int j4 = 0; j4 < 8; j4++) {
+                    const float4 nr = tn4[j4];
+                    const float nv[4] = {nr.x, nr.y, nr.z, nr.w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int j = j4 * 4 + u;
+                        const float dot = __uint_as_float(r[j]);
+                        float x = p.metric == 0 ? fmaf(-2.0f, dot, nv[u]) : -dot * nv[u];
+                        x = x == x ? x : INFINITY;
+                        sc[j] = x;
+                        mn = fminf(mn, ((sel >> j) & 1u) ? x : INFINITY);
+                    }
+                }
+                if (!(mn <= thr_f)) continue;
 #pragma unroll
                 for (int j = 0; j < 32; j++) {
-                    const float dot = __uint_as_float(r[j]);
-                    const float nr = tn[c * 32 + j];
-                    const float sc = p.metric == 0 ? fmaf(-2.0f, dot, nr) : -dot * nr;
-                    const unsigned o = sc == sc ? f32_order(__float_as_uint(sc)) : 0xFFFFFFFFu;
-                    const unsigned long long key = ((unsigned long long)o << 32) | (row0 + j);
-                    if (((sel >> j) & 1u) && key < thr) sb[(size_t)(cnt++) * kQTile] = key;
+                    if (!((sel >> j) & 1u) || !(sc[j] <= thr_f)) continue;
+                    const unsigned long long key =
+                        ((unsigned long long)f32_order(__float_as_uint(sc[j])) << 32) | (row0 + j);
+                    if (key < thr) sb[(size_t)(cnt++) * kQTile] = key;
                 }
             }
             tc_fence_before();
