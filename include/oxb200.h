@@ -337,6 +337,25 @@ typedef struct oxb_aggregate_args {
 OXB_API oxb_status oxb_aggregate(oxb_backend* backend, oxb_stream* stream,
                          const oxb_aggregate_args* args, oxb_batch** out);
 
+/* Every RecordBatch of one GpuAggregateExec input partition folded into one
+ * result (compute/src/exec/aggregate.rs:35-321 emits one batch at the end
+ * of the stream; the reference merges per-batch device partials on the host,
+ * operator.rs:994-1075).  The batches share a schema and may differ in row
+ * count; one persistent launch takes their rows from one work queue into
+ * one table sized by a distinct-count estimate of the keys.  Same output as
+ * oxb_aggregate over the batches' concatenation. */
+typedef struct oxb_aggregate_batches_args {
+    const oxb_batch* const* inputs;
+    int32_t ninputs;
+    int32_t reserved;
+    const oxb_aggregate_spec* spec;
+    const oxb_leaf* leaves; /* WHERE over each batch, NULL/0 = every row */
+    int32_t nleaves;
+    int32_t reserved2;
+} oxb_aggregate_batches_args;
+OXB_API oxb_status oxb_aggregate_batches(oxb_backend* backend, oxb_stream* stream,
+                                         const oxb_aggregate_batches_args* args, oxb_batch** out);
+
 /* ORDER BY l2|cosine(vector, query) LIMIT k over the rows a WHERE keeps, for
  * a batch of queries: the reference's GpuVectorDistanceExec followed by its
  * CPU SortExec(fetch = k) (compute/src/exec/vector.rs:29-249,

@@ -125,6 +125,18 @@ class AggregateArgs(C.Structure):
     ]
 
 
+class AggregateBatchesArgs(C.Structure):
+    _fields_ = [
+        ("inputs", C.c_void_p),
+        ("ninputs", C.c_int32),
+        ("reserved", C.c_int32),
+        ("spec", C.c_void_p),
+        ("leaves", C.c_void_p),
+        ("nleaves", C.c_int32),
+        ("reserved2", C.c_int32),
+    ]
+
+
 class VectorTopkArgs(C.Structure):
     _fields_ = [
         ("index", C.c_void_p),
@@ -233,6 +245,7 @@ PROTOTYPES = {
     "oxb_aggregate": (_S, [_P, _P, C.POINTER(AggregateArgs), _PP]),
     "oxb_join_aggregate": (_S, [_P, _P, C.POINTER(JoinAggregateArgs), _PP]),
     "oxb_vector_distance": (_S, [_P, _P, C.POINTER(VectorDistanceArgs), _PP]),
+    "oxb_aggregate_batches": (_S, [_P, _P, C.POINTER(AggregateBatchesArgs), _PP]),
     "oxb_vector_index_build": (_S, [_P, _P, _P, C.c_int32, _PP]),
     "oxb_vector_index_free": (None, [_P]),
     "oxb_vector_topk": (_S, [_P, _P, C.POINTER(VectorTopkArgs), _P, _P, C.POINTER(VectorTopkStats)]),

@@ -445,6 +445,35 @@ class CudaBackend:
         _abi.check(_L().oxb_aggregate(self.handle, stream.handle, C.byref(a), C.byref(h)))
         return DeviceBatch(h.value, aggregate_output_schema(input.schema, spec))
 
+    def aggregate_batches(
+        self,
+        stream: DeviceStream,
+        inputs: Sequence[DeviceBatch],
+        spec: AggregateSpec,
+        predicate: Optional[Predicate] = None,
+    ) -> DeviceBatch:
+        """Every batch of one input partition folded into one result in one
+        persistent launch (GpuAggregateExec, compute/src/exec/aggregate.rs)."""
+        if not inputs:
+            raise Plan("no input batches")
+        if len(spec.aggregates) > _abi.OXB_MAX_AGGREGATES:
+            raise Unsupported("too many aggregates")
+        cs = _abi.AggregateSpecC()
+        cs.group_by = spec.group_by
+        cs.naggregates = len(spec.aggregates)
+        for j, (f, c) in enumerate(spec.aggregates):
+            cs.funcs[j] = int(f)
+            cs.columns[j] = int(c)
+        lv, nl = _leaf_array(predicate)
+        handles = (C.c_void_p * len(inputs))(*[b.handle for b in inputs])
+        a = _abi.AggregateBatchesArgs(
+            C.cast(handles, C.c_void_p), len(inputs), 0, C.cast(C.pointer(cs), C.c_void_p),
+            C.cast(lv, C.c_void_p) if lv is not None else None, nl, 0,
+        )
+        h = C.c_void_p()
+        _abi.check(_L().oxb_aggregate_batches(self.handle, stream.handle, C.byref(a), C.byref(h)))
+        return DeviceBatch(h.value, aggregate_output_schema(inputs[0].schema, spec))
+
     def join_aggregate(
         self,
         stream: DeviceStream,

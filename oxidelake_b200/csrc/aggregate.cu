@@ -2298,10 +2298,12 @@ unsigned int next_pow2(long long v, long long floor_v) {
 struct AggInputCol {
     const Column* col;
     int side;
+    int index = -1;  // the column's index when it names a column of many batches
 };
 
 struct AggPlan {
     AggProgram P{};
+    int acc_index[kMaxAccs];  // each accumulator's column index (-1 when not given)
     std::vector<int> out_types;
     int key_type = kInt64;
 };
@@ -2318,12 +2320,16 @@ AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInput
         return na++;
     };
     // Accumulators are shared by every aggregate that needs the same one.
-    auto acc_for = [&](int kind, const Column* c, int side) -> int {
-        for (int j = 0; j < P.nacc; j++)
-            if (P.acc[j].kind == kind && P.acc[j].values == c->values && P.acc[j].side == side &&
-                P.acc[j].validity == c->validity && P.acc[j].in_type == c->type)
+    // By column index when given (batches whose buffers differ), else by buffer.
+    auto acc_for = [&](int kind, const Column* c, int side, int index) -> int {
+        for (int j = 0; j < P.nacc; j++) {
+            const bool same = index >= 0 ? plan.acc_index[j] == index
+                                         : P.acc[j].values == c->values && P.acc[j].validity == c->validity;
+            if (P.acc[j].kind == kind && same && P.acc[j].side == side && P.acc[j].in_type == c->type)
                 return P.acc[j].arr;
+        }
         if (P.nacc == kMaxAccs) fail(OXB_UNSUPPORTED, "too many distinct aggregate inputs");
+        plan.acc_index[P.nacc] = index;
         DevAcc& a = P.acc[P.nacc++];
         a.values = c->values;
         a.validity = c->validity;
@@ -2349,7 +2355,8 @@ AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInput
         const int side = inputs[j].side;
         o.in_type = c ? c->type : kInt64;
         // Rows with a non-NULL input: the group's rows when the column has no bitmap.
-        auto nn = [&]() { return c && c->validity ? acc_for(kAccCount, c, side) : 0; };
+        const int index = inputs[j].index;
+        auto nn = [&]() { return c && c->validity ? acc_for(kAccCount, c, side, index) : 0; };
         int out_type = kInt64;
         switch (o.func) {
             case OXB_AGG_COUNT_STAR:
@@ -2361,22 +2368,22 @@ AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInput
                 o.nn = 0;
                 break;
             case OXB_AGG_SUM:
-                o.arr = acc_for(o.in_type == kFloat64 ? kAccSumF64 : kAccSumInt, c, side);
+                o.arr = acc_for(o.in_type == kFloat64 ? kAccSumF64 : kAccSumInt, c, side, index);
                 o.nn = nn();
                 out_type = o.in_type == kFloat64 ? kFloat64 : kInt64;
                 break;
             case OXB_AGG_AVG:
-                o.arr = acc_for(kAccSumF64, c, side);
+                o.arr = acc_for(kAccSumF64, c, side, index);
                 o.nn = nn();
                 out_type = kFloat64;
                 break;
             case OXB_AGG_MIN:
-                o.arr = acc_for(kAccMin, c, side);
+                o.arr = acc_for(kAccMin, c, side, index);
                 o.nn = nn();
                 out_type = o.in_type;
                 break;
             case OXB_AGG_MAX:
-                o.arr = acc_for(kAccMax, c, side);
+                o.arr = acc_for(kAccMax, c, side, index);
                 o.nn = nn();
                 out_type = o.in_type;
                 break;
@@ -2478,6 +2485,132 @@ bool plan_stream(const AggProgram& P, const DevPredicate& pred, const void* key_
     return true;
 }
 
+
+// ---- many batches, one persistent launch ----------------------------------
+//
+// GpuAggregateExec folds every RecordBatch of a partition into one result
+// (compute/src/exec/aggregate.rs:35-321); the reference runs one device
+// aggregate per batch and merges on the host.  Here every batch's columns
+// are described once in HBM and a persistent kernel takes 1024-row tiles of
+// all batches from one work queue (uneven batch sizes cost nothing extra),
+// folding into one HBM table sized from a HyperLogLog count of the keys.
+
+struct BatchCols {
+    long long n;      // rows
+    long long tile0;  // the batch's first tile in the queue
+    const void* key;
+    const uint8_t* key_valid;
+    const void* vals[kMaxAccs];
+    const uint8_t* valid[kMaxAccs];
+    const void* lvals[kMaxLeaves];
+    const uint8_t* lvalid[kMaxLeaves];
+};
+
+constexpr int kBatchTile = 1024;
+
+template <int MAXACC>
+__global__ void __launch_bounds__(kThreads) agg_batches_kernel(const __grid_constant__ AggProgram P,
+                                                               const __grid_constant__ DevPredicate pred, int key_type,
+                                                               const BatchCols* __restrict__ batches, int nb,
+                                                               long long ntiles,
+                                                               unsigned long long* __restrict__ queue) {
+    __shared__ long long s_tile;
+    __shared__ int s_b;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const long long t = (long long)atomicAdd(queue, 1ull);
+            int lo = 0, hi = nb - 1;  // the last batch whose first tile is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (batches[mid].tile0 <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_tile = t;
+            s_b = lo;
+        }
+        __syncthreads();
+        const long long t = s_tile;
+        if (t >= ntiles) break;
+        const BatchCols& B = batches[s_b];
+        const long long base = (t - B.tile0) * kBatchTile;
+        for (int i = threadIdx.x; i < kBatchTile; i += blockDim.x) {
+            const long long r = base + i;
+            if (r >= B.n) break;
+            bool keep = true;
+            for (int l = 0; l < pred.nleaves; l++) {
+                const DevLeaf& lf = pred.leaves[l];
+                if (!valid_at(B.lvalid[l], r)) {
+                    keep = false;
+                    break;
+                }
+                const long long a = lf.type == kFloat64 ? filter_order_key(__ldg((const double*)B.lvals[l] + r))
+                                    : lf.type == kInt64 ? __ldg((const long long*)B.lvals[l] + r)
+                                                        : (long long)__ldg((const int*)B.lvals[l] + r);
+                if (!cmp_holds(lf.op, a, lf.lit)) {
+                    keep = false;
+                    break;
+                }
+            }
+            if (!keep) continue;
+            const bool kv = valid_at(B.key_valid, r);
+            const long long key = kv ? load_int(B.key, key_type, r) : 0;
+            const long long g = global_slot(P, kv, key);
+            if (g < 0) continue;
+            unsigned long long val[MAXACC];
+            double comp[MAXACC];
+#pragma unroll
+            for (int j = 0; j < MAXACC; j++) {
+                comp[j] = 0.0;
+                if (j >= P.nacc) break;
+                const DevAcc& a = P.acc[j];
+                const bool v = valid_at(B.valid[j], r);
+                long long raw = 0;
+                if (v && a.kind != kAccCount)
+                    raw = a.in_type == kInt32 ? (long long)__ldg((const int*)B.vals[j] + r)
+                                              : __ldg((const long long*)B.vals[j] + r);
+                val[j] = contribution_raw(a.kind, a.in_type, v, raw);
+            }
+            apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+        }
+    }
+}
+
+// HyperLogLog registers of the non-NULL keys (4096 registers: about 1.6 %
+// standard error), to size the table before the fold.
+constexpr int kHllBits = 12;
+constexpr int kHllRegs = 1 << kHllBits;
+
+__global__ void hll_kernel(const void* __restrict__ key, const uint8_t* __restrict__ valid, int type, long long n,
+                           unsigned* __restrict__ regs) {
+    __shared__ unsigned sr[kHllRegs];
+    for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x) sr[i] = 0;
+    __syncthreads();
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+        if (!valid_at(valid, r)) continue;
+        const unsigned long long h = fmix64((unsigned long long)load_int(key, type, r) ^ 0x9E3779B97F4A7C15ull);
+        const unsigned idx = (unsigned)(h >> (64 - kHllBits));
+        const unsigned rank = (unsigned)__clzll((h << kHllBits) | (1ull << (kHllBits - 1))) + 1u;
+        atomicMax(&sr[idx], rank);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x)
+        if (sr[i]) atomicMax(&regs[i], sr[i]);
+}
+
+double hll_estimate(const std::vector<unsigned>& regs) {
+    double sum = 0.0;
+    int zeros = 0;
+    for (unsigned r : regs) {
+        sum += std::ldexp(1.0, -(int)r);
+        zeros += r == 0;
+    }
+    const double m = (double)regs.size();
+    double e = 0.7213 / (1.0 + 1.079 / m) * m * m / sum;
+    if (e <= 2.5 * m && zeros > 0) e = m * std::log(m / zeros);
+    return e;
+}
+
 int maxacc_for(int nacc) { return nacc <= 2 ? 2 : (nacc <= 4 ? 4 : kMaxAccs); }
 
 using RowsKernel = void (*)(const AggProgram, const DevPredicate, const AggKey, long long);
@@ -2560,6 +2693,85 @@ std::string variant_name(const char* base, const AggVariant& v) {
     if (v.tile) return std::string(base) + "<" + std::to_string(v.maxacc) + ",tile>";
     return std::string(base) + "<" + std::to_string(v.maxacc) + (v.combine ? ",combine," : ",atomic,") +
            std::to_string(v.rpt) + ">";
+}
+
+// Collects the occupied slots of a filled table into the output batch: the
+// groups sorted by key with the NULL group last (aggregate.rs:35-66), one
+// column per aggregate.  nullptr when the table overflowed and the caller
+// may retry with a bigger one.
+oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan, const AggProgram& P, unsigned int cap,
+                       const unsigned int* status, bool allow_retry) {
+    // Collect the occupied slots and their key range.
+    const long long m = (long long)cap + 2;
+    Scratch<unsigned int> flags(s, m);
+    Scratch<unsigned long long> pos(s, m + 1);
+    Scratch<unsigned long long> range(s, 2);
+    unsigned long long init_range[2] = {~0ull, 0ull};
+    OXB_CUDA(cudaMemcpyAsync(range.get(), init_range, sizeof init_range, cudaMemcpyHostToDevice, s->stream));
+    note_launch(), agg_flags_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), range.get());
+    OXB_CUDA(cudaGetLastError());
+    scan_u32_to_u64(s, b, flags.get(), pos.get(), m);
+    struct {
+        unsigned long long G, lo, hi, null_rows;
+        uint32_t status;
+    } h{};
+    OXB_CUDA(cudaMemcpyAsync(&h.G, pos.get() + m, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.lo, range.get(), 16, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.null_rows, P.arr + cap, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.status, status, 4, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    if ((h.status & kStatusTableFull) && allow_retry) return nullptr;
+    check_status_word(h.status, "aggregate");
+
+    const long long G = (long long)h.G;
+    const bool has_null = h.null_rows > 0;
+    const long long rows = G + (has_null ? 1 : 0);
+    Scratch<unsigned long long> skeys(s, G + 1);
+    Scratch<unsigned int> sslots(s, G + 1);
+    unsigned long long lo = G > 0 ? h.lo : 0;
+    if (G > 0) {
+        note_launch(), agg_compact_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), pos.get(), lo,
+                                                                                        skeys.get(), sslots.get());
+        OXB_CUDA(cudaGetLastError());
+        unsigned long long span = h.hi - h.lo;
+        int bits = 0;
+        while (bits < 64 && (span >> bits) != 0) bits++;
+        radix_sort_pairs(s, b, skeys.get(), sslots.get(), G, bits);
+    }
+
+    auto out = std::make_unique<oxb_batch>();
+    out->rows = rows;
+    AggOutput O{};
+    O.key_type = plan.key_type;
+    auto make_col = [&](int type, bool nullable) {
+        Column c;
+        c.type = type;
+        c.length = rows;
+        if (rows > 0) {
+            c.owner_values = dev_alloc(s, rows * (size_t)type_width(type, 1), false);
+            c.values = c.owner_values->ptr;
+            if (nullable) {
+                c.owner_validity = dev_alloc(s, ((rows + 31) / 32) * 4, true);
+                c.validity = (uint8_t*)c.owner_validity->ptr;
+            }
+        }
+        return c;
+    };
+    out->cols.push_back(make_col(plan.key_type, has_null));
+    O.key = OutCol{out->cols[0].values, (unsigned int*)out->cols[0].validity};
+    for (int j = 0; j < P.nout; j++) {
+        const int f = P.out[j].func;
+        const bool nullable = !(f == OXB_AGG_COUNT || f == OXB_AGG_COUNT_STAR);
+        out->cols.push_back(make_col(plan.out_types[j], nullable));
+        O.cols[j] = OutCol{out->cols.back().values, (unsigned int*)out->cols.back().validity};
+    }
+    if (rows > 0) {
+        note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, skeys.get(), sslots.get(),
+                                                                                        lo, G, rows);
+        OXB_CUDA(cudaGetLastError());
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    return out.release();
 }
 
 // Choices the autotuner made, per query shape, for this process.
@@ -2810,80 +3022,12 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         }
         OXB_CUDA(cudaGetLastError());
 
-        // Collect the occupied slots and their key range.
-        const long long m = (long long)cap + 2;
-        Scratch<unsigned int> flags(s, m);
-        Scratch<unsigned long long> pos(s, m + 1);
-        Scratch<unsigned long long> range(s, 2);
-        unsigned long long init_range[2] = {~0ull, 0ull};
-        OXB_CUDA(cudaMemcpyAsync(range.get(), init_range, sizeof init_range, cudaMemcpyHostToDevice, s->stream));
-        note_launch(), agg_flags_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), range.get());
-        OXB_CUDA(cudaGetLastError());
-        scan_u32_to_u64(s, b, flags.get(), pos.get(), m);
-        struct {
-            unsigned long long G, lo, hi, null_rows;
-            uint32_t status;
-        } h{};
-        OXB_CUDA(cudaMemcpyAsync(&h.G, pos.get() + m, 8, cudaMemcpyDeviceToHost, s->stream));
-        OXB_CUDA(cudaMemcpyAsync(&h.lo, range.get(), 16, cudaMemcpyDeviceToHost, s->stream));
-        OXB_CUDA(cudaMemcpyAsync(&h.null_rows, P.arr + cap, 8, cudaMemcpyDeviceToHost, s->stream));
-        OXB_CUDA(cudaMemcpyAsync(&h.status, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
-        OXB_CUDA(cudaStreamSynchronize(s->stream));
-        if ((h.status & kStatusTableFull) && attempt == 0) {
+        oxb_batch* out = emit_groups(s, b, plan, P, cap, status.get(), attempt == 0);
+        if (!out) {
             cap = next_pow2(2 * (max_groups < 1 ? 1 : max_groups), 4096);
             continue;  // the small table overflowed: rerun with room for every row
         }
-        check_status_word(h.status, "aggregate");
-
-        const long long G = (long long)h.G;
-        const bool has_null = h.null_rows > 0;
-        const long long rows = G + (has_null ? 1 : 0);
-        Scratch<unsigned long long> skeys(s, G + 1);
-        Scratch<unsigned int> sslots(s, G + 1);
-        unsigned long long lo = G > 0 ? h.lo : 0;
-        if (G > 0) {
-            note_launch(), agg_compact_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), pos.get(), lo,
-                                                                                            skeys.get(), sslots.get());
-            OXB_CUDA(cudaGetLastError());
-            unsigned long long span = h.hi - h.lo;
-            int bits = 0;
-            while (bits < 64 && (span >> bits) != 0) bits++;
-            radix_sort_pairs(s, b, skeys.get(), sslots.get(), G, bits);
-        }
-
-        auto out = std::make_unique<oxb_batch>();
-        out->rows = rows;
-        AggOutput O{};
-        O.key_type = plan.key_type;
-        auto make_col = [&](int type, bool nullable) {
-            Column c;
-            c.type = type;
-            c.length = rows;
-            if (rows > 0) {
-                c.owner_values = dev_alloc(s, rows * (size_t)type_width(type, 1), false);
-                c.values = c.owner_values->ptr;
-                if (nullable) {
-                    c.owner_validity = dev_alloc(s, ((rows + 31) / 32) * 4, true);
-                    c.validity = (uint8_t*)c.owner_validity->ptr;
-                }
-            }
-            return c;
-        };
-        out->cols.push_back(make_col(plan.key_type, has_null));
-        O.key = OutCol{out->cols[0].values, (unsigned int*)out->cols[0].validity};
-        for (int j = 0; j < P.nout; j++) {
-            const int f = P.out[j].func;
-            const bool nullable = !(f == OXB_AGG_COUNT || f == OXB_AGG_COUNT_STAR);
-            out->cols.push_back(make_col(plan.out_types[j], nullable));
-            O.cols[j] = OutCol{out->cols.back().values, (unsigned int*)out->cols.back().validity};
-        }
-        if (rows > 0) {
-            note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, skeys.get(), sslots.get(),
-                                                                                            lo, G, rows);
-            OXB_CUDA(cudaGetLastError());
-            OXB_CUDA(cudaStreamSynchronize(s->stream));
-        }
-        return out.release();
+        return out;
     }
     fail(OXB_TABLE_FULL, "aggregate hash table full after a retry");
 }
@@ -2904,6 +3048,125 @@ int resident_grid(const Backend& b, K kernel, size_t smem, long long work) {
 }
 
 }  // namespace
+
+
+oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_aggregate_batches_args& a) {
+    if (a.ninputs < 1 || !a.inputs || !a.spec) fail(OXB_PLAN, "aggregate_batches: no inputs or no spec");
+    for (int i = 0; i < a.ninputs; i++)
+        if (!a.inputs[i]) fail(OXB_PLAN, "aggregate_batches: input batch " + std::to_string(i) + " is null");
+    const oxb_batch& first = *a.inputs[0];
+    const int ncols = (int)first.cols.size();
+    for (int i = 1; i < a.ninputs; i++) {
+        const oxb_batch& bt = *a.inputs[i];
+        if ((int)bt.cols.size() != ncols) fail(OXB_PLAN, "input batches have different column counts");
+        for (int c = 0; c < ncols; c++)
+            if (bt.cols[c].type != first.cols[c].type || bt.cols[c].dim != first.cols[c].dim)
+                fail(OXB_PLAN, "input batches differ in the type of column " + std::to_string(c));
+    }
+    const oxb_aggregate_spec& spec = *a.spec;
+    if (spec.group_by < 0 || spec.group_by >= ncols) fail(OXB_PLAN, "group-by column out of range");
+    // The plan's view of each column: a validity bitmap when any batch has
+    // one (a batch without NULLs may carry none), so NULL-aware counts exist.
+    std::vector<Column> rep(first.cols.begin(), first.cols.end());
+    for (int c = 0; c < ncols; c++)
+        for (int i = 0; i < a.ninputs && !rep[c].validity; i++) rep[c].validity = a.inputs[i]->cols[c].validity;
+    const Column& key = rep[spec.group_by];
+    if (key.type != kInt64 && key.type != kInt32)
+        fail(OXB_UNSUPPORTED, "group key must be Int64 or Int32 on the device");
+    if (spec.naggregates < 0 || spec.naggregates > kMaxOuts) fail(OXB_UNSUPPORTED, "too many aggregates");
+    std::vector<int> funcs;
+    std::vector<AggInputCol> inputs;
+    for (int j = 0; j < spec.naggregates; j++) {
+        const int f = spec.funcs[j];
+        const Column* c = nullptr;
+        if (f != OXB_AGG_COUNT_STAR) {
+            if (spec.columns[j] < 0 || spec.columns[j] >= ncols) fail(OXB_PLAN, "aggregate column out of range");
+            c = &rep[spec.columns[j]];
+        }
+        check_agg_input(f, c, spec.columns[j]);
+        funcs.push_back(f);
+        inputs.push_back(AggInputCol{c, 0, f == OXB_AGG_COUNT_STAR ? -1 : spec.columns[j]});
+    }
+    const DevPredicate pred = make_predicate(first, a.leaves, a.nleaves);
+    AggPlan plan = plan_aggregate(funcs, inputs, key.type);
+    AggProgram& P = plan.P;
+    const int* acc_col = plan.acc_index;
+    std::vector<BatchCols> hb(a.ninputs);
+    long long ntiles = 0, total = 0;
+    for (int i = 0; i < a.ninputs; i++) {
+        const oxb_batch& bt = *a.inputs[i];
+        BatchCols& c = hb[i];
+        c = BatchCols{};
+        c.n = bt.rows;
+        c.tile0 = ntiles;
+        ntiles += (bt.rows + kBatchTile - 1) / kBatchTile;
+        total += bt.rows;
+        c.key = bt.cols[spec.group_by].values;
+        c.key_valid = bt.cols[spec.group_by].validity;
+        for (int j = 0; j < P.nacc; j++) {
+            c.vals[j] = bt.cols[acc_col[j]].values;
+            c.valid[j] = bt.cols[acc_col[j]].validity;
+        }
+        for (int l = 0; l < a.nleaves; l++) {
+            c.lvals[l] = bt.cols[a.leaves[l].column].values;
+            c.lvalid[l] = bt.cols[a.leaves[l].column].validity;
+        }
+    }
+    Scratch<BatchCols> dbatches(s, hb.size());
+    OXB_CUDA(cudaMemcpyAsync(dbatches.get(), hb.data(), hb.size() * sizeof(BatchCols), cudaMemcpyHostToDevice, s->stream));
+
+    // Distinct keys across every batch, for the table's size.
+    Scratch<unsigned> regs(s, kHllRegs, true);
+    for (int i = 0; i < a.ninputs; i++) {
+        if (hb[i].n == 0) continue;
+        note_launch(), hll_kernel<<<grid_for(b, hb[i].n, 256, 4), 256, 0, s->stream>>>(hb[i].key, hb[i].key_valid, key.type,
+                                                                                     hb[i].n, regs.get());
+    }
+    OXB_CUDA(cudaGetLastError());
+    std::vector<unsigned> hregs(kHllRegs);
+    OXB_CUDA(cudaMemcpyAsync(hregs.data(), regs.get(), kHllRegs * 4, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    const double est = hll_estimate(hregs);
+    const long long all_rows = next_pow2(2 * std::max<long long>(total, 1), 4096);
+    unsigned int cap = next_pow2(std::max<long long>(4096, (long long)(est * 1.2 * 2.0) + 1), 4096);
+    if ((long long)cap > all_rows) cap = (unsigned int)all_rows;
+
+    const int maxacc = maxacc_for(P.nacc);
+    auto kern = maxacc == 2 ? agg_batches_kernel<2> : (maxacc == 4 ? agg_batches_kernel<4> : agg_batches_kernel<kMaxAccs>);
+    int per_sm = 0;
+    OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0));
+    const long long grid = std::max<long long>(1, std::min<long long>(ntiles, (long long)b.sms * std::max(per_sm, 1)));
+    for (int attempt = 0;; attempt++) {
+        P.capacity = cap;
+        P.stride = (long long)cap + 2;
+        P.smem_slots = 0;
+        P.wslots = 0;
+        AllocRef keys_mem = dev_alloc(s, (size_t)cap * 8, false);
+        AllocRef arr_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
+        Scratch<unsigned int> status(s, 1, true);
+        Scratch<unsigned long long> fill(s, 1, true);
+        Scratch<unsigned long long> queue(s, 1, true);
+        P.keys = (long long*)keys_mem->ptr;
+        P.arr = (unsigned long long*)arr_mem->ptr;
+        P.status = status.get();
+        P.fill = fill.get();
+        P.fill_limit = (unsigned long long)cap / 4 * 3;
+        note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(P);
+        OXB_CUDA(cudaGetLastError());
+        if (ntiles > 0) {
+            KernelTimer timer(b, s, "agg_batches_kernel");
+            timer.begin();
+            note_launch(), kern<<<(unsigned)grid, kThreads, 0, s->stream>>>(P, pred, key.type, dbatches.get(), a.ninputs,
+                                                                            ntiles, queue.get());
+            timer.end();
+            OXB_CUDA(cudaGetLastError());
+        }
+        const bool can_retry = (long long)cap < all_rows;
+        oxb_batch* out = emit_groups(s, b, plan, P, cap, status.get(), can_retry);
+        if (out) return out;
+        cap = (unsigned int)std::min<long long>(2ll * cap, all_rows);  // the estimate was low: double the table
+    }
+}
 
 oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_args& a) {
     if (!a.input || !a.spec) fail(OXB_PLAN, "aggregate: null input or spec");

@@ -495,6 +495,15 @@ oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream, const o
     OXB_CATCH
 }
 
+oxb_status oxb_aggregate_batches(oxb_backend* backend, oxb_stream* stream, const oxb_aggregate_batches_args* args,
+                                 oxb_batch** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!args || !out) fail(OXB_PLAN, "null argument");
+    *out = aggregate_batches(stream_of(stream), backend->b, *args);
+    OXB_CATCH
+}
+
 oxb_status oxb_vector_index_build(oxb_backend* backend, oxb_stream* stream, const oxb_batch* input, int32_t column,
                                   oxb_vector_index** out) {
     OXB_TRY

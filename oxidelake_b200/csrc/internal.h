@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstring>
 #include <cstdint>
@@ -227,6 +228,7 @@ bool key_range(const StreamRef& s, const Backend& b, const Column& key, long lon
 // Operators.
 oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a);
 AllocRef predicate_bits(const StreamRef& s, const Backend& b, const DevPredicate& pred, long long n);
+oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_aggregate_batches_args& a);
 oxb_vector_index* vector_index_build(const StreamRef& s, const Backend& b, const oxb_batch& in, int column);
 void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_args& a, int64_t* out_ids,
                  float* out_dist, oxb_vector_topk_stats* stats);

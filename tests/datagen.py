@@ -213,3 +213,26 @@ def config2(build_rows: int, probe_rows: int, seed: int = 0x0A11CE + 2):
     build = pa.RecordBatch.from_arrays([pa.array(key), pa.array(attr)], names=["key", "attr"])
     probe = pa.RecordBatch.from_arrays([pa.array(fk), pa.array(payload), pa.array(qty)], names=["fk", "payload", "qty"])
     return build, probe
+
+
+def config3_batches(total_rows: int, distinct: int, seed: int = 0x0A11CE + 3, min_rows: int = 8192,
+                    max_rows: int = 1 << 20):
+    """High-cardinality input as uneven RecordBatches: g i64 uniform over
+    `distinct` values, x i32 U(-1e6, 1e6) with 2% NULLs, f i32 U[0,100) (the
+    filter column: `f < s` keeps s %).  Batch sizes are seeded in
+    [min_rows, max_rows]."""
+    rng = np.random.default_rng(seed)
+    batches = []
+    left = total_rows
+    while left > 0:
+        n = int(min(left, rng.integers(min_rows, max_rows + 1)))
+        g = rng.integers(0, distinct, n, dtype=np.int64)
+        x = rng.integers(-1_000_000, 1_000_001, n, dtype=np.int32)
+        f = rng.integers(0, 100, n, dtype=np.int32)
+        batches.append(
+            pa.RecordBatch.from_arrays(
+                [pa.array(g), pa.array(x, mask=rng.random(n) < 0.02), pa.array(f)], names=["g", "x", "f"]
+            )
+        )
+        left -= n
+    return batches
