@@ -383,7 +383,14 @@ typedef struct oxb_vector_topk_args {
     int32_t metric;          /* oxb_metric */
     int32_t overfetch;       /* re-ranked candidates per query = overfetch * k (0: 4) */
     int32_t exact;           /* 1: skip the BF16 scan, the exact FP32 path for every query */
+    /* A leaf each query has with its own literal, so queries whose WHERE
+     * differs share one scan: query q also needs
+     * `qleaf_column <qleaf_op> qleaf_lits[q]` (qleaf_column -1: none). */
+    int32_t qleaf_column;
+    int32_t qleaf_op;        /* oxb_cmp */
+    int32_t qleaf_type;      /* the column's oxb_type: INT64, INT32 or FLOAT64 */
     int32_t reserved;
+    const int64_t* qleaf_lits; /* host, nqueries literals (a Float64 one as its bit pattern) */
 } oxb_vector_topk_args;
 
 typedef struct oxb_vector_topk_stats {

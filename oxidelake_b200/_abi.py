@@ -150,7 +150,11 @@ class VectorTopkArgs(C.Structure):
         ("metric", C.c_int32),
         ("overfetch", C.c_int32),
         ("exact", C.c_int32),
+        ("qleaf_column", C.c_int32),
+        ("qleaf_op", C.c_int32),
+        ("qleaf_type", C.c_int32),
         ("reserved", C.c_int32),
+        ("qleaf_lits", C.c_void_p),
     ]
 
 

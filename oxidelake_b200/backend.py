@@ -560,17 +560,31 @@ class CudaBackend:
         metric: DistanceMetric,
         overfetch: int = 0,
         exact: bool = False,
+        query_leaf=None,
     ):
         """ORDER BY distance, row LIMIT k per query over the rows `predicate`
-        keeps: (ids int64 [Q, k], dist float32 [Q, k], stats dict)."""
+        keeps: (ids int64 [Q, k], dist float32 [Q, k], stats dict).
+        `query_leaf` = (column, Comparison, literals): query q also needs
+        `column op literals[q]` (Literal objects of one type)."""
         q = np.ascontiguousarray(np.asarray(queries, dtype=np.float32))
         if q.ndim != 2:
             raise Plan("queries must be a 2-D array")
         lv, nl = _leaf_array(predicate)
         nq, dim = q.shape
+        qcol, qop, qtype, qlits = -1, 0, 0, None
+        if query_leaf is not None:
+            qcol, cmp, lits = query_leaf
+            if len(lits) != nq:
+                raise Plan("one literal per query")
+            qop, qtype = int(cmp), int(lits[0].type)
+            raw = [
+                int(np.float64(l.value).view(np.int64)) if int(l.type) == 2 else int(l.value) for l in lits
+            ]
+            qlits = np.ascontiguousarray(raw, dtype=np.int64)
         a = _abi.VectorTopkArgs(
             index.handle, input.handle, C.cast(lv, C.c_void_p) if lv is not None else None, nl, nq,
-            q.ctypes.data, dim, k, int(metric), overfetch, 1 if exact else 0, 0,
+            q.ctypes.data, dim, k, int(metric), overfetch, 1 if exact else 0, qcol, qop, qtype, 0,
+            qlits.ctypes.data if qlits is not None else None,
         )
         ids = np.empty((max(nq, 1), k), np.int64)
         dist = np.empty((max(nq, 1), k), np.float32)

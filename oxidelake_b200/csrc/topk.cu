@@ -45,7 +45,9 @@ constexpr int kTmemCols = 2 * kRTile;
 // Shared memory of the scan: the stage ring, the candidate buffers of the
 // 128 queries (C keys each, interleaved by query), two tiles' row norms and
 // selection words for the epilogue, the barriers, and alignment slack.
-constexpr size_t kTileAux = (size_t)kRTile * 4 + (kRTile / 32) * 4;  // norms + selection words
+// Per tile: row norms, selection words, and the per-query filter column's
+// order keys.
+constexpr size_t kTileAux = (size_t)kRTile * 4 + (kRTile / 32) * 4 + (size_t)kRTile * 8;
 constexpr size_t scan_smem(int stages, int C) {
     return (size_t)stages * kStageBytes + (size_t)C * kQTile * 8 + 2 * kTileAux + 128 + 1024;
 }
@@ -177,6 +179,13 @@ struct ScanParams {
     const uint8_t* valid;       // vector validity, null = all
     const float* norm2;         // per row ||x||^2
     const float* inv;           // per row 1 / ||x||
+    // A leaf every query has with its own literal: `qcol <qop> qlits[q]`
+    // (qcol null: none); its NULLs fail every query.
+    const void* qcol;
+    const uint8_t* qvalid;
+    int qtype;
+    int qop;
+    const long long* qlits;     // per query, as filter order keys
     unsigned long long* lists;  // [grid * 128][L]
     unsigned* counts;           // [grid * 128]
     unsigned long long* bounds; // [grid * 128]: every row missing from the list has a larger key
@@ -190,8 +199,9 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
     unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
     const int stages = p.stages;
     unsigned long long* cands = (unsigned long long*)(smem + (size_t)stages * kStageBytes);
-    float* tnorm = (float*)(cands + (size_t)p.C * kQTile);     // [2][256]
-    unsigned* tsel = (unsigned*)(tnorm + 2 * kRTile);            // [2][8]
+    long long* tqkey = (long long*)(cands + (size_t)p.C * kQTile);  // [2][256]
+    float* tnorm = (float*)(tqkey + 2 * kRTile);                      // [2][256]
+    unsigned* tsel = (unsigned*)(tnorm + 2 * kRTile);                 // [2][8]
     unsigned long long* bars = (unsigned long long*)(tsel + 2 * (kRTile / 32));
     unsigned long long* full = bars;
     unsigned long long* empty = bars + kMaxStages;
@@ -296,6 +306,7 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
         int buf = 0;
         unsigned tph = 0;
         const float* nsrc = p.metric == 0 ? p.norm2 : p.inv;
+        const long long qlit = p.qcol && active ? __ldg(p.qlits + q) : 0;
         int par = 0;
         for (long long t = ci; t < ntiles; t += cpg, par ^= 1) {
             // The four epilogue warps stage this tile's row norms and
@@ -307,19 +318,26 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                 for (int h = 0; h < kRTile / kQTile; h++) {
                     const long long r = t * kRTile + h * kQTile + ql;
                     tn[h * kQTile + ql] = r < p.n ? __ldg(nsrc + r) : 0.0f;
+                    if (p.qcol && r < p.n)
+                        tqkey[par * kRTile + h * kQTile + ql] =
+                            p.qtype == kFloat64 ? filter_order_key(__ldg((const double*)p.qcol + r))
+                            : p.qtype == kInt64 ? __ldg((const long long*)p.qcol + r)
+                                                : (long long)__ldg((const int*)p.qcol + r);
                 }
                 if (ql < kRTile / 32) {
                     const long long row0 = t * kRTile + ql * 32;
                     unsigned sel = 0;
                     if (row0 < p.n) {
                         sel = p.sel ? __ldg(p.sel + (row0 >> 5)) : ~0u;
-                        if (p.valid) {
-                            // The bitmap's bytes for these 32 rows, none past its end.
-                            const long long b0 = row0 >> 3, nbytes = (p.n + 7) >> 3;
+                        // The bitmaps' bytes for these 32 rows, none past their end.
+                        const long long b0 = row0 >> 3, nbytes = (p.n + 7) >> 3;
+                        for (int bm = 0; bm < 2; bm++) {
+                            const uint8_t* vb = bm == 0 ? p.valid : (p.qcol ? p.qvalid : nullptr);
+                            if (!vb) continue;
                             unsigned v = 0;
 #pragma unroll
                             for (int bi = 0; bi < 4; bi++)
-                                if (b0 + bi < nbytes) v |= (unsigned)__ldg(p.valid + b0 + bi) << (8 * bi);
+                                if (b0 + bi < nbytes) v |= (unsigned)__ldg(vb + b0 + bi) << (8 * bi);
                             sel &= v;
                         }
                         if (row0 + 32 > p.n) sel &= (1u << (p.n - row0)) - 1u;
@@ -358,7 +376,35 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
                     cnt = p.L;
                     dropped = true;
                 }
-                const unsigned sel = tsel[par * (kRTile / 32) + c];
+                unsigned sel = tsel[par * (kRTile / 32) + c];
+                if (p.qcol && active && sel) {
+                    // This query's own leaf over the chunk's rows.
+                    const long long* qk = tqkey + par * kRTile + c * 32;
+                    unsigned m = 0;
+                    switch (p.qop) {
+                        case 0:
+#pragma unroll
+                            for (int j = 0; j < 32; j++) m |= (unsigned)(qk[j] == qlit) << j;
+                            break;
+                        case 1:
+#pragma unroll
+                            for (int j = 0; j < 32; j++) m |= (unsigned)(qk[j] < qlit) << j;
+                            break;
+                        case 2:
+#pragma unroll
+                            for (int j = 0; j < 32; j++) m |= (unsigned)(qk[j] <= qlit) << j;
+                            break;
+                        case 3:
+#pragma unroll
+                            for (int j = 0; j < 32; j++) m |= (unsigned)(qk[j] > qlit) << j;
+                            break;
+                        default:
+#pragma unroll
+                            for (int j = 0; j < 32; j++) m |= (unsigned)(qk[j] >= qlit) << j;
+                            break;
+                    }
+                    sel &= m;
+                }
                 if (!active || !sel) continue;
                 const unsigned row0 = (unsigned)(t * kRTile + c * 32);
                 // Scores (a NaN counts as +inf, after every finite score) and
@@ -613,10 +659,19 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
 // The exact path's keys: (distance order, row) for rows the WHERE keeps with
 // a valid vector, the largest key for the rest.
 __global__ void topk_exact_keys_kernel(const float* __restrict__ d, const unsigned* __restrict__ sel,
-                                       const uint8_t* __restrict__ valid, long long n,
+                                       const uint8_t* __restrict__ valid, long long n, DevLeaf qleaf,
                                        unsigned long long* __restrict__ keys) {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
-        const bool ok = (!sel || ((__ldg(sel + (r >> 5)) >> (r & 31)) & 1u)) && valid_at(valid, r);
+        bool ok = (!sel || ((__ldg(sel + (r >> 5)) >> (r & 31)) & 1u)) && valid_at(valid, r);
+        if (ok && qleaf.values) {
+            if (!valid_at(qleaf.validity, r)) ok = false;
+            else {
+                const long long a = qleaf.type == kFloat64 ? filter_order_key(__ldg((const double*)qleaf.values + r))
+                                    : qleaf.type == kInt64 ? __ldg((const long long*)qleaf.values + r)
+                                                           : (long long)__ldg((const int*)qleaf.values + r);
+                ok = cmp_holds(qleaf.op, a, qleaf.lit);
+            }
+        }
         // The distance's bits, loaded as an integer: a NaN keeps its bits.
         const unsigned bits = __ldg((const unsigned*)d + r);
         keys[r] = ok ? ((unsigned long long)f32_order(bits) << 32) | (unsigned long long)r : kNoKey;
@@ -752,6 +807,23 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     if (a.nqueries < 0) fail(OXB_PLAN, "negative query count");
     if (a.nqueries > 0 && (!a.queries || !out_ids || !out_dist)) fail(OXB_PLAN, "null queries or outputs");
     DevPredicate pred = make_predicate(in, a.leaves, a.nleaves);
+    // The per-query leaf: checked like a shared one, literals as order keys.
+    DevLeaf qleaf{};
+    std::vector<long long> qlits_h;
+    if (a.qleaf_column >= 0 && a.nqueries > 0) {
+        if (!a.qleaf_lits) fail(OXB_PLAN, "per-query literals are null");
+        oxb_leaf probe{};
+        probe.column = a.qleaf_column;
+        probe.op = a.qleaf_op;
+        probe.lit_type = a.qleaf_type;
+        qlits_h.resize(a.nqueries);
+        for (int q = 0; q < a.nqueries; q++) {
+            probe.lit.i = a.qleaf_lits[q];
+            const DevPredicate one = make_predicate(in, &probe, 1);
+            qlits_h[q] = one.leaves[0].lit;
+            qleaf = one.leaves[0];
+        }
+    }
     oxb_vector_topk_stats st{};
     const int nq = a.nqueries, k = a.k, dim = ix.dim, dp = ix.dp;
     const long long n = ix.n;
@@ -770,6 +842,11 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     OXB_CUDA(cudaGetLastError());
     AllocRef sel;
     if (pred.nleaves > 0 && n > 0) sel = predicate_bits(s, b, pred, n);
+    Scratch<long long> qlits;
+    if (qleaf.values || (!qlits_h.empty() && n == 0)) {
+        qlits = Scratch<long long>(s, nq);
+        OXB_CUDA(cudaMemcpyAsync(qlits.get(), qlits_h.data(), (size_t)nq * 8, cudaMemcpyHostToDevice, s->stream));
+    }
     const unsigned* selp = sel ? (const unsigned*)sel->ptr : nullptr;
 
     Scratch<long long> ids(s, (size_t)nq * k);
@@ -821,6 +898,11 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.valid = ix.vec.validity;
         sp.norm2 = (const float*)ix.norm2->ptr;
         sp.inv = (const float*)ix.inv->ptr;
+        sp.qcol = qleaf.values;
+        sp.qvalid = qleaf.validity;
+        sp.qtype = qleaf.type;
+        sp.qop = qleaf.op;
+        sp.qlits = qlits.get();
         sp.lists = lists.get();
         sp.counts = counts.get();
         sp.bounds = bounds.get();
@@ -890,8 +972,11 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
             keys = Scratch<unsigned long long>(s, n);
         }
         launch_vector_distance(s, b, ix.vec, n, qf.get() + (size_t)q * dim, a.metric, d.get());
+        DevLeaf ql = qleaf;
+        if (ql.values) ql.lit = qlits_h[q];
         note_launch(), topk_exact_keys_kernel<<<grid_for(b, n, 256, 8), 256, 0, s->stream>>>(d.get(), selp,
-                                                                                             ix.vec.validity, n, keys.get());
+                                                                                             ix.vec.validity, n, ql,
+                                                                                             keys.get());
         radix_sort_pairs(s, b, keys.get(), nullptr, n, 64);
         note_launch(), topk_exact_out_kernel<<<1, 256, 0, s->stream>>>(keys.get(), n, k, ids.get() + (size_t)q * k,
                                                                        dist.get() + (size_t)q * k);

@@ -110,3 +110,29 @@ def test_overfetch_one_still_exact(backend, stream):
     ids, dist, stats = run(backend, stream, batch, q, 25, DistanceMetric.L2, overfetch=1)
     want_ids, want_dist = oracle.vector_topk(batch, 2, q, 25, int(DistanceMetric.L2), threads=oracle.cpu_threads())
     check(ids, dist, want_ids, want_dist)
+
+
+@pytest.mark.parametrize("metric", [DistanceMetric.L2, DistanceMetric.Cosine], ids=["l2", "cosine"])
+def test_per_query_filter_literals(backend, stream, metric):
+    """Queries whose WHERE differs only in a literal share one scan: each
+    query's answer equals its own top-k under its own predicate."""
+    batch, v = table(60_000, 128, seed=31, null_frac=0.01)
+    rng = np.random.default_rng(32)
+    nq = 150
+    q = rng.standard_normal((nq, 128)).astype(np.float32)
+    lits = [int(t) for t in rng.integers(1, 100, nq)]
+    shared = compare(0, Cmp.GtEq, Literal.int64(100))
+    dev = backend.upload(stream, batch)
+    ix = backend.vector_index(stream, dev, 2)
+    ids, dist, st = backend.vector_topk(
+        stream, ix, dev, shared, q, 9, metric, query_leaf=(1, Cmp.Lt, [Literal.int64(t) for t in lits])
+    )
+    for i in range(nq):
+        pred = compare(1, Cmp.Lt, Literal.int64(lits[i]))
+        wi, wd = oracle.vector_topk(batch, 2, q[i : i + 1], 9, int(metric), leaves(shared) + leaves(pred))
+        check(ids[i : i + 1], dist[i : i + 1], wi, wd)
+    # and the exact path with the same per-query literals
+    ide, de, _ = backend.vector_topk(
+        stream, ix, dev, shared, q[:4], 9, metric, exact=True, query_leaf=(1, Cmp.Lt, [Literal.int64(t) for t in lits[:4]])
+    )
+    check(ide, de, ids[:4], dist[:4])
