@@ -448,6 +448,62 @@ typedef struct oxb_join_aggregate_args {
 OXB_API oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream,
                               const oxb_join_aggregate_args* args, oxb_batch** out);
 
+/* ---- serving (the request loop the reference lacks; its queries run one at
+ *      a time through compute/src/operator.rs) ---------------------------- */
+
+/* A request loop over resident tables: submit returns a ticket at once;
+ * worker threads (one CUDA stream each) run admitted work concurrently, and
+ * top-k requests that queue while others run are stacked into one scan when
+ * they share the index, batch, metric and WHERE except for their own query
+ * vector, k and per-query literal.  Work is admitted while the estimated
+ * device memory of what runs stays within the budget; a request that alone
+ * exceeds it is refused with OXB_OOM_ADMISSION.  Results equal the direct
+ * calls'.  The resident batches, indexes and join tables outlive the server. */
+typedef struct oxb_server oxb_server;
+typedef struct oxb_server_config {
+    uint64_t memory_budget; /* bytes (0: 150 GB) */
+    int32_t workers;        /* concurrent work items (0: 2) */
+    int32_t max_batch;      /* queries stacked into one top-k scan (0: 256; 1: no batching) */
+} oxb_server_config;
+OXB_API oxb_status oxb_server_create(oxb_backend* backend, const oxb_server_config* config, oxb_server** out);
+/* Finishes the submitted work, then stops the workers. */
+OXB_API void oxb_server_destroy(oxb_server* server);
+
+typedef struct oxb_topk_request {
+    const oxb_vector_index* index;
+    const oxb_batch* input;
+    const oxb_leaf* leaves; /* the WHERE */
+    int32_t nleaves;
+    int32_t qleaf;          /* 1: leaves[nleaves - 1] is this query's own literal (see oxb_vector_topk) */
+    const float* query;     /* dim floats, copied at submit */
+    int32_t dim;
+    int32_t k;
+    int32_t metric;
+    int32_t reserved;
+} oxb_topk_request;
+OXB_API oxb_status oxb_server_submit_topk(oxb_server* server, const oxb_topk_request* request, uint64_t* ticket);
+/* The arguments (and leaves) are copied at submit. */
+OXB_API oxb_status oxb_server_submit_join_aggregate(oxb_server* server, const oxb_join_aggregate_args* request,
+                                                    uint64_t* ticket);
+/* Blocks until the request is done.  Top-k: k ids and distances into
+ * caller buffers; join-aggregate: the result batch.  latency_us (may be
+ * NULL): submit to completion. */
+OXB_API oxb_status oxb_server_wait_topk(oxb_server* server, uint64_t ticket, int64_t* ids, float* dist,
+                                        double* latency_us);
+OXB_API oxb_status oxb_server_wait_batch(oxb_server* server, uint64_t ticket, oxb_batch** out, double* latency_us);
+
+typedef struct oxb_server_stats {
+    int64_t completed;
+    int64_t rejected;
+    int64_t dispatches;      /* work items run */
+    int64_t batched_queries; /* top-k requests that shared a scan */
+    int64_t peak_bytes;      /* largest admitted estimate in flight */
+    double p50_us, p99_us;   /* submit-to-result latency */
+    double qps;              /* completed / (last completion - first submit) */
+} oxb_server_stats;
+/* reset: 1 starts a new measurement window. */
+OXB_API oxb_status oxb_server_stats_get(oxb_server* server, oxb_server_stats* out, int32_t reset);
+
 /* ---- instrumentation (no counterpart in the reference) ------------------ */
 
 /* When enabled, each operator records CUDA events on its stream around its

@@ -137,6 +137,38 @@ class AggregateBatchesArgs(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("memory_budget", C.c_uint64), ("workers", C.c_int32), ("max_batch", C.c_int32)]
+
+
+class TopkRequest(C.Structure):
+    _fields_ = [
+        ("index", C.c_void_p),
+        ("input", C.c_void_p),
+        ("leaves", C.c_void_p),
+        ("nleaves", C.c_int32),
+        ("qleaf", C.c_int32),
+        ("query", C.c_void_p),
+        ("dim", C.c_int32),
+        ("k", C.c_int32),
+        ("metric", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int64),
+        ("rejected", C.c_int64),
+        ("dispatches", C.c_int64),
+        ("batched_queries", C.c_int64),
+        ("peak_bytes", C.c_int64),
+        ("p50_us", C.c_double),
+        ("p99_us", C.c_double),
+        ("qps", C.c_double),
+    ]
+
+
 class VectorTopkArgs(C.Structure):
     _fields_ = [
         ("index", C.c_void_p),
@@ -250,6 +282,13 @@ PROTOTYPES = {
     "oxb_join_aggregate": (_S, [_P, _P, C.POINTER(JoinAggregateArgs), _PP]),
     "oxb_vector_distance": (_S, [_P, _P, C.POINTER(VectorDistanceArgs), _PP]),
     "oxb_aggregate_batches": (_S, [_P, _P, C.POINTER(AggregateBatchesArgs), _PP]),
+    "oxb_server_create": (_S, [_P, C.POINTER(ServerConfig), _PP]),
+    "oxb_server_destroy": (None, [_P]),
+    "oxb_server_submit_topk": (_S, [_P, C.POINTER(TopkRequest), C.POINTER(C.c_uint64)]),
+    "oxb_server_submit_join_aggregate": (_S, [_P, C.POINTER(JoinAggregateArgs), C.POINTER(C.c_uint64)]),
+    "oxb_server_wait_topk": (_S, [_P, C.c_uint64, _P, _P, C.POINTER(C.c_double)]),
+    "oxb_server_wait_batch": (_S, [_P, C.c_uint64, _PP, C.POINTER(C.c_double)]),
+    "oxb_server_stats_get": (_S, [_P, C.POINTER(ServerStats), C.c_int32]),
     "oxb_vector_index_build": (_S, [_P, _P, _P, C.c_int32, _PP]),
     "oxb_vector_index_free": (None, [_P]),
     "oxb_vector_topk": (_S, [_P, _P, C.POINTER(VectorTopkArgs), _P, _P, C.POINTER(VectorTopkStats)]),

@@ -487,42 +487,14 @@ class CudaBackend:
         """The fused probe -> WHERE -> GROUP BY pass (no reference counterpart;
         equals GpuHashJoinExec followed by the aggregate).  `group` and each
         aggregate name a side (0 probe, 1 build) and a column."""
-        build = table.build
-        a = _abi.JoinAggregateArgs()
-        a.probe = probe.handle
-        a.probe_key = probe_key
-        a.table = table.handle
-        a.build = build.handle
-        lv, nl = _leaf_array(predicate)
-        a.leaves = lv
-        a.nleaves = nl
-        a.group_side, a.group_column = group
-        a.naggregates = len(aggregates)
-        for j, (f, side, col) in enumerate(aggregates):
-            a.funcs[j] = int(f)
-            a.sides[j] = int(side)
-            a.columns[j] = int(col)
+        a, schema, keep = _join_aggregate_args(probe, probe_key, table, predicate, group, aggregates)
         h = C.c_void_p()
         _abi.check(_L().oxb_join_aggregate(self.handle, stream.handle, C.byref(a), C.byref(h)))
-        schemas = (probe.schema, build.schema)
-        key = schemas[group[0]].field(group[1])
-        fields = [pa.field(key.name, key.type, True)]
-        for f, side, col in aggregates:
-            f = AggregateFunction(f)
-            if f == AggregateFunction.CountStar:
-                fields.append(pa.field("COUNT(*)", pa.int64(), True))
-                continue
-            fld = schemas[side].field(col)
-            if f == AggregateFunction.Count:
-                t = pa.int64()
-            elif f == AggregateFunction.Sum:
-                t = pa.float64() if pa.types.is_float64(fld.type) else pa.int64()
-            elif f == AggregateFunction.Avg:
-                t = pa.float64()
-            else:
-                t = fld.type
-            fields.append(pa.field(f"{f.sql_name()}({fld.name})", t, True))
-        return DeviceBatch(h.value, pa.schema(fields))
+        return DeviceBatch(h.value, schema)
+
+    def server(self, memory_budget: int = 0, workers: int = 0, max_batch: int = 0) -> "Server":
+        """A serving loop over resident tables (oxb_server_create)."""
+        return Server(self, memory_budget, workers, max_batch)
 
     def vector_distance(
         self,
@@ -633,3 +605,114 @@ class CudaBackend:
 
     def supports_aggregate(self) -> bool:
         return bool(_L().oxb_supports_aggregate(self.handle))
+
+def _join_aggregate_args(probe, probe_key, table, predicate, group, aggregates):
+    """The C arguments of a join-aggregate, its output schema, and what must
+    stay alive while the call reads them."""
+    build = table.build
+    a = _abi.JoinAggregateArgs()
+    a.probe = probe.handle
+    a.probe_key = probe_key
+    a.table = table.handle
+    a.build = build.handle
+    lv, nl = _leaf_array(predicate)
+    a.leaves = lv
+    a.nleaves = nl
+    a.group_side, a.group_column = group
+    a.naggregates = len(aggregates)
+    for j, (f, side, col) in enumerate(aggregates):
+        a.funcs[j] = int(f)
+        a.sides[j] = int(side)
+        a.columns[j] = int(col)
+    schemas = (probe.schema, build.schema)
+    key = schemas[group[0]].field(group[1])
+    fields = [pa.field(key.name, key.type, True)]
+    for f, side, col in aggregates:
+        f = AggregateFunction(f)
+        if f == AggregateFunction.CountStar:
+            fields.append(pa.field("COUNT(*)", pa.int64(), True))
+            continue
+        fld = schemas[side].field(col)
+        if f == AggregateFunction.Count:
+            t = pa.int64()
+        elif f == AggregateFunction.Sum:
+            t = pa.float64() if pa.types.is_float64(fld.type) else pa.int64()
+        elif f == AggregateFunction.Avg:
+            t = pa.float64()
+        else:
+            t = fld.type
+        fields.append(pa.field(f"{f.sql_name()}({fld.name})", t, True))
+    return a, pa.schema(fields), lv
+
+
+class Server:
+    """The serving loop (oxb_server_*): submit returns a ticket at once,
+    worker threads run admitted work on their own streams, and top-k requests
+    that differ only in query, k and per-query literal share a scan."""
+
+    def __init__(self, backend: "CudaBackend", memory_budget: int = 0, workers: int = 0, max_batch: int = 0):
+        self._backend = backend
+        cfg = _abi.ServerConfig(memory_budget, workers, max_batch)
+        h = C.c_void_p()
+        _abi.check(_L().oxb_server_create(backend.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h.value
+        self._schemas = {}
+
+    def submit_topk(self, index, input, predicate, query, k: int, metric, query_leaf=None) -> int:
+        """`query_leaf` = (column, Comparison, Literal): this query's own leaf,
+        appended to `predicate`'s leaves."""
+        lfs = list(leaves(predicate))
+        if query_leaf is not None:
+            from .params import Compare
+
+            col, cmp, lit = query_leaf
+            lfs.append(Compare(col, cmp, lit))
+        arr = (_abi.Leaf * max(1, len(lfs)))()
+        for i, lf in enumerate(lfs):
+            arr[i].column = lf.column
+            arr[i].op = int(lf.op)
+            arr[i].lit_type = int(lf.literal.type)
+            if int(lf.literal.type) == 2:
+                arr[i].lit.f = float(lf.literal.value)
+            else:
+                arr[i].lit.i = int(lf.literal.value)
+        q = np.ascontiguousarray(np.asarray(query, dtype=np.float32))
+        r = _abi.TopkRequest(index.handle, input.handle, C.cast(arr, C.c_void_p), len(lfs),
+                             1 if query_leaf is not None else 0, q.ctypes.data, q.size, k, int(metric), 0)
+        t = C.c_uint64()
+        _abi.check(_L().oxb_server_submit_topk(self.handle, C.byref(r), C.byref(t)))
+        return t.value
+
+    def submit_join_aggregate(self, probe, probe_key, table, predicate, group, aggregates) -> int:
+        a, schema, keep = _join_aggregate_args(probe, probe_key, table, predicate, group, aggregates)
+        t = C.c_uint64()
+        _abi.check(_L().oxb_server_submit_join_aggregate(self.handle, C.byref(a), C.byref(t)))
+        self._schemas[t.value] = schema
+        return t.value
+
+    def wait_topk(self, ticket: int, k: int):
+        ids = np.empty(k, np.int64)
+        dist = np.empty(k, np.float32)
+        lat = C.c_double()
+        _abi.check(_L().oxb_server_wait_topk(self.handle, ticket, ids.ctypes.data, dist.ctypes.data, C.byref(lat)))
+        return ids, dist, lat.value
+
+    def wait_batch(self, ticket: int):
+        h = C.c_void_p()
+        lat = C.c_double()
+        schema = self._schemas.pop(ticket, None)
+        _abi.check(_L().oxb_server_wait_batch(self.handle, ticket, C.byref(h), C.byref(lat)))
+        return DeviceBatch(h.value, schema), lat.value
+
+    def stats(self, reset: bool = False) -> dict:
+        st = _abi.ServerStats()
+        _abi.check(_L().oxb_server_stats_get(self.handle, C.byref(st), 1 if reset else 0))
+        return {f: getattr(st, f) for f, _ in _abi.ServerStats._fields_}
+
+    def close(self) -> None:
+        h, self.handle = getattr(self, "handle", None), None
+        if h:
+            _L().oxb_server_destroy(h)
+
+    def __del__(self):
+        self.close()

@@ -504,6 +504,56 @@ oxb_status oxb_aggregate_batches(oxb_backend* backend, oxb_stream* stream, const
     OXB_CATCH
 }
 
+oxb_status oxb_server_create(oxb_backend* backend, const oxb_server_config* config, oxb_server** out) {
+    OXB_TRY
+    use_device(backend);
+    if (!out) fail(OXB_PLAN, "null argument");
+    oxb_server_config cfg{};
+    if (config) cfg = *config;
+    *out = server_create(backend, cfg);
+    OXB_CATCH
+}
+
+void oxb_server_destroy(oxb_server* server) { server_destroy(server); }
+
+oxb_status oxb_server_submit_topk(oxb_server* server, const oxb_topk_request* request, uint64_t* ticket) {
+    OXB_TRY
+    if (!server || !request || !ticket) fail(OXB_PLAN, "null argument");
+    *ticket = server_submit_topk(server, *request);
+    OXB_CATCH
+}
+
+oxb_status oxb_server_submit_join_aggregate(oxb_server* server, const oxb_join_aggregate_args* request,
+                                            uint64_t* ticket) {
+    OXB_TRY
+    if (!server || !request || !ticket) fail(OXB_PLAN, "null argument");
+    *ticket = server_submit_join_aggregate(server, *request);
+    OXB_CATCH
+}
+
+oxb_status oxb_server_wait_topk(oxb_server* server, uint64_t ticket, int64_t* ids, float* dist, double* latency_us) {
+    OXB_TRY
+    if (!server) fail(OXB_PLAN, "null argument");
+    const double l = server_wait(server, ticket, ids, dist, nullptr);
+    if (latency_us) *latency_us = l;
+    OXB_CATCH
+}
+
+oxb_status oxb_server_wait_batch(oxb_server* server, uint64_t ticket, oxb_batch** out, double* latency_us) {
+    OXB_TRY
+    if (!server) fail(OXB_PLAN, "null argument");
+    const double l = server_wait(server, ticket, nullptr, nullptr, out);
+    if (latency_us) *latency_us = l;
+    OXB_CATCH
+}
+
+oxb_status oxb_server_stats_get(oxb_server* server, oxb_server_stats* out, int32_t reset) {
+    OXB_TRY
+    if (!server || !out) fail(OXB_PLAN, "null argument");
+    server_stats(server, out, reset != 0);
+    OXB_CATCH
+}
+
 oxb_status oxb_vector_index_build(oxb_backend* backend, oxb_stream* stream, const oxb_batch* input, int32_t column,
                                   oxb_vector_index** out) {
     OXB_TRY

@@ -229,6 +229,12 @@ bool key_range(const StreamRef& s, const Backend& b, const Column& key, long lon
 oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter_project_args& a);
 AllocRef predicate_bits(const StreamRef& s, const Backend& b, const DevPredicate& pred, long long n);
 oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_aggregate_batches_args& a);
+oxb_server* server_create(oxb_backend* backend, const oxb_server_config& cfg);
+void server_destroy(oxb_server* srv);
+uint64_t server_submit_topk(oxb_server* srv, const oxb_topk_request& q);
+uint64_t server_submit_join_aggregate(oxb_server* srv, const oxb_join_aggregate_args& a);
+double server_wait(oxb_server* srv, uint64_t ticket, int64_t* ids, float* dist, oxb_batch** out);
+void server_stats(oxb_server* srv, oxb_server_stats* out, bool reset);
 oxb_vector_index* vector_index_build(const StreamRef& s, const Backend& b, const oxb_batch& in, int column);
 void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_args& a, int64_t* out_ids,
                  float* out_dist, oxb_vector_topk_stats* stats);
