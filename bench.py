@@ -288,29 +288,22 @@ def main() -> int:
         if dist is not None:
             dist.barrier()
 
+    # On more than one GPU each rank folds its shard into partial groups (AVG
+    # as SUM and COUNT); one exchange merges them into the query's result.
+    from oxidelake_b200.distributed import exchange_and_merge, partial_aggregates
+
+    partial, finish = partial_aggregates(aggs)
+    names = ["attr", "SUM(payload)", "SUM(qty)", "COUNT(*)", "AVG(payload)"]
+
     def exchange(res):
-        """All ranks' group partials: NCCL all_gather of padded columns."""
         if dist is None:
             return res
-        g = torch.tensor([res.num_rows], device="cuda")
-        sizes = [torch.zeros_like(g) for _ in range(world)]
-        dist.all_gather(sizes, g)
-        gmax = int(max(s.item() for s in sizes))
-        cols = []
-        for c in (0, 1, 2, 3):
-            t = torch.zeros(gmax, dtype=torch.float64, device="cuda")
-            t[: res.num_rows] = torch.from_numpy(res.column(c).to_numpy(zero_copy_only=False).astype(np.float64)).cuda()
-            parts = [torch.zeros_like(t) for _ in range(world)]
-            dist.all_gather(parts, t)
-            cols.append(parts)
-        return cols
+        return exchange_and_merge(res, partial, finish, names)
 
     def step():
         table = backend.prepare_join_build(stream, bdev, 0)
-        out = backend.join_aggregate(stream, pdev, 0, table, pred, (1, 1), aggs)
-        res = backend.download(stream, out)
-        exchange(res)
-        return res
+        out = backend.join_aggregate(stream, pdev, 0, table, pred, (1, 1), partial if dist is not None else aggs)
+        return exchange(backend.download(stream, out))
 
     # warm-up
     backend.set_kernel_timing(True)
@@ -355,9 +348,9 @@ def main() -> int:
         bd = backend.upload(stream, pin_build)
         pd = backend.upload(stream, pin_probe)
         table = backend.prepare_join_build(stream, bd, 0)
-        out = backend.download(stream, backend.join_aggregate(stream, pd, 0, table, pred, (1, 1), aggs))
-        exchange(out)
-        return out
+        out = backend.download(stream, backend.join_aggregate(stream, pd, 0, table, pred, (1, 1),
+                                                              partial if dist is not None else aggs))
+        return exchange(out)
 
     e2e_step()
     barrier()
