@@ -525,7 +525,10 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * build-side group key with a small span; its dense form when the build
  * keys fill at least a quarter of their range), 6 (the fused probe table,
  * hashed form), 7 or 8 (5 or 6 interpreted a vector of rows per thread at
- * a time); rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
+ * a time), 9 or 10 (oxb_aggregate_batches only: the hash-partitioned
+ * passes with the planned partitions, or with their fewest; there 0..8 pin
+ * the single persistent kernel);
+ * rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
  * 1 or 2, the fused kernels 2 or 4, the vector ones 4 or 8; other values
  * round to the nearest the kernel has). */
 OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);

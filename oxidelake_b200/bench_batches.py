@@ -6,7 +6,11 @@ Prints one JSON line per selectivity: kernel time (CUDA events), algorithmic
 GB/s (f and its bitmap for every row, key and x for the kept rows), the
 whole call's time and the group count.
 
-    python -m oxidelake_b200.bench_batches [--rows N]
+    python -m oxidelake_b200.bench_batches [--rows N] [--variant V]
+
+--variant pins the kernels as oxb_set_agg_variant does (-1 automatic, 9 the
+hash-partitioned passes, 0 the single persistent kernel).  The kernel time
+covers the pass over the input that sizes the table and the fold itself.
 """
 from __future__ import annotations
 
@@ -26,6 +30,7 @@ def main() -> int:
     ap.add_argument("--rows", type=int, default=200_000_000)
     ap.add_argument("--distinct", type=int, default=10_000_000)
     ap.add_argument("--repeats", type=int, default=2)
+    ap.add_argument("--variant", type=int, default=-1)
     args = ap.parse_args()
 
     from datagen import config3_batches
@@ -38,6 +43,7 @@ def main() -> int:
     b = CudaBackend(0)
     s = b.create_stream()
     b.set_kernel_timing(True)
+    b.set_agg_variant(args.variant, 0)
     devs = [b.upload(s, x) for x in batches]
     spec = AggregateSpec(0, [(F.Sum, 1), (F.Min, 1), (F.Max, 1), (F.Count, 1)])
     for sel in (1, 50, 99):
@@ -48,12 +54,13 @@ def main() -> int:
             out = b.aggregate_batches(s, devs, spec, pred)
             groups = out.num_rows()
             call.append((time.perf_counter() - t0) * 1e3)
-            kms.append(b.last_kernel_time()[1])
+            name, kt = b.last_kernel_time()
+            kms.append(kt)
         gb = args.rows * (4 + 1 / 8) / 1e9 + args.rows * sel / 100 * (8 + 4 + 1 / 8) / 1e9
         ms = min(kms)
         print(json.dumps({
             "workload": "grouped aggregate, many batches", "rows": args.rows, "batches": len(batches),
-            "distinct": args.distinct, "selectivity_pct": sel, "kernel_ms": round(ms, 3),
+            "distinct": args.distinct, "selectivity_pct": sel, "kernel": name, "kernel_ms": round(ms, 3),
             "algorithmic_gbs": round(gb / ms * 1e3, 1), "call_ms": round(min(call), 1), "groups": groups,
             "data": "synthetic",
         }), flush=True)

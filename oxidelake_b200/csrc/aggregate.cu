@@ -84,9 +84,17 @@ struct AggProgram {
     int wdirect;       // warp caches indexed by key - wdirect_lo (else tagged by key)
     long long wdirect_lo;
     unsigned int* status;
-    unsigned long long* fill;       // keys placed in the HBM table
-    unsigned long long fill_limit;  // 3/4 of capacity: no insert beyond it
+    unsigned int probe_limit;  // a new key is refused a slot this far past its home
 };
+
+// While the host can still retry with a larger table, a new key is refused
+// a slot more than kMaxInsertProbes slots past its home: at the planned
+// load (at most 1/2) such a run has odds far below 1e-20 a key, and a table
+// that the estimate left too small reaches it quickly.  A bound on the run
+// instead of a count of placed keys: a shared counter bumped once per group
+// serialises every insert of a many-group fold in one L2 slice.  The last
+// attempt takes every slot (probe_limit = capacity).
+constexpr unsigned kMaxInsertProbes = 256;
 
 struct AggKey {
     const void* values;
@@ -180,16 +188,10 @@ __device__ __forceinline__ long long global_slot(const AggProgram& P, bool kvali
         long long k = __ldcg(&P.keys[h]);
         if (k == key) return h;
         if (k == kEmptyKey) {
-            // Past 3/4 load a new key is refused (the host retries with a
-            // table sized for every row), which keeps every probe sequence short.
-            if (__ldcg(P.fill) >= P.fill_limit) break;
+            if (p >= P.probe_limit) break;
             unsigned long long old = atomicCAS((unsigned long long*)&P.keys[h], (unsigned long long)kEmptyKey,
                                                (unsigned long long)key);
-            if (old == (unsigned long long)kEmptyKey) {
-                atomicAdd(P.fill, 1ull);
-                return h;
-            }
-            if (old == (unsigned long long)key) return h;
+            if (old == (unsigned long long)kEmptyKey || old == (unsigned long long)key) return h;
         }
         h = (h + 1u) & (P.capacity - 1u);
     }
@@ -1801,14 +1803,19 @@ __device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const Jo
 
 // Adds a fused kernel's CTA table into the HBM table: each occupied slot's
 // rows and arrays, Float64 sums with their compensation.
-__device__ void fused_flush(const AggProgram& P, const unsigned int* rows, const unsigned long long* tab, int S) {
+// `keys` (shared memory) names each slot's key; null: slot i holds key
+// direct_lo + i.
+// `narrow`: bit a set when array a holds a 32-bit MIN/MAX in its low word.
+__device__ void fused_flush(const AggProgram& P, const unsigned int* rows, const unsigned long long* tab, int S,
+                            const long long* keys = nullptr, unsigned narrow = 0) {
     for (int i = threadIdx.x; i < S; i += blockDim.x) {
         if (rows[i] == 0) continue;
-        const long long g = global_slot(P, true, P.direct_lo + i);
+        const long long g = global_slot(P, true, keys ? keys[i] : P.direct_lo + i);
         if (g < 0) continue;
         atomicAdd(&P.arr[g], (unsigned long long)rows[i]);
         for (int a = 1; a < P.narrays; a++) {
-            const unsigned long long x = tab[a * S + i];
+            unsigned long long x = tab[a * S + i];
+            if ((narrow >> a) & 1u) x = (unsigned long long)(long long)(int)(unsigned)x;
             unsigned long long* d = P.arr + a * P.stride + g;
             switch (P.merge[a]) {
                 case kMergeAddU64:
@@ -2498,6 +2505,7 @@ bool plan_stream(const AggProgram& P, const DevPredicate& pred, const void* key_
 struct BatchCols {
     long long n;      // rows
     long long tile0;  // the batch's first tile in the queue
+    long long ptile0; // ... in the partitioning passes' queue (kPartTile rows per tile)
     const void* key;
     const uint8_t* key_valid;
     const void* vals[kMaxAccs];
@@ -2581,23 +2589,6 @@ __global__ void __launch_bounds__(kThreads) agg_batches_kernel(const __grid_cons
 constexpr int kHllBits = 12;
 constexpr int kHllRegs = 1 << kHllBits;
 
-__global__ void hll_kernel(const void* __restrict__ key, const uint8_t* __restrict__ valid, int type, long long n,
-                           unsigned* __restrict__ regs) {
-    __shared__ unsigned sr[kHllRegs];
-    for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x) sr[i] = 0;
-    __syncthreads();
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
-        if (!valid_at(valid, r)) continue;
-        const unsigned long long h = fmix64((unsigned long long)load_int(key, type, r) ^ 0x9E3779B97F4A7C15ull);
-        const unsigned idx = (unsigned)(h >> (64 - kHllBits));
-        const unsigned rank = (unsigned)__clzll((h << kHllBits) | (1ull << (kHllBits - 1))) + 1u;
-        atomicMax(&sr[idx], rank);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x)
-        if (sr[i]) atomicMax(&regs[i], sr[i]);
-}
-
 double hll_estimate(const std::vector<unsigned>& regs) {
     double sum = 0.0;
     int zeros = 0;
@@ -2610,6 +2601,534 @@ double hll_estimate(const std::vector<unsigned>& regs) {
     if (e <= 2.5 * m && zeros > 0) e = m * std::log(m / zeros);
     return e;
 }
+
+
+// ---- hash-partitioned folding, for many groups ------------------------------
+// With millions of groups the HBM table does not fit in L2 and the direct
+// fold costs about six random HBM accesses per row.  Instead the kept rows
+// are partitioned by the top bits of their key's hash, so that each final
+// partition holds a few hundred groups, and each partition is folded in a
+// shared-memory table of its own keys; each group then reaches the HBM table
+// once.  Partitions split the key space, so no two CTAs fold the same group.
+//
+//   count   kept rows per final partition (a shared histogram per CTA)
+//   split1  rows -> records (key, stored columns, validity byte) in F1 <= 128
+//           level-1 partitions: each 2048-row sub-tile reserves its slice of
+//           a partition with one atomic, so concurrent writes stay adjacent
+//   split2  each level-1 partition -> its F2 final partitions, alike
+//   fold    one final partition at a time in shared memory; keys that do not
+//           fit fold into HBM directly
+//
+// NULL keys and the key INT64_MIN fold into their HBM slots during split1.
+// A record is a whole number of 16-byte units: word 0 the key, then for one
+// Int32 column its value and the validity byte in word 1 (16 bytes), else
+// one word per column and a word of validity bits.
+
+constexpr int kPartTile = 8192;  // rows per tile of the count pass and the HLL
+constexpr int kSplitRows = 8;    // rows per thread in a split sub-tile
+constexpr int kSplitTile = kThreads * kSplitRows;
+constexpr int kMaxParts = 32768;
+constexpr int kMaxF1 = 128;
+constexpr int kMaxF2 = kMaxParts / kMaxF1;
+constexpr int kPartKeys = 256;   // keys per final partition the sizing aims at
+constexpr int kPartSlots = 1024; // shared slots of the fold (3/4 may fill)
+constexpr int kFoldRows = 4;     // rows in flight per thread in the fold
+constexpr int kScanThreads = 1024;  // the scan pass: one CTA per SM (shared fine histogram)
+constexpr int kFineBits = 15;       // fine histogram buckets: the top 15 bits of the partition hash
+constexpr int kFine = 1 << kFineBits;
+static_assert(kMaxParts == kFine, "final partitions are unions of fine buckets");
+constexpr unsigned long long kPartSeed = 0x5BD1E9955BD1E995ull;
+
+struct PartPlan {
+    int nparts;   // final partitions: a power of two
+    int shift;    // 64 - log2(nparts)
+    int f2_bits;  // log2(F2): final partition = level-1 partition * F2 + p2
+    int fstride;  // fine buckets per final partition: partition p starts at offs[p * fstride]
+    int ncols;    // input columns stored per record
+    bool compact; // one Int32 column: 16-byte records
+    int col_of_acc[kMaxAccs];  // the stored column an accumulator reads
+    int width[kMaxAccs];       // bytes per stored column (4 or 8)
+    int src_of_col[kMaxAccs];  // an accumulator reading each stored column
+    uint4* recs;   // level-1 partitions
+    uint4* recs2;  // final partitions (recs again when F2 == 1)
+};
+
+__device__ __forceinline__ unsigned long long part_hash(long long key) {
+    return fmix64((unsigned long long)key ^ kPartSeed);
+}
+
+__device__ __forceinline__ int part_of(const PartPlan& pp, long long key) { return (int)(part_hash(key) >> pp.shift); }
+
+// The batch holding partitioning tile t: the last whose first tile is <= t.
+__device__ __forceinline__ int batch_of_tile(const BatchCols* batches, int nb, long long t) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (batches[mid].ptile0 <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool keep_row(const DevPredicate& pred, const BatchCols& B, long long r) {
+    for (int l = 0; l < pred.nleaves; l++) {
+        const DevLeaf& lf = pred.leaves[l];
+        if (!valid_at(B.lvalid[l], r)) return false;
+        const long long a = lf.type == kFloat64 ? filter_order_key(__ldg((const double*)B.lvals[l] + r))
+                            : lf.type == kInt64 ? __ldg((const long long*)B.lvals[l] + r)
+                                                : (long long)__ldg((const int*)B.lvals[l] + r);
+        if (!cmp_holds(lf.op, a, lf.lit)) return false;
+    }
+    return true;
+}
+
+// Rows r0 + j * T (j < R, below `end`) that pass the WHERE and have a
+// valid key, with their keys: every leaf's loads issued before any test.
+template <int R, int T = kThreads>
+__device__ __forceinline__ unsigned kept_keys(const DevPredicate& pred, const BatchCols& B, int key_type, long long r0,
+                                              long long end, long long* key, unsigned* nullkey) {
+    unsigned live = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++)
+        if (r0 + (long long)j * T < end) live |= 1u << j;
+    unsigned keep = live;
+    for (int l = 0; l < pred.nleaves; l++) {
+        const DevLeaf& lf = pred.leaves[l];
+        long long a[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const long long r = r0 + (long long)j * T;
+            a[j] = 0;
+            if (!((keep >> j) & 1u)) continue;
+            if (!valid_at(B.lvalid[l], r)) {
+                keep &= ~(1u << j);
+                continue;
+            }
+            a[j] = lf.type == kFloat64 ? filter_order_key(__ldg((const double*)B.lvals[l] + r))
+                   : lf.type == kInt64 ? __ldg((const long long*)B.lvals[l] + r)
+                                       : (long long)__ldg((const int*)B.lvals[l] + r);
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (((keep >> j) & 1u) && !cmp_holds(lf.op, a[j], lf.lit)) keep &= ~(1u << j);
+    }
+    unsigned nk = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const long long r = r0 + (long long)j * T;
+        key[j] = 0;
+        if (!((keep >> j) & 1u)) continue;
+        if (!valid_at(B.key_valid, r)) {
+            nk |= 1u << j;
+            continue;
+        }
+        key[j] = load_int(B.key, key_type, r);
+        if (key[j] == kEmptyKey) nk |= 1u << j;
+    }
+    *nullkey = nk;  // kept rows whose key is NULL or INT64_MIN
+    return keep & ~nk;
+}
+
+// The one pass over the input before the fold: for the kept rows with a
+// valid key (not INT64_MIN), (1) HyperLogLog registers of their keys
+// (2^kHllBits registers: a key's register is the top bits of its partition
+// hash, its rank the leading zeros of the rest plus one), which size the
+// HBM table and pick the path; (2) their count; (3) their histogram over
+// kFine buckets (the top kFineBits bits of the same hash), from which the
+// partitioned path takes every partition's size.
+__global__ void __launch_bounds__(kScanThreads) part_scan_kernel(const __grid_constant__ DevPredicate pred, int key_type,
+                                                                 const BatchCols* __restrict__ batches, int nb,
+                                                                 long long ntiles, unsigned* __restrict__ regs,
+                                                                 unsigned int* __restrict__ fine,
+                                                                 unsigned long long* __restrict__ kept) {
+    extern __shared__ unsigned int scan_smem[];
+    unsigned* sr = scan_smem;             // kHllRegs
+    unsigned* hist = scan_smem + kHllRegs;  // kFine
+    for (int i = threadIdx.x; i < kHllRegs + kFine; i += blockDim.x) scan_smem[i] = 0;
+    __syncthreads();
+    unsigned n = 0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchCols& B = batches[batch_of_tile(batches, nb, t)];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
+        for (long long r0 = base + threadIdx.x; r0 < end; r0 += (long long)kScanThreads * 4) {
+            long long key[4];
+            unsigned nk;
+            const unsigned m = kept_keys<4, kScanThreads>(pred, B, key_type, r0, end, key, &nk);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (!((m >> j) & 1u)) continue;
+                const unsigned long long h = part_hash(key[j]);
+                const unsigned rank = (unsigned)__clzll((h << kHllBits) | (1ull << (kHllBits - 1))) + 1u;
+                atomicMax(&sr[h >> (64 - kHllBits)], rank);
+                atomicAdd(&hist[h >> (64 - kFineBits)], 1u);
+                n++;
+            }
+        }
+    }
+    // kept rows: a warp sum, then one atomic a warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(kept, (unsigned long long)n);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHllRegs; i += blockDim.x)
+        if (sr[i]) atomicMax(&regs[i], sr[i]);
+    for (int i = threadIdx.x; i < kFine; i += blockDim.x)
+        if (hist[i]) atomicAdd(&fine[i], hist[i]);
+}
+
+// Split pass 1: tiles of rows from a queue; each sub-tile of kSplitTile rows
+// ranks its kept rows per level-1 partition in shared memory, reserves each
+// partition's slice with one atomic on cursor1, and writes the records.
+template <int MAXACC>
+__global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_constant__ AggProgram P,
+                                                               const __grid_constant__ DevPredicate pred, int key_type,
+                                                               const BatchCols* __restrict__ batches, int nb,
+                                                               long long ntiles, unsigned long long* __restrict__ queue,
+                                                               const __grid_constant__ PartPlan pp,
+                                                               unsigned long long* __restrict__ cursor1) {
+    __shared__ unsigned int hist[kMaxF1];
+    __shared__ unsigned long long base1[kMaxF1];
+    __shared__ long long s_tile;
+    const int f1 = pp.nparts >> pp.f2_bits;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const long long t = s_tile;
+        if (t >= ntiles) break;
+        const BatchCols& B = batches[batch_of_tile(batches, nb, t)];
+        const long long tbase = (t - B.ptile0) * kPartTile;
+        const long long tend = tbase + kPartTile < B.n ? tbase + kPartTile : B.n;
+        for (long long sub = tbase; sub < tend; sub += kSplitTile) {
+            if (threadIdx.x < kMaxF1) hist[threadIdx.x] = 0;
+            __syncthreads();
+            long long key[kSplitRows];
+            unsigned nk;
+            const unsigned m = kept_keys<kSplitRows>(pred, B, key_type, sub + threadIdx.x, tend, key, &nk);
+            unsigned rank[kSplitRows];
+#pragma unroll
+            for (int j = 0; j < kSplitRows; j++) {
+                rank[j] = 0;
+                if ((m >> j) & 1u) {
+                    const int p1 = part_of(pp, key[j]) >> pp.f2_bits;
+                    rank[j] = (unsigned)p1 << 24 | atomicAdd(&hist[p1], 1u);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < f1 && hist[threadIdx.x])
+                base1[threadIdx.x] = atomicAdd(&cursor1[threadIdx.x], (unsigned long long)hist[threadIdx.x]);
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < kSplitRows; j++) {
+                const long long r = sub + threadIdx.x + (long long)j * kThreads;
+                if ((nk >> j) & 1u) {
+                    // NULL group and the key INT64_MIN: straight into their HBM slots.
+                    const bool kv = valid_at(B.key_valid, r);
+                    unsigned long long val[MAXACC];
+                    double comp[MAXACC];
+#pragma unroll
+                    for (int q = 0; q < MAXACC; q++) {
+                        comp[q] = 0.0;
+                        if (q >= P.nacc) break;
+                        const DevAcc& a = P.acc[q];
+                        const bool v = valid_at(B.valid[q], r);
+                        long long raw = 0;
+                        if (v && a.kind != kAccCount)
+                            raw = a.in_type == kInt32 ? (long long)__ldg((const int*)B.vals[q] + r)
+                                                      : __ldg((const long long*)B.vals[q] + r);
+                        val[q] = contribution_raw(a.kind, a.in_type, v, raw);
+                    }
+                    const long long g = global_slot(P, kv, kv ? kEmptyKey : 0);
+                    if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+                    continue;
+                }
+                if (!((m >> j) & 1u)) continue;
+                const unsigned long long pos = base1[rank[j] >> 24] + (rank[j] & 0xFFFFFFu);
+                constexpr int W = MAXACC + 2;  // key, columns, validity
+                unsigned long long w[W];
+                unsigned long long flags = 0;
+#pragma unroll
+                for (int i = 0; i < W; i++) w[i] = 0;
+                w[0] = (unsigned long long)key[j];
+#pragma unroll
+                for (int c = 0; c < MAXACC; c++) {
+                    if (c >= pp.ncols) break;
+                    const int q = pp.src_of_col[c];
+                    const bool v = valid_at(B.valid[q], r);
+                    flags |= (unsigned long long)v << c;
+                    if (v)
+                        w[1 + c] = pp.width[c] == 4 ? (unsigned long long)(long long)__ldg((const int*)B.vals[q] + r)
+                                                    : (unsigned long long)__ldg((const long long*)B.vals[q] + r);
+                }
+                if (pp.compact) {
+                    pp.recs[pos] = make_uint4((unsigned)w[0], (unsigned)(w[0] >> 32), (unsigned)w[1], (unsigned)flags);
+                    continue;
+                }
+#pragma unroll
+                for (int i = 1; i < W; i++)
+                    if (i == 1 + pp.ncols) w[i] = flags;
+                const int units = (pp.ncols + 3) >> 1;
+                uint4* o = pp.recs + pos * units;
+#pragma unroll
+                for (int u = 0; u < W / 2; u++)
+                    if (u < units)
+                        o[u] = make_uint4((unsigned)w[2 * u], (unsigned)(w[2 * u] >> 32), (unsigned)w[2 * u + 1],
+                                          (unsigned)(w[2 * u + 1] >> 32));
+            }
+        }
+    }
+}
+
+// The first split-2 tile of each level-1 partition (kSplitTile records a
+// tile) and, at [f1], their total.
+__global__ void part_tiles_kernel(const unsigned long long* __restrict__ offs, int f1, int f2, int fstride,
+                                  long long* __restrict__ tstart) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    long long t = 0;
+    const long long step = (long long)f2 * fstride;  // fine buckets a level-1 partition
+    for (int i = 0; i < f1; i++) {
+        tstart[i] = t;
+        const unsigned long long n = offs[(i + 1) * step] - offs[i * step];
+        t += (long long)((n + kSplitTile - 1) / kSplitTile);
+    }
+    tstart[f1] = t;
+}
+
+// Split pass 2: tiles of one level-1 partition's records from a queue, each
+// ranked per final partition in shared memory, reserved with one atomic per
+// final partition on cursor2 and copied.
+template <int UNITS>
+__global__ void __launch_bounds__(kThreads) part_split2_kernel(const __grid_constant__ PartPlan pp,
+                                                               const unsigned long long* __restrict__ offs,
+                                                               const long long* __restrict__ tstart,
+                                                               unsigned long long* __restrict__ queue,
+                                                               unsigned long long* __restrict__ cursor2) {
+    __shared__ unsigned int hist[kMaxF2];
+    __shared__ unsigned long long base2[kMaxF2];
+    __shared__ long long s_tile;
+    const int f2 = 1 << pp.f2_bits, f1 = pp.nparts >> pp.f2_bits;
+    const long long ntiles = tstart[f1];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const long long t = s_tile;
+        if (t >= ntiles) break;
+        int lo = 0, hi = f1 - 1;  // the last level-1 partition whose first tile is <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tstart[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const int p1 = lo;
+        const long long step = (long long)f2 * pp.fstride;
+        const unsigned long long first = offs[p1 * step] + (unsigned long long)(t - tstart[p1]) * kSplitTile;
+        const unsigned long long last = offs[(p1 + 1) * step];
+        const unsigned long long end = first + kSplitTile < last ? first + kSplitTile : last;
+        for (int i = threadIdx.x; i < kMaxF2; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        uint4 rec[kSplitRows][UNITS];
+        unsigned rank[kSplitRows];
+#pragma unroll
+        for (int j = 0; j < kSplitRows; j++) {
+            const unsigned long long i = first + threadIdx.x + (unsigned long long)j * kThreads;
+            rank[j] = 0xFFFFFFFFu;
+            if (i >= end) continue;
+#pragma unroll
+            for (int u = 0; u < UNITS; u++) rec[j][u] = __ldcs(pp.recs + i * UNITS + u);
+        }
+#pragma unroll
+        for (int j = 0; j < kSplitRows; j++) {
+            const unsigned long long i = first + threadIdx.x + (unsigned long long)j * kThreads;
+            if (i >= end) continue;
+            const long long key = (long long)((unsigned long long)rec[j][0].x | (unsigned long long)rec[j][0].y << 32);
+            const int p2 = part_of(pp, key) & (f2 - 1);
+            rank[j] = (unsigned)p2 << 24 | atomicAdd(&hist[p2], 1u);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < f2; i += blockDim.x)
+            if (hist[i]) base2[i] = atomicAdd(&cursor2[(long long)p1 * f2 + i], (unsigned long long)hist[i]);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSplitRows; j++) {
+            if (rank[j] == 0xFFFFFFFFu) continue;
+            const unsigned long long pos = base2[rank[j] >> 24] + (rank[j] & 0xFFFFFFu);
+#pragma unroll
+            for (int u = 0; u < UNITS; u++) pp.recs2[pos * UNITS + u] = rec[j][u];
+        }
+    }
+}
+
+// A fold row whose key found no shared slot, into the HBM table (out of
+// line, its values passed by value so that the caller keeps them in registers).
+template <int MAXACC>
+__device__ __noinline__ void part_row_to_hbm(const AggProgram& P, long long key, unsigned long long v0,
+                                             unsigned long long v1, unsigned long long v2, unsigned long long v3) {
+    unsigned long long val[4] = {v0, v1, v2, v3};
+    double comp[4] = {0.0, 0.0, 0.0, 0.0};
+    const long long g = global_slot(P, true, key);
+    if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+}
+
+// Fold: one final partition at a time (rows offs[p] .. offs[p + 1] of
+// recs2) in a shared table of its keys; kFoldRows records in flight per
+// thread.  Keys that find no shared slot fold into HBM directly.
+template <int MAXACC, int UNITS>
+__global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_constant__ AggProgram P,
+                                                             const __grid_constant__ PartPlan pp,
+                                                             const unsigned long long* __restrict__ offs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int S = kPartSlots;
+    long long* keys = (long long*)smem;
+    unsigned int* rows = (unsigned int*)(keys + S);
+    unsigned long long* tab = (unsigned long long*)(rows + S) - S;  // array a at tab + a * S
+    __shared__ int fill;
+    // MIN/MAX of an Int32 column: 32-bit shared atomics on the low word
+    // (64-bit shared MIN/MAX/ADD are not single instructions).  A group's
+    // value is only emitted when it has a non-NULL input, so the 32-bit
+    // identity never reaches a result.
+    unsigned narrow = 0;
+    for (int q = 0; q < P.nacc; q++)
+        if (P.acc[q].in_type == kInt32 && (P.acc[q].kind == kAccMin || P.acc[q].kind == kAccMax))
+            narrow |= 1u << P.acc[q].arr;
+    for (int part = blockIdx.x; part < pp.nparts; part += gridDim.x) {
+        for (int i = threadIdx.x; i < S; i += blockDim.x) {
+            keys[i] = kEmptyKey;
+            rows[i] = 0;
+        }
+        for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) {
+            const int a = 1 + i / S;
+            tab[S + i] = (narrow >> a) & 1u ? (P.init[a] == kInitMax ? 0x7fffffffull : 0x80000000ull)
+                                            : init_value(P.init[a]);
+        }
+        if (threadIdx.x == 0) fill = 0;
+        __syncthreads();
+        const unsigned long long lo = offs[(long long)part * pp.fstride], hi = offs[(long long)(part + 1) * pp.fstride];
+        for (unsigned long long b0 = lo + threadIdx.x; b0 < hi; b0 += (unsigned long long)kThreads * kFoldRows) {
+            uint4 rec[kFoldRows][UNITS];
+#pragma unroll
+            for (int j = 0; j < kFoldRows; j++) {
+                const unsigned long long i = b0 + (unsigned long long)j * kThreads;
+                if (i < hi) {
+#pragma unroll
+                    for (int u = 0; u < UNITS; u++) rec[j][u] = __ldcs(pp.recs2 + i * UNITS + u);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kFoldRows; j++) {
+                if (b0 + (unsigned long long)j * kThreads >= hi) break;
+                unsigned long long w[2 * UNITS];
+#pragma unroll
+                for (int u = 0; u < UNITS; u++) {
+                    w[2 * u] = (unsigned long long)rec[j][u].x | (unsigned long long)rec[j][u].y << 32;
+                    w[2 * u + 1] = (unsigned long long)rec[j][u].z | (unsigned long long)rec[j][u].w << 32;
+                }
+                const long long key = (long long)w[0];
+                unsigned long long flags = 0;
+                if (UNITS == 1) {
+                    flags = rec[j][0].w;
+                } else {
+#pragma unroll
+                    for (int i = 1; i < 2 * UNITS; i++)
+                        if (i == 1 + pp.ncols) flags = w[i];
+                }
+                unsigned long long val[MAXACC];
+#pragma unroll
+                for (int q = 0; q < MAXACC; q++) {
+                    val[q] = 0;
+                    if (q >= P.nacc) break;
+                    const DevAcc& a = P.acc[q];
+                    const int c = pp.col_of_acc[q];
+                    const bool v = (flags >> c) & 1u;
+                    long long raw = 0;
+                    if (UNITS == 1) {
+                        raw = (long long)(int)rec[j][0].z;
+                    } else {
+#pragma unroll
+                        for (int i = 1; i < 2 * UNITS; i++)
+                            if (i == 1 + c) raw = (long long)w[i];
+                    }
+                    val[q] = contribution_raw(a.kind, a.in_type, v, raw);
+                }
+                // This partition's shared slot of the key; HBM when there is none.
+                int slot = -1;
+                unsigned int h = (unsigned int)(fmix64((unsigned long long)key) & (unsigned)(S - 1));
+                for (int q = 0; q < 64; q++) {
+                    const long long k = ((volatile long long*)keys)[h];
+                    if (k == key) {
+                        slot = (int)h;
+                        break;
+                    }
+                    if (k == kEmptyKey) {
+                        if (*(volatile int*)&fill >= S * 3 / 4) break;
+                        const unsigned long long old = atomicCAS((unsigned long long*)&keys[h],
+                                                                 (unsigned long long)kEmptyKey, (unsigned long long)key);
+                        if (old == (unsigned long long)kEmptyKey) {
+                            atomicAdd(&fill, 1);
+                            slot = (int)h;
+                            break;
+                        }
+                        if ((long long)old == key) {
+                            slot = (int)h;
+                            break;
+                        }
+                    }
+                    h = (h + 1u) & (unsigned)(S - 1);
+                }
+                if (slot < 0) {
+                    part_row_to_hbm<MAXACC>(P, key, val[0], val[1], MAXACC > 2 ? val[2 % MAXACC] : 0,
+                                            MAXACC > 3 ? val[3 % MAXACC] : 0);
+                    continue;
+                }
+                atomicAdd(&rows[slot], 1u);
+#pragma unroll
+                for (int q = 0; q < MAXACC; q++) {
+                    if (q >= P.nacc) break;
+                    const DevAcc& a = P.acc[q];
+                    unsigned long long* p = tab + a.arr * S + slot;
+                    unsigned* w32 = (unsigned*)p;  // little-endian: [0] the low word
+                    switch (a.kind) {
+                        case kAccCount:  // at most 2^32 rows a partition
+                            if (val[q]) atomicAdd(w32, 1u);
+                            break;
+                        case kAccSumInt: {
+                            // 64-bit wrapping add as a 32-bit add and its carry
+                            const unsigned vlo = (unsigned)val[q], vhi = (unsigned)(val[q] >> 32);
+                            const unsigned old = vlo ? atomicAdd(w32, vlo) : 0u;
+                            const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
+                            if (up) atomicAdd(w32 + 1, up);
+                            break;
+                        }
+                        case kAccSumF64: {
+                            const double x = as_f64(val[q]);
+                            const double old = atomicAdd((double*)p, x);
+                            double c = 0.0;
+                            two_sum_into(old, x, &c);
+                            if (c != 0.0) atomicAdd((double*)(p + S), c);
+                            break;
+                        }
+                        case kAccMin:
+                            if (val[q] == 0x7fffffffffffffffull) break;
+                            if ((narrow >> a.arr) & 1u) atomicMin((int*)w32, (int)val[q]);
+                            else atomicMin((long long*)p, (long long)val[q]);
+                            break;
+                        default:
+                            if (val[q] == 0x8000000000000000ull) break;
+                            if ((narrow >> a.arr) & 1u) atomicMax((int*)w32, (int)val[q]);
+                            else atomicMax((long long*)p, (long long)val[q]);
+                            break;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        fused_flush(P, rows, tab, S, keys, narrow);
+        __syncthreads();
+    }
+}
+
+size_t part_fold_smem(int narrays) { return (size_t)kPartSlots * (8 + 4 + 8 * (narrays - 1)); }
 
 int maxacc_for(int nacc) { return nacc <= 2 ? 2 : (nacc <= 4 ? 4 : kMaxAccs); }
 
@@ -2973,19 +3492,16 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
 
     for (int attempt = 0; attempt < 2; attempt++) {
         P.capacity = cap;
+        P.probe_limit = attempt == 0 ? kMaxInsertProbes : cap;
         P.stride = (long long)cap + 2;
         AllocRef keys_mem = dev_alloc(s, (size_t)cap * 8, false);
         AllocRef arr_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
         Scratch<unsigned int> status(s, 1, true);
-        Scratch<unsigned long long> fill(s, 1, true);
         P.keys = (long long*)keys_mem->ptr;
         P.arr = (unsigned long long*)arr_mem->ptr;
         P.status = status.get();
-        P.fill = fill.get();
-        P.fill_limit = (unsigned long long)cap / 4 * 3;
         auto init = [&]() {
             OXB_CUDA(cudaMemsetAsync(status.get(), 0, 4, s->stream));
-            OXB_CUDA(cudaMemsetAsync(fill.get(), 0, 8, s->stream));
             note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(P);
             OXB_CUDA(cudaGetLastError());
         };
@@ -3092,14 +3608,16 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
     AggProgram& P = plan.P;
     const int* acc_col = plan.acc_index;
     std::vector<BatchCols> hb(a.ninputs);
-    long long ntiles = 0, total = 0;
+    long long ntiles = 0, nptiles = 0, total = 0;
     for (int i = 0; i < a.ninputs; i++) {
         const oxb_batch& bt = *a.inputs[i];
         BatchCols& c = hb[i];
         c = BatchCols{};
         c.n = bt.rows;
         c.tile0 = ntiles;
+        c.ptile0 = nptiles;
         ntiles += (bt.rows + kBatchTile - 1) / kBatchTile;
+        nptiles += (bt.rows + kPartTile - 1) / kPartTile;
         total += bt.rows;
         c.key = bt.cols[spec.group_by].values;
         c.key_valid = bt.cols[spec.group_by].validity;
@@ -3115,16 +3633,28 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
     Scratch<BatchCols> dbatches(s, hb.size());
     OXB_CUDA(cudaMemcpyAsync(dbatches.get(), hb.data(), hb.size() * sizeof(BatchCols), cudaMemcpyHostToDevice, s->stream));
 
-    // Distinct keys across every batch, for the table's size.
+    // One pass over the input: distinct keys and count of the kept rows, and
+    // their fine partition histogram (KernelTimer: this pass plus the fold).
+    KernelTimer timer(b, s, "agg_batches_kernel");
     Scratch<unsigned> regs(s, kHllRegs, true);
-    for (int i = 0; i < a.ninputs; i++) {
-        if (hb[i].n == 0) continue;
-        note_launch(), hll_kernel<<<grid_for(b, hb[i].n, 256, 4), 256, 0, s->stream>>>(hb[i].key, hb[i].key_valid, key.type,
-                                                                                     hb[i].n, regs.get());
+    Scratch<unsigned int> fine(s, kFine, true);
+    Scratch<unsigned long long> kept_dev(s, 1, true);
+    const size_t scan_smem = (size_t)(kHllRegs + kFine) * 4;
+    set_smem(part_scan_kernel, scan_smem);
+    timer.begin();
+    if (nptiles > 0) {
+        int socc = 0;
+        OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&socc, part_scan_kernel, kScanThreads, scan_smem));
+        const long long sgrid0 = std::max<long long>(1, std::min<long long>(nptiles, (long long)b.sms * std::max(socc, 1)));
+        note_launch(), part_scan_kernel<<<(unsigned)sgrid0, kScanThreads, scan_smem, s->stream>>>(
+            pred, key.type, dbatches.get(), a.ninputs, nptiles, regs.get(), fine.get(), kept_dev.get());
+        OXB_CUDA(cudaGetLastError());
     }
-    OXB_CUDA(cudaGetLastError());
+    timer.end();
     std::vector<unsigned> hregs(kHllRegs);
+    unsigned long long kept = 0;
     OXB_CUDA(cudaMemcpyAsync(hregs.data(), regs.get(), kHllRegs * 4, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&kept, kept_dev.get(), 8, cudaMemcpyDeviceToHost, s->stream));
     OXB_CUDA(cudaStreamSynchronize(s->stream));
     const double est = hll_estimate(hregs);
     const long long all_rows = next_pow2(2 * std::max<long long>(total, 1), 4096);
@@ -3136,28 +3666,110 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
     int per_sm = 0;
     OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0));
     const long long grid = std::max<long long>(1, std::min<long long>(ntiles, (long long)b.sms * std::max(per_sm, 1)));
+
+    // The hash-partitioned passes pay two more passes over the kept rows and
+    // a second read of the input; they win when the HBM table is well beyond
+    // L2 (each kept row then costs the direct fold several random HBM
+    // accesses) and enough rows are kept: measured on B200, about 0.22 ms per
+    // million kept rows direct against 0.10 partitioned, plus about 9 us per
+    // million input rows.  The stored columns are the distinct inputs of the
+    // accumulators.  Pinned variants: 9 the partitioned passes as planned,
+    // 10 with the fewest partitions (so that partitions overflow their shared
+    // tables), 0..8 the direct kernel.
+    PartPlan pp{};
+    const bool pinned = b.force_combine >= 0;
+    const double table_bytes = (double)cap * 8.0 * (1 + P.narrays);
+    const bool worth = table_bytes > 64.0 * (1 << 20) && (double)kept >= (double)total / 12.0 + 4e6;
+    bool partitioned = maxacc <= 4 && total < (1ll << 32) && nptiles > 0 &&
+                       (pinned ? (b.force_combine == 9 || b.force_combine == 10) : worth);
+    if (partitioned) {
+        for (int j = 0; j < P.nacc; j++) {
+            int c = 0;
+            while (c < pp.ncols && plan.acc_index[pp.src_of_col[c]] != acc_col[j]) c++;
+            if (c == pp.ncols) {
+                pp.src_of_col[c] = j;
+                pp.width[c] = rep[acc_col[j]].type == kInt32 ? 4 : 8;
+                pp.ncols++;
+            }
+            pp.col_of_acc[j] = c;
+        }
+        int np = 64, lg = 6;
+        while (b.force_combine != 10 && np < kMaxParts && (double)np * kPartKeys < est) {
+            np <<= 1;
+            lg++;
+        }
+        pp.nparts = np;
+        pp.shift = 64 - lg;
+        pp.fstride = kFine >> lg;
+        pp.f2_bits = lg > 7 ? lg - 7 : 0;  // at most kMaxF1 level-1 partitions
+        pp.compact = pp.ncols == 1 && pp.width[0] == 4;
+    }
+    const int units = pp.compact ? 1 : (pp.ncols + 3) >> 1;
+    AllocRef recs_mem, recs2_mem;
+    if (partitioned) {
+        recs_mem = dev_alloc(s, (size_t)total * units * 16, false);
+        pp.recs = (uint4*)recs_mem->ptr;
+        pp.recs2 = pp.recs;
+        if (pp.f2_bits > 0) {
+            recs2_mem = dev_alloc(s, (size_t)total * units * 16, false);
+            pp.recs2 = (uint4*)recs2_mem->ptr;
+        }
+        timer.rename("agg_batches_partitioned");
+    }
+    auto psplit1 = maxacc == 2 ? part_split1_kernel<2> : part_split1_kernel<4>;
+    auto psplit2 = units == 1 ? part_split2_kernel<1> : (units == 2 ? part_split2_kernel<2> : part_split2_kernel<3>);
+    auto pfold = maxacc == 2 ? (units == 1 ? part_fold_kernel<2, 1> : part_fold_kernel<2, 2>)
+                             : (units == 1 ? part_fold_kernel<4, 1>
+                                           : (units == 2 ? part_fold_kernel<4, 2> : part_fold_kernel<4, 3>));
     for (int attempt = 0;; attempt++) {
         P.capacity = cap;
+        P.probe_limit = (long long)cap < all_rows ? kMaxInsertProbes : cap;
         P.stride = (long long)cap + 2;
         P.smem_slots = 0;
         P.wslots = 0;
         AllocRef keys_mem = dev_alloc(s, (size_t)cap * 8, false);
         AllocRef arr_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
         Scratch<unsigned int> status(s, 1, true);
-        Scratch<unsigned long long> fill(s, 1, true);
         Scratch<unsigned long long> queue(s, 1, true);
         P.keys = (long long*)keys_mem->ptr;
         P.arr = (unsigned long long*)arr_mem->ptr;
         P.status = status.get();
-        P.fill = fill.get();
-        P.fill_limit = (unsigned long long)cap / 4 * 3;
+        timer.begin();
         note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(P);
         OXB_CUDA(cudaGetLastError());
-        if (ntiles > 0) {
-            KernelTimer timer(b, s, "agg_batches_kernel");
-            timer.begin();
-            note_launch(), kern<<<(unsigned)grid, kThreads, 0, s->stream>>>(P, pred, key.type, dbatches.get(), a.ninputs,
-                                                                            ntiles, queue.get());
+        if (partitioned) {
+            const int f1 = pp.nparts >> pp.f2_bits, f2 = 1 << pp.f2_bits;
+            const size_t fsmem = part_fold_smem(P.narrays);
+            set_smem(pfold, fsmem);
+            // one CTA per unit of work (a tile, a partition) up to a full GPU
+            const long long sgrid = resident_grid(b, psplit1, 0, nptiles * kThreads);
+            const long long fgrid = resident_grid(b, pfold, fsmem, (long long)pp.nparts * kThreads);
+            Scratch<unsigned long long> offs(s, kFine + 1);
+            Scratch<unsigned long long> cursor1(s, f1);
+            Scratch<unsigned long long> cursor2(s, pp.nparts);
+            Scratch<long long> tstart(s, f1 + 1);
+            Scratch<unsigned long long> queue2(s, 1, true);
+            // every fine bucket's first record; partition p starts at bucket p * fstride
+            scan_u32_to_u64(s, b, fine.get(), offs.get(), kFine);
+            OXB_CUDA(cudaMemcpy2DAsync(cursor1.get(), 8, offs.get(), (size_t)f2 * pp.fstride * 8, 8, f1,
+                                       cudaMemcpyDeviceToDevice, s->stream));
+            note_launch(), psplit1<<<(unsigned)sgrid, kThreads, 0, s->stream>>>(P, pred, key.type, dbatches.get(), a.ninputs,
+                                                                               nptiles, queue.get(), pp, cursor1.get());
+            if (f2 > 1) {
+                OXB_CUDA(cudaMemcpy2DAsync(cursor2.get(), 8, offs.get(), (size_t)pp.fstride * 8, 8, pp.nparts,
+                                           cudaMemcpyDeviceToDevice, s->stream));
+                note_launch(), part_tiles_kernel<<<1, 32, 0, s->stream>>>(offs.get(), f1, f2, pp.fstride, tstart.get());
+                const long long grid2 = resident_grid(b, psplit2, 0, ((total + kSplitTile - 1) / kSplitTile + f1) * kThreads);
+                note_launch(), psplit2<<<(unsigned)grid2, kThreads, 0, s->stream>>>(pp, offs.get(), tstart.get(),
+                                                                                   queue2.get(), cursor2.get());
+            }
+            note_launch(), pfold<<<(unsigned)fgrid, kThreads, fsmem, s->stream>>>(P, pp, offs.get());
+            timer.end();
+            OXB_CUDA(cudaGetLastError());
+        } else {
+            if (ntiles > 0)
+                note_launch(), kern<<<(unsigned)grid, kThreads, 0, s->stream>>>(P, pred, key.type, dbatches.get(),
+                                                                                a.ninputs, ntiles, queue.get());
             timer.end();
             OXB_CUDA(cudaGetLastError());
         }

@@ -20,36 +20,47 @@ std::atomic<unsigned long long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 KernelTimer::KernelTimer(const Backend& b, const StreamRef& s, const char* name)
-    : on_(b.timing), name_(name), stream_(s->stream) {
-    if (on_) {
-        OXB_CUDA(cudaEventCreate(&start_));
-        OXB_CUDA(cudaEventCreate(&stop_));
-    }
-}
+    : on_(b.timing), name_(name), stream_(s->stream) {}
 
 void KernelTimer::begin() {
-    if (on_) OXB_CUDA(cudaEventRecord(start_, stream_));
+    if (!on_) return;
+    cudaEvent_t a = nullptr, z = nullptr;
+    OXB_CUDA(cudaEventCreate(&a));
+    if (cudaEventCreate(&z) != cudaSuccess) {
+        cudaEventDestroy(a);
+        fail(OXB_DEVICE, "cudaEventCreate failed");
+    }
+    segs_.emplace_back(a, z);
+    OXB_CUDA(cudaEventRecord(a, stream_));
 }
 
 void KernelTimer::end() {
-    if (on_) {
-        OXB_CUDA(cudaEventRecord(stop_, stream_));
+    if (on_ && !segs_.empty()) {
+        OXB_CUDA(cudaEventRecord(segs_.back().second, stream_));
         ended_ = true;
     }
 }
 
 KernelTimer::~KernelTimer() {
     if (!on_) return;
-    if (ended_ && cudaEventSynchronize(stop_) == cudaSuccess) {
-        float ms = 0.0f;
-        if (cudaEventElapsedTime(&ms, start_, stop_) == cudaSuccess) {
+    if (ended_ && cudaEventSynchronize(segs_.back().second) == cudaSuccess) {
+        float total = 0.0f;
+        bool ok = true;
+        for (auto& sg : segs_) {
+            float ms = 0.0f;
+            ok = ok && cudaEventElapsedTime(&ms, sg.first, sg.second) == cudaSuccess;
+            total += ms;
+        }
+        if (ok) {
             g_last_kernel = name_;
-            g_last_kernel_ms = ms;
+            g_last_kernel_ms = total;
         }
     }
     cudaGetLastError();
-    cudaEventDestroy(start_);
-    cudaEventDestroy(stop_);
+    for (auto& sg : segs_) {
+        cudaEventDestroy(sg.first);
+        cudaEventDestroy(sg.second);
+    }
 }
 
 void fail(oxb_status status, const std::string& message) { throw Error{status, message}; }
@@ -607,7 +618,7 @@ uint64_t oxb_kernel_launches(void) { return g_launches.load(); }
 oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread) {
     OXB_TRY
     if (!backend) fail(OXB_PLAN, "backend is null");
-    if (combine < -1 || combine > 8) fail(OXB_PLAN, "combine must be -1 or 0..8");
+    if (combine < -1 || combine > 10) fail(OXB_PLAN, "combine must be -1 or 0..10");
     if (rows_per_thread != 0 && rows_per_thread != 1 && rows_per_thread != 2 && rows_per_thread != 4 &&
         rows_per_thread != 8)
         fail(OXB_UNSUPPORTED, "rows per thread must be 0 (automatic), 1, 2 or 4");

@@ -91,14 +91,17 @@ class KernelTimer {
   public:
     KernelTimer(const Backend& b, const StreamRef& s, const char* name);
     ~KernelTimer();
+    // Each begin()/end() pair is one timed segment; the recorded time is
+    // the sum of the segments (host work between them is not counted).
     void begin();
     void end();
+    void rename(const char* name) { name_ = name; }
 
   private:
     bool on_;
     const char* name_;
     cudaStream_t stream_;
-    cudaEvent_t start_ = nullptr, stop_ = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> segs_;
     bool ended_ = false;
 };
 

@@ -28,12 +28,17 @@ def want(batches, spec, pred):
     return whole, oracle.aggregate(whole, spec.group_by, [(int(f), c) for f, c in spec.aggregates], leaves(pred))
 
 
+@pytest.mark.parametrize("variant", [-1, 9], ids=["auto", "partitioned"])
 @pytest.mark.parametrize("selectivity", [1, 50, 99])
-def test_high_cardinality_uneven_batches(backend, stream, selectivity):
+def test_high_cardinality_uneven_batches(backend, stream, selectivity, variant):
     batches = config3_batches(3_000_000, 200_000, seed=selectivity, min_rows=800, max_rows=400_000)
     assert len({b.num_rows for b in batches}) > 3
     pred = compare(2, Cmp.Lt, Literal.int32(selectivity))
-    got = fold(backend, stream, batches, SPEC, pred)
+    backend.set_agg_variant(variant, 0)
+    try:
+        got = fold(backend, stream, batches, SPEC, pred)
+    finally:
+        backend.set_agg_variant(-1, 0)
     _, w = want(batches, SPEC, pred)
     assert got.num_rows == w.num_rows
     assert_batches_equal(got, w)
@@ -68,3 +73,69 @@ def test_one_batch_equals_aggregate(backend, stream):
     single = backend.download(stream, backend.aggregate(stream, dev, SPEC))
     got = fold(backend, stream, batches, SPEC, None)
     assert_batches_equal(got, single)
+
+
+def _wide_batches(seed, distinct, sizes):
+    """Many groups with Float64 values that cancel (5 % NULL), an Int32
+    column without NULLs, NULL keys and the key INT64_MIN."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in sizes:
+        g = rng.integers(-distinct // 2, distinct // 2, n).astype(np.int64)
+        if n > 4:
+            g[:2] = np.iinfo(np.int64).min
+        v = rng.uniform(-1e6, 1e6, n) * rng.choice([1.0, 1e-9], n)
+        out.append(
+            pa.RecordBatch.from_arrays(
+                [pa.array(g, mask=rng.random(n) < 0.03), pa.array(v, mask=rng.random(n) < 0.05),
+                 pa.array(rng.integers(-1000, 1000, n).astype(np.int32)),
+                 pa.array(rng.integers(0, 100, n).astype(np.int32))],
+                names=["g", "v", "x", "f"],
+            )
+        )
+    return out
+
+
+@pytest.mark.parametrize("variant", [-1, 9, 10, 0], ids=["auto", "partitioned", "partitioned-64", "direct"])
+def test_many_groups_every_variant(backend, stream, variant):
+    """The hash-partitioned passes (two levels of partitions here; pinned
+    with 64 partitions their shared tables overflow into the HBM table) and
+    the single persistent kernel give the oracle's groups: Float64 SUM and
+    AVG to the stated tolerance, everything else bit-exact."""
+    batches = _wide_batches(40 + variant, 400_000, (0, 70_001, 1, 300_000, 8192, 0, 621_807))
+    # four accumulators (SUM, COUNT and MIN of v, MAX of x): two stored columns
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Avg, 1), (F.Min, 1), (F.Max, 2), (F.CountStar, 0), (F.Count, 1)])
+    pred = compare(3, Cmp.Lt, Literal.int32(70))
+    backend.set_agg_variant(variant, 0)
+    backend.set_kernel_timing(True)
+    try:
+        got = fold(backend, stream, batches, spec, pred)
+        name = backend.last_kernel_time()[0]
+    finally:
+        backend.set_agg_variant(-1, 0)
+        backend.set_kernel_timing(False)
+    if variant >= 0:
+        assert ("partitioned" in name) == (variant in (9, 10)), name
+    whole, w = want(batches, spec, pred)
+    scale = oracle.aggregate(abs_columns(whole, {1}), 0, [(int(f), c) for f, c in spec.aggregates], leaves(pred))
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w, float_sum_cols=(1, 2), scale=scale)
+
+
+def test_partitioned_int32_key_and_sums(backend, stream):
+    """An Int32 group key, integer SUM that wraps, and two accumulators on
+    one column: one stored column in the partition buffers."""
+    rng = np.random.default_rng(77)
+    batches = []
+    for n in (123_457, 500_000, 3):
+        g = rng.integers(-300_000, 300_000, n).astype(np.int32)
+        x = rng.integers(np.iinfo(np.int64).min // 2, np.iinfo(np.int64).max // 2, n, dtype=np.int64)
+        batches.append(pa.RecordBatch.from_arrays([pa.array(g, mask=rng.random(n) < 0.01), pa.array(x)], names=["g", "x"]))
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Min, 1), (F.Count, 1)])
+    backend.set_agg_variant(9, 0)  # about 600K groups: 4096 partitions in two levels
+    try:
+        got = fold(backend, stream, batches, spec, None)
+    finally:
+        backend.set_agg_variant(-1, 0)
+    _, w = want(batches, spec, None)
+    assert_batches_equal(got, w)
