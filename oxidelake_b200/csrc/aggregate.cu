@@ -1849,6 +1849,17 @@ __device__ __noinline__ void fused_slow(const AggProgram& P, const AggKey& gkey,
     fused_slow_row<4>(P, gkey, jt, s_or_special, i, val);
 }
 
+// A 64-bit wrapping add into shared memory as 32-bit atomics (the 64-bit
+// shared add is not a single instruction): the low word's add, then its
+// carry with the high word.
+__device__ __forceinline__ void shared_add_u64(unsigned long long* p, unsigned long long v) {
+    unsigned* w = (unsigned*)p;  // little-endian: w[0] the low word
+    const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    const unsigned old = lo ? atomicAdd(w, lo) : 0u;
+    const unsigned up = hi + (old + lo < old ? 1u : 0u);
+    if (up) atomicAdd(w + 1, up);
+}
+
 template <int MAXACC, int RPT, bool DENSE>
 __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
@@ -1907,12 +1918,12 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
         }
 #pragma unroll
         for (int r = 0; r < RPT; r++) {
-            if (sidx[r] == -2) continue;
             const long long i = base + r * (long long)blockDim.x + threadIdx.x;
             unsigned long long val[MAXACC];
 #pragma unroll
             for (int j = 0; j < MAXACC; j++) {
-                if (j >= P.nacc) break;
+                val[j] = 0;
+                if (j >= P.nacc || sidx[r] == -2) continue;
                 const DevAcc& a = P.acc[j];
                 const bool v = valid_at(a.validity, i);
                 long long raw = 0;
@@ -1920,6 +1931,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
                                                  : __ldcs((const long long*)a.values + i);
                 val[j] = contribution_raw(a.kind, a.in_type, v, raw);
             }
+            if (sidx[r] == -2) continue;
             if (cslot[r] < 0) {
                 fused_slow_row<MAXACC>(P, gkey, jt, sidx[r], i, val);
                 continue;
@@ -1934,7 +1946,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
                 switch (a.kind) {
                     case kAccCount:
                     case kAccSumInt:
-                        if (val[j]) atomicAdd(p, val[j]);
+                        if (val[j]) shared_add_u64(p, val[j]);
                         break;
                     case kAccSumF64: {
                         // The atomic rounds old + x once; TwoSum recovers that
