@@ -2792,6 +2792,29 @@ __global__ void __launch_bounds__(kScanThreads) part_scan_kernel(const __grid_co
 // Split pass 1: tiles of rows from a queue; each sub-tile of kSplitTile rows
 // ranks its kept rows per level-1 partition in shared memory, reserves each
 // partition's slice with one atomic on cursor1, and writes the records.
+// A kept row whose group key is NULL or INT64_MIN: straight into its HBM
+// slot (out of line: rare, and kept out of the split's instruction cache).
+template <int MAXACC>
+__device__ __noinline__ void part_null_row_to_hbm(const AggProgram& P, const BatchCols& B, long long r) {
+    const bool kv = valid_at(B.key_valid, r);
+    unsigned long long val[MAXACC];
+    double comp[MAXACC];
+#pragma unroll
+    for (int q = 0; q < MAXACC; q++) {
+        val[q] = 0;
+        comp[q] = 0.0;
+        if (q >= P.nacc) continue;
+        const DevAcc& a = P.acc[q];
+        const bool v = valid_at(B.valid[q], r);
+        long long raw = 0;
+        if (v && a.kind != kAccCount)
+            raw = a.in_type == kInt32 ? (long long)__ldg((const int*)B.vals[q] + r) : __ldg((const long long*)B.vals[q] + r);
+        val[q] = contribution_raw(a.kind, a.in_type, v, raw);
+    }
+    const long long g = global_slot(P, kv, kv ? kEmptyKey : 0);
+    if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
+}
+
 template <int MAXACC>
 __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_constant__ AggProgram P,
                                                                const __grid_constant__ DevPredicate pred, int key_type,
@@ -2831,62 +2854,53 @@ __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_cons
             if (threadIdx.x < f1 && hist[threadIdx.x])
                 base1[threadIdx.x] = atomicAdd(&cursor1[threadIdx.x], (unsigned long long)hist[threadIdx.x]);
             __syncthreads();
-#pragma unroll
-            for (int j = 0; j < kSplitRows; j++) {
+            // One row at a time from a register queue: a single copy of the
+            // row code, which stays in the instruction cache.
+            unsigned mm = m, nn = nk;
+#pragma unroll 1
+            for (int j = 0; j < kSplitRows && (mm | nn); j++) {
                 const long long r = sub + threadIdx.x + (long long)j * kThreads;
-                if ((nk >> j) & 1u) {
-                    // NULL group and the key INT64_MIN: straight into their HBM slots.
-                    const bool kv = valid_at(B.key_valid, r);
-                    unsigned long long val[MAXACC];
-                    double comp[MAXACC];
+                if (nn & 1u) {
+                    part_null_row_to_hbm<MAXACC>(P, B, r);
+                } else if (mm & 1u) {
+                    const unsigned long long pos = base1[rank[0] >> 24] + (rank[0] & 0xFFFFFFu);
+                    unsigned long long w[MAXACC + 2];  // key, columns, validity
+                    unsigned long long flags = 0;
 #pragma unroll
-                    for (int q = 0; q < MAXACC; q++) {
-                        comp[q] = 0.0;
-                        if (q >= P.nacc) break;
-                        const DevAcc& a = P.acc[q];
+                    for (int i = 0; i < MAXACC + 2; i++) w[i] = 0;
+                    w[0] = (unsigned long long)key[0];
+#pragma unroll
+                    for (int c = 0; c < MAXACC; c++) {
+                        if (c >= pp.ncols) break;
+                        const int q = pp.src_of_col[c];
                         const bool v = valid_at(B.valid[q], r);
-                        long long raw = 0;
-                        if (v && a.kind != kAccCount)
-                            raw = a.in_type == kInt32 ? (long long)__ldg((const int*)B.vals[q] + r)
-                                                      : __ldg((const long long*)B.vals[q] + r);
-                        val[q] = contribution_raw(a.kind, a.in_type, v, raw);
+                        flags |= (unsigned long long)v << c;
+                        if (v)
+                            w[1 + c] = pp.width[c] == 4 ? (unsigned long long)(long long)__ldg((const int*)B.vals[q] + r)
+                                                        : (unsigned long long)__ldg((const long long*)B.vals[q] + r);
                     }
-                    const long long g = global_slot(P, kv, kv ? kEmptyKey : 0);
-                    if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
-                    continue;
+                    if (pp.compact) {
+                        pp.recs[pos] = make_uint4((unsigned)w[0], (unsigned)(w[0] >> 32), (unsigned)w[1], (unsigned)flags);
+                    } else {
+#pragma unroll
+                        for (int i = 1; i < MAXACC + 2; i++)
+                            if (i == 1 + pp.ncols) w[i] = flags;
+                        const int units = (pp.ncols + 3) >> 1;
+                        uint4* o = pp.recs + pos * units;
+#pragma unroll
+                        for (int u = 0; u < (MAXACC + 2) / 2; u++)
+                            if (u < units)
+                                o[u] = make_uint4((unsigned)w[2 * u], (unsigned)(w[2 * u] >> 32), (unsigned)w[2 * u + 1],
+                                                  (unsigned)(w[2 * u + 1] >> 32));
+                    }
                 }
-                if (!((m >> j) & 1u)) continue;
-                const unsigned long long pos = base1[rank[j] >> 24] + (rank[j] & 0xFFFFFFu);
-                constexpr int W = MAXACC + 2;  // key, columns, validity
-                unsigned long long w[W];
-                unsigned long long flags = 0;
+                mm >>= 1;
+                nn >>= 1;
 #pragma unroll
-                for (int i = 0; i < W; i++) w[i] = 0;
-                w[0] = (unsigned long long)key[j];
-#pragma unroll
-                for (int c = 0; c < MAXACC; c++) {
-                    if (c >= pp.ncols) break;
-                    const int q = pp.src_of_col[c];
-                    const bool v = valid_at(B.valid[q], r);
-                    flags |= (unsigned long long)v << c;
-                    if (v)
-                        w[1 + c] = pp.width[c] == 4 ? (unsigned long long)(long long)__ldg((const int*)B.vals[q] + r)
-                                                    : (unsigned long long)__ldg((const long long*)B.vals[q] + r);
+                for (int t = 0; t + 1 < kSplitRows; t++) {
+                    key[t] = key[t + 1];
+                    rank[t] = rank[t + 1];
                 }
-                if (pp.compact) {
-                    pp.recs[pos] = make_uint4((unsigned)w[0], (unsigned)(w[0] >> 32), (unsigned)w[1], (unsigned)flags);
-                    continue;
-                }
-#pragma unroll
-                for (int i = 1; i < W; i++)
-                    if (i == 1 + pp.ncols) w[i] = flags;
-                const int units = (pp.ncols + 3) >> 1;
-                uint4* o = pp.recs + pos * units;
-#pragma unroll
-                for (int u = 0; u < W / 2; u++)
-                    if (u < units)
-                        o[u] = make_uint4((unsigned)w[2 * u], (unsigned)(w[2 * u] >> 32), (unsigned)w[2 * u + 1],
-                                          (unsigned)(w[2 * u + 1] >> 32));
             }
         }
     }
@@ -2972,20 +2986,54 @@ __global__ void __launch_bounds__(kThreads) part_split2_kernel(const __grid_cons
     }
 }
 
-// A fold row whose key found no shared slot, into the HBM table (out of
-// line, its values passed by value so that the caller keeps them in registers).
-template <int MAXACC>
-__device__ __noinline__ void part_row_to_hbm(const AggProgram& P, long long key, unsigned long long v0,
-                                             unsigned long long v1, unsigned long long v2, unsigned long long v3) {
-    unsigned long long val[4] = {v0, v1, v2, v3};
-    double comp[4] = {0.0, 0.0, 0.0, 0.0};
+// A record's input word for stored column c, and its validity bits.
+template <int UNITS>
+__device__ __forceinline__ long long rec_raw(const uint4* rec, int c) {
+    if (UNITS == 1) return (long long)(int)rec[0].z;  // one Int32 column
+    unsigned long long w = 0;
+#pragma unroll
+    for (int u = 0; u < UNITS; u++) {
+        const unsigned long long lo = (unsigned long long)rec[u].x | (unsigned long long)rec[u].y << 32;
+        const unsigned long long hi = (unsigned long long)rec[u].z | (unsigned long long)rec[u].w << 32;
+        if (2 * u == 1 + c) w = lo;
+        if (2 * u + 1 == 1 + c) w = hi;
+    }
+    return (long long)w;
+}
+
+template <int UNITS>
+__device__ __forceinline__ unsigned rec_flags(const PartPlan& pp, const uint4* rec) {
+    return UNITS == 1 ? rec[0].w : (unsigned)rec_raw<UNITS>(rec, pp.ncols);
+}
+
+// A fold record whose key found no shared slot, into the HBM table (out of
+// line: the common path keeps only its own code in the instruction cache).
+template <int MAXACC, int UNITS>
+__device__ __noinline__ void part_rec_to_hbm(const AggProgram& P, const PartPlan& pp, uint4 u0, uint4 u1, uint4 u2) {
+    const uint4 rec[3] = {u0, u1, u2};
+    const long long key = (long long)((unsigned long long)rec[0].x | (unsigned long long)rec[0].y << 32);
+    const unsigned flags = rec_flags<UNITS>(pp, rec);
+    unsigned long long val[MAXACC];
+    double comp[MAXACC];
+#pragma unroll
+    for (int q = 0; q < MAXACC; q++) {
+        val[q] = 0;
+        comp[q] = 0.0;
+        if (q >= P.nacc) continue;
+        const int c = pp.col_of_acc[q];
+        val[q] = contribution_raw(P.acc[q].kind, P.acc[q].in_type, (flags >> c) & 1u, rec_raw<UNITS>(rec, c));
+    }
     const long long g = global_slot(P, true, key);
     if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
 }
 
-// Fold: one final partition at a time (rows offs[p] .. offs[p + 1] of
-// recs2) in a shared table of its keys; kFoldRows records in flight per
-// thread.  Keys that find no shared slot fold into HBM directly.
+// Fold: one final partition at a time (records offs[p * fstride] ..
+// offs[(p + 1) * fstride] of recs2) in a shared table of its keys.  Each
+// thread loads kFoldRows records at once, then folds them one at a time from
+// a register queue: one copy of the row code, which keeps it in the
+// instruction cache (an unrolled copy per record and per accumulator kind
+// stalled the warps on instruction fetch).  Keys that find no shared slot
+// fold into HBM directly.
 template <int MAXACC, int UNITS>
 __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_constant__ AggProgram P,
                                                              const __grid_constant__ PartPlan pp,
@@ -3027,42 +3075,12 @@ __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_consta
                     for (int u = 0; u < UNITS; u++) rec[j][u] = __ldcs(pp.recs2 + i * UNITS + u);
                 }
             }
-#pragma unroll
-            for (int j = 0; j < kFoldRows; j++) {
-                if (b0 + (unsigned long long)j * kThreads >= hi) break;
-                unsigned long long w[2 * UNITS];
-#pragma unroll
-                for (int u = 0; u < UNITS; u++) {
-                    w[2 * u] = (unsigned long long)rec[j][u].x | (unsigned long long)rec[j][u].y << 32;
-                    w[2 * u + 1] = (unsigned long long)rec[j][u].z | (unsigned long long)rec[j][u].w << 32;
-                }
-                const long long key = (long long)w[0];
-                unsigned long long flags = 0;
-                if (UNITS == 1) {
-                    flags = rec[j][0].w;
-                } else {
-#pragma unroll
-                    for (int i = 1; i < 2 * UNITS; i++)
-                        if (i == 1 + pp.ncols) flags = w[i];
-                }
-                unsigned long long val[MAXACC];
-#pragma unroll
-                for (int q = 0; q < MAXACC; q++) {
-                    val[q] = 0;
-                    if (q >= P.nacc) break;
-                    const DevAcc& a = P.acc[q];
-                    const int c = pp.col_of_acc[q];
-                    const bool v = (flags >> c) & 1u;
-                    long long raw = 0;
-                    if (UNITS == 1) {
-                        raw = (long long)(int)rec[j][0].z;
-                    } else {
-#pragma unroll
-                        for (int i = 1; i < 2 * UNITS; i++)
-                            if (i == 1 + c) raw = (long long)w[i];
-                    }
-                    val[q] = contribution_raw(a.kind, a.in_type, v, raw);
-                }
+            const int nrec = (int)min((unsigned long long)kFoldRows, (hi - b0 + kThreads - 1) / kThreads);
+#pragma unroll 1
+            for (int j = 0; j < nrec; j++) {
+                const uint4* r0 = rec[0];
+                const long long key = (long long)((unsigned long long)r0[0].x | (unsigned long long)r0[0].y << 32);
+                const unsigned flags = rec_flags<UNITS>(pp, r0);
                 // This partition's shared slot of the key; HBM when there is none.
                 int slot = -1;
                 unsigned int h = (unsigned int)(fmix64((unsigned long long)key) & (unsigned)(S - 1));
@@ -3089,49 +3107,56 @@ __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_consta
                     h = (h + 1u) & (unsigned)(S - 1);
                 }
                 if (slot < 0) {
-                    part_row_to_hbm<MAXACC>(P, key, val[0], val[1], MAXACC > 2 ? val[2 % MAXACC] : 0,
-                                            MAXACC > 3 ? val[3 % MAXACC] : 0);
-                    continue;
-                }
-                atomicAdd(&rows[slot], 1u);
-#pragma unroll
-                for (int q = 0; q < MAXACC; q++) {
-                    if (q >= P.nacc) break;
-                    const DevAcc& a = P.acc[q];
-                    unsigned long long* p = tab + a.arr * S + slot;
-                    unsigned* w32 = (unsigned*)p;  // little-endian: [0] the low word
-                    switch (a.kind) {
-                        case kAccCount:  // at most 2^32 rows a partition
-                            if (val[q]) atomicAdd(w32, 1u);
-                            break;
-                        case kAccSumInt: {
-                            // 64-bit wrapping add as a 32-bit add and its carry
-                            const unsigned vlo = (unsigned)val[q], vhi = (unsigned)(val[q] >> 32);
-                            const unsigned old = vlo ? atomicAdd(w32, vlo) : 0u;
-                            const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
-                            if (up) atomicAdd(w32 + 1, up);
-                            break;
+                    part_rec_to_hbm<MAXACC, UNITS>(P, pp, r0[0], UNITS > 1 ? r0[UNITS > 1 ? 1 : 0] : r0[0],
+                                                   UNITS > 2 ? r0[UNITS > 2 ? 2 : 0] : r0[0]);
+                } else {
+                    atomicAdd(&rows[slot], 1u);
+#pragma unroll 1
+                    for (int q = 0; q < P.nacc; q++) {
+                        const DevAcc& a = P.acc[q];
+                        const int c = pp.col_of_acc[q];
+                        const unsigned long long v =
+                            contribution_raw(a.kind, a.in_type, (flags >> c) & 1u, rec_raw<UNITS>(r0, c));
+                        unsigned long long* p = tab + a.arr * S + slot;
+                        unsigned* w32 = (unsigned*)p;  // little-endian: [0] the low word
+                        switch (a.kind) {
+                            case kAccCount:  // at most 2^32 rows a partition
+                                if (v) atomicAdd(w32, 1u);
+                                break;
+                            case kAccSumInt: {
+                                // 64-bit wrapping add as a 32-bit add and its carry
+                                const unsigned vlo = (unsigned)v, vhi = (unsigned)(v >> 32);
+                                const unsigned old = vlo ? atomicAdd(w32, vlo) : 0u;
+                                const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
+                                if (up) atomicAdd(w32 + 1, up);
+                                break;
+                            }
+                            case kAccSumF64: {
+                                const double x = as_f64(v);
+                                const double old = atomicAdd((double*)p, x);
+                                double cc = 0.0;
+                                two_sum_into(old, x, &cc);
+                                if (cc != 0.0) atomicAdd((double*)(p + S), cc);
+                                break;
+                            }
+                            case kAccMin:
+                                if (v == 0x7fffffffffffffffull) break;
+                                if ((narrow >> a.arr) & 1u) atomicMin((int*)w32, (int)v);
+                                else atomicMin((long long*)p, (long long)v);
+                                break;
+                            default:
+                                if (v == 0x8000000000000000ull) break;
+                                if ((narrow >> a.arr) & 1u) atomicMax((int*)w32, (int)v);
+                                else atomicMax((long long*)p, (long long)v);
+                                break;
                         }
-                        case kAccSumF64: {
-                            const double x = as_f64(val[q]);
-                            const double old = atomicAdd((double*)p, x);
-                            double c = 0.0;
-                            two_sum_into(old, x, &c);
-                            if (c != 0.0) atomicAdd((double*)(p + S), c);
-                            break;
-                        }
-                        case kAccMin:
-                            if (val[q] == 0x7fffffffffffffffull) break;
-                            if ((narrow >> a.arr) & 1u) atomicMin((int*)w32, (int)val[q]);
-                            else atomicMin((long long*)p, (long long)val[q]);
-                            break;
-                        default:
-                            if (val[q] == 0x8000000000000000ull) break;
-                            if ((narrow >> a.arr) & 1u) atomicMax((int*)w32, (int)val[q]);
-                            else atomicMax((long long*)p, (long long)val[q]);
-                            break;
                     }
                 }
+                // the next record to the front of the queue
+#pragma unroll
+                for (int t = 0; t + 1 < kFoldRows; t++)
+#pragma unroll
+                    for (int u = 0; u < UNITS; u++) rec[t][u] = rec[t + 1][u];
             }
         }
         __syncthreads();
