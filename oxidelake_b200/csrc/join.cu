@@ -73,6 +73,37 @@ __global__ void join_pairs_kernel(const void* __restrict__ kv, const uint8_t* __
     }
 }
 
+// Dense build, step 1: rows per key offset (key - lo) of the valid keys; a
+// key seen twice raises *dup (the sorted build then runs instead).
+__global__ void join_dense_count_kernel(const void* __restrict__ kv, const uint8_t* __restrict__ kvalid, int type,
+                                        long long n, long long lo, unsigned int* __restrict__ cnt,
+                                        unsigned int* __restrict__ dup) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!valid_at(kvalid, i)) continue;
+        const unsigned long long d = (unsigned long long)(join_key_at(kv, type, i) - lo);
+        if (atomicAdd(&cnt[d], 1u) != 0u) *dup = 1u;
+    }
+}
+
+// Dense build, step 2 (every key unique): a valid row's position in key
+// order is the count of smaller keys, pos[key - lo]; it is its own run.
+__global__ void join_dense_place_kernel(const void* __restrict__ kv, const uint8_t* __restrict__ kvalid, int type,
+                                        long long n, long long lo, const unsigned long long* __restrict__ pos,
+                                        unsigned int* __restrict__ rows, long long* __restrict__ rkeys,
+                                        unsigned int* __restrict__ rstart, unsigned int* __restrict__ rcount) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!valid_at(kvalid, i)) continue;
+        const long long key = join_key_at(kv, type, i);
+        const unsigned long long p = pos[(unsigned long long)(key - lo)];
+        rows[p] = (unsigned int)i;
+        rkeys[p] = key;
+        rstart[p] = (unsigned int)p;
+        rcount[p] = 1u;
+    }
+}
+
 // Device build step 2: 1 where a run of equal keys starts.
 __global__ void join_heads_kernel(const unsigned long long* __restrict__ ukeys, long long nvalid,
                                   unsigned int* __restrict__ heads) {
@@ -289,9 +320,43 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
             t.key_lo = lo == kEmptyKey ? lo + 1 : lo;
             t.key_hi = hi;
         }
+        // Keys that fill at least a quarter of their range (and stay under
+        // 2^26 offsets): when every key is unique, counting the rows per key
+        // offset and scanning the counts places each row at its position in
+        // key order, the order the sort below gives, without the sort.
+        bool placed = false;
+        const unsigned long long dspan = (unsigned long long)hi - (unsigned long long)lo;
+        if (any && lo != kEmptyKey && dspan < (1ull << 26) && (long long)dspan < 4 * nvalid + 4096) {
+            const long long m = (long long)dspan + 1;
+            Scratch<unsigned int> cnt(s, m, true);
+            Scratch<unsigned int> dup(s, 1, true);
+            const int grid = grid_for(b, n, 256, 8);
+            note_launch(), join_dense_count_kernel<<<grid, 256, 0, s->stream>>>(key.values, key.validity, key.type, n, lo,
+                                                                               cnt.get(), dup.get());
+            OXB_CUDA(cudaGetLastError());
+            unsigned int hdup = 0;
+            OXB_CUDA(cudaMemcpyAsync(&hdup, dup.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+            OXB_CUDA(cudaStreamSynchronize(s->stream));
+            if (!hdup) {
+                Scratch<unsigned long long> pos(s, m + 1);
+                scan_u32_to_u64(s, b, cnt.get(), pos.get(), m);
+                nruns = nvalid;
+                rkeys = Scratch<long long>(s, nruns);
+                rstart = Scratch<unsigned int>(s, nruns);
+                rcount = Scratch<unsigned int>(s, nruns);
+                t.nrows = nvalid;
+                out->rows_mem = dev_alloc(s, (size_t)(nvalid + 1) * 4, false);
+                t.rows = (unsigned int*)out->rows_mem->ptr;
+                note_launch(), join_dense_place_kernel<<<grid, 256, 0, s->stream>>>(
+                    key.values, key.validity, key.type, n, lo, pos.get(), t.rows, rkeys.get(), rstart.get(),
+                    rcount.get());
+                OXB_CUDA(cudaGetLastError());
+                placed = true;
+            }
+        }
         Scratch<unsigned long long> ukeys;
         Scratch<unsigned int> srows;
-        if (any) {
+        if (any && !placed) {
             unsigned long long span = (unsigned long long)hi - (unsigned long long)lo;
             unsigned long long null_key = span + 1;  // wraps to 0 only for the full i64 range
             int bits = 64;
@@ -307,10 +372,12 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
             OXB_CUDA(cudaGetLastError());
             radix_sort_pairs(s, b, ukeys.get(), srows.get(), n, bits);
         }
-        t.nrows = nvalid;
-        out->rows_mem = dev_alloc(s, (size_t)(nvalid + 1) * 4, false);
-        t.rows = (unsigned int*)out->rows_mem->ptr;
-        if (nvalid > 0) {
+        if (!placed) {
+            t.nrows = nvalid;
+            out->rows_mem = dev_alloc(s, (size_t)(nvalid + 1) * 4, false);
+            t.rows = (unsigned int*)out->rows_mem->ptr;
+        }
+        if (nvalid > 0 && !placed) {
             OXB_CUDA(cudaMemcpyAsync(t.rows, srows.get(), nvalid * 4, cudaMemcpyDeviceToDevice, s->stream));
             Scratch<unsigned int> heads(s, nvalid);
             Scratch<unsigned long long> run_of(s, nvalid + 1);

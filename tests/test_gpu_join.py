@@ -137,3 +137,33 @@ def test_one_key_everywhere(backend, stream):
     got = backend.download(stream, backend.hash_join(stream, ldev, rdev, table, m, 65_536, 65_536))
     want = oracle.hash_join_gather(probe, build, otable, om, 65_536, 65_536)
     assert_batches_equal(got, want)
+
+
+@pytest.mark.parametrize("key_type", [pa.int64(), pa.int32()])
+@pytest.mark.parametrize("dup", [False, True], ids=["unique", "one-repeat"])
+def test_dense_keys_placed_without_sort(backend, stream, key_type, dup):
+    """Build keys that fill their range: unique ones are placed by key offset
+    (no sort), a single repeated key sends the build back to the sort; both
+    give the oracle's table, matches and gathered rows."""
+    rng = np.random.default_rng(11 + dup)
+    nb, npr = 200_000, 600_000
+    bk = (rng.permutation(nb) - 70_000).astype(key_type.to_pandas_dtype())
+    if dup:
+        bk[5] = bk[123_456]
+    pk = rng.integers(-80_000, 140_000, npr).astype(key_type.to_pandas_dtype())
+    build = pa.RecordBatch.from_arrays(
+        [pa.array(bk, key_type, mask=rng.random(nb) < 0.03), pa.array(np.arange(nb, dtype=np.int64))], names=["bk", "bv"]
+    )
+    probe = pa.RecordBatch.from_arrays(
+        [pa.array(pk, key_type, mask=rng.random(npr) < 0.03), pa.array(np.arange(npr, dtype=np.int64))], names=["pk", "pid"]
+    )
+    otable = oracle.JoinTable(build, 0)
+    om = oracle.JoinMatches(probe, 0, otable)
+    ldev, rdev = backend.upload(stream, probe), backend.upload(stream, build)
+    table = backend.prepare_join_build(stream, rdev, 0)
+    assert table.distinct_keys() == otable.distinct_keys()
+    m = backend.probe_join(stream, ldev, 0, table)
+    assert len(m) == len(om)
+    got = backend.download(stream, backend.hash_join(stream, ldev, rdev, table, m, 0, len(m), [1, 3, 0, 2]))
+    want = oracle.hash_join_gather(probe, build, otable, om, 0, len(om), [1, 3, 0, 2])
+    assert_batches_equal(got, want)
