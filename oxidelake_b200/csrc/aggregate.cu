@@ -3285,14 +3285,26 @@ oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan
     Scratch<unsigned long long> skeys(s, G + 1);
     Scratch<unsigned int> sslots(s, G + 1);
     unsigned long long lo = G > 0 ? h.lo : 0;
+    const unsigned long long* okeys = skeys.get();  // the groups in key order
+    const unsigned int* oslots = sslots.get();
+    Scratch<unsigned long long> ukeys;
+    Scratch<unsigned int> uslots;
     if (G > 0) {
         note_launch(), agg_compact_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(P, flags.get(), pos.get(), lo,
                                                                                         skeys.get(), sslots.get());
         OXB_CUDA(cudaGetLastError());
         unsigned long long span = h.hi - h.lo;
-        int bits = 0;
-        while (bits < 64 && (span >> bits) != 0) bits++;
-        radix_sort_pairs(s, b, skeys.get(), sslots.get(), G, bits);
+        // Group keys are distinct: a narrow span is ordered in one launch.
+        ukeys = Scratch<unsigned long long>(s, G + 1);
+        uslots = Scratch<unsigned int>(s, G + 1);
+        if (order_distinct_small(s, skeys.get(), sslots.get(), G, span, ukeys.get(), uslots.get())) {
+            okeys = ukeys.get();
+            oslots = uslots.get();
+        } else {
+            int bits = 0;
+            while (bits < 64 && (span >> bits) != 0) bits++;
+            radix_sort_pairs(s, b, skeys.get(), sslots.get(), G, bits);
+        }
     }
 
     auto out = std::make_unique<oxb_batch>();
@@ -3322,8 +3334,8 @@ oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan
         O.cols[j] = OutCol{out->cols.back().values, (unsigned int*)out->cols.back().validity};
     }
     if (rows > 0) {
-        note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, skeys.get(), sslots.get(),
-                                                                                        lo, G, rows);
+        note_launch(), agg_emit_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(P, O, okeys, oslots, lo, G,
+                                                                                        rows);
         OXB_CUDA(cudaGetLastError());
         OXB_CUDA(cudaStreamSynchronize(s->stream));
     }

@@ -223,6 +223,12 @@ void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsign
 // Stable LSD radix sort of (key, value) pairs on bits [0, bits) of the key.
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
                       unsigned int* values, long long n, int bits);
+// Orders n distinct keys below `span_limit` (span_limit <= 32768) and their
+// values by key in one launch (a presence bitmap and its ranks in shared
+// memory), into keys_out / values_out.  False, with nothing launched, when
+// the keys' span is too wide for it.
+bool order_distinct_small(const StreamRef& s, const unsigned long long* keys, const unsigned int* values, long long n,
+                          unsigned long long span, unsigned long long* keys_out, unsigned int* values_out);
 
 // Minimum and maximum valid int key (as int64) of a column; false when none.
 bool key_range(const StreamRef& s, const Backend& b, const Column& key, long long n,

@@ -56,6 +56,35 @@ __global__ void scan_reduce_kernel(const unsigned int* __restrict__ counts, long
     if (threadIdx.x == 0) partials[blockIdx.x] = total;
 }
 
+// A short scan (up to kSmallScan counts) in one launch: one block walks the
+// counts a chunk at a time, carrying the running total, and stores it at [n].
+constexpr long long kSmallScan = 16 * kScanChunk;
+__global__ void scan_small_kernel(const unsigned int* __restrict__ counts, long long n,
+                                  unsigned long long* __restrict__ offsets) {
+    __shared__ unsigned long long warp_sums[32];
+    unsigned long long carry = 0;
+    for (long long base = 0; base < n; base += kScanChunk) {
+        unsigned int c[kScanItems];
+        unsigned long long s = 0;
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            const long long idx = base + (long long)threadIdx.x * kScanItems + i;
+            c[i] = idx < n ? counts[idx] : 0u;
+            s += c[i];
+        }
+        unsigned long long total;
+        unsigned long long run = carry + block_exclusive_scan(s, warp_sums, &total);
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            const long long idx = base + (long long)threadIdx.x * kScanItems + i;
+            if (idx < n) offsets[idx] = run;
+            run += c[i];
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) offsets[n] = carry;
+}
+
 // One block scans `m` partials in place (exclusive) and stores the total at [m].
 __global__ void scan_partials_kernel(unsigned long long* __restrict__ p, long long m) {
     __shared__ unsigned long long warp_sums[32];
@@ -214,6 +243,11 @@ void scan_u32_to_u64(const StreamRef& s, const Backend& b, const unsigned int* c
         OXB_CUDA(cudaMemsetAsync(offsets, 0, sizeof(unsigned long long), s->stream));
         return;
     }
+    if (n <= kSmallScan) {
+        note_launch(), scan_small_kernel<<<1, kScanThreads, 0, s->stream>>>(counts, n, offsets);
+        OXB_CUDA(cudaGetLastError());
+        return;
+    }
     long long blocks = (n + kScanChunk - 1) / kScanChunk;
     Scratch<unsigned long long> partials(s, blocks + 1);
     note_launch(), scan_reduce_kernel<<<(unsigned)blocks, kScanThreads, 0, s->stream>>>(counts, n, partials.get());
@@ -236,6 +270,49 @@ void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsign
     note_launch(), scan_partials_kernel<<<1, 1024, 0, s->stream>>>(partials, blocks);
     note_launch(), scan_apply_kernel<<<(unsigned)blocks, kScanThreads, 0, s->stream>>>(counts, n, partials, offsets);
     OXB_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+constexpr int kOrderWords = 1024;  // presence bits for keys below 32768
+
+__global__ void __launch_bounds__(1024) order_distinct_small_kernel(const unsigned long long* __restrict__ keys,
+                                                                    const unsigned int* __restrict__ values, long long n,
+                                                                    unsigned long long* __restrict__ keys_out,
+                                                                    unsigned int* __restrict__ values_out) {
+    __shared__ unsigned bits[kOrderWords];
+    __shared__ unsigned long long before[kOrderWords];
+    __shared__ unsigned long long warp_sums[32];
+    for (int w = threadIdx.x; w < kOrderWords; w += blockDim.x) bits[w] = 0;
+    __syncthreads();
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned d = (unsigned)keys[i];
+        atomicOr(&bits[d >> 5], 1u << (d & 31));
+    }
+    __syncthreads();
+    // one word a thread (blockDim.x == kOrderWords): keys present in earlier words
+    unsigned long long total;
+    before[threadIdx.x] = block_exclusive_scan((unsigned long long)__popc(bits[threadIdx.x]), warp_sums, &total);
+    __syncthreads();
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned d = (unsigned)keys[i];
+        const unsigned long long p = before[d >> 5] + __popc(bits[d >> 5] & ((1u << (d & 31)) - 1u));
+        keys_out[p] = d;
+        values_out[p] = values[i];
+    }
+}
+
+}  // namespace
+
+bool order_distinct_small(const StreamRef& s, const unsigned long long* keys, const unsigned int* values, long long n,
+                          unsigned long long span, unsigned long long* keys_out, unsigned int* values_out) {
+    if (span >= 32ull * kOrderWords) return false;
+    if (n > 0) {
+        note_launch(), order_distinct_small_kernel<<<1, kOrderWords, 0, s->stream>>>(keys, values, n, keys_out,
+                                                                                     values_out);
+        OXB_CUDA(cudaGetLastError());
+    }
+    return true;
 }
 
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
