@@ -2682,6 +2682,21 @@ __device__ __forceinline__ int batch_of_tile(const BatchCols* batches, int nb, l
     return lo;
 }
 
+// The same search over a shared copy of the first 2048 batches' first tiles
+// (`cached` of them): a tile whose batch is past them searches HBM.
+constexpr int kTileCache = 2048;
+__device__ __forceinline__ int batch_of_tile_cached(const long long* ptile0, int cached, const BatchCols* batches,
+                                                    int nb, long long t) {
+    if (cached < nb && batches[cached].ptile0 <= t) return cached + batch_of_tile(batches + cached, nb - cached, t);
+    int lo = 0, hi = cached - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ptile0[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ bool keep_row(const DevPredicate& pred, const BatchCols& B, long long r) {
     for (int l = 0; l < pred.nleaves; l++) {
         const DevLeaf& lf = pred.leaves[l];
@@ -2695,7 +2710,9 @@ __device__ __forceinline__ bool keep_row(const DevPredicate& pred, const BatchCo
 }
 
 // Rows r0 + j * T (j < R, below `end`) that pass the WHERE and have a
-// valid key, with their keys: every leaf's loads issued before any test.
+// valid key, with their keys.  The keys are loaded with the first leaf's
+// values, before any test: one memory round trip instead of two, for
+// 8 bytes more a row that the WHERE drops.
 template <int R, int T = kThreads>
 __device__ __forceinline__ unsigned kept_keys(const DevPredicate& pred, const BatchCols& B, int key_type, long long r0,
                                               long long end, long long* key, unsigned* nullkey) {
@@ -2703,6 +2720,17 @@ __device__ __forceinline__ unsigned kept_keys(const DevPredicate& pred, const Ba
 #pragma unroll
     for (int j = 0; j < R; j++)
         if (r0 + (long long)j * T < end) live |= 1u << j;
+    unsigned kvalid = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const long long r = r0 + (long long)j * T;
+        key[j] = 0;
+        if (!((live >> j) & 1u)) continue;
+        if (valid_at(B.key_valid, r)) {
+            kvalid |= 1u << j;
+            key[j] = load_int(B.key, key_type, r);
+        }
+    }
     unsigned keep = live;
     for (int l = 0; l < pred.nleaves; l++) {
         const DevLeaf& lf = pred.leaves[l];
@@ -2724,19 +2752,10 @@ __device__ __forceinline__ unsigned kept_keys(const DevPredicate& pred, const Ba
         for (int j = 0; j < R; j++)
             if (((keep >> j) & 1u) && !cmp_holds(lf.op, a[j], lf.lit)) keep &= ~(1u << j);
     }
-    unsigned nk = 0;
+    unsigned nk = keep & ~kvalid;
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        const long long r = r0 + (long long)j * T;
-        key[j] = 0;
-        if (!((keep >> j) & 1u)) continue;
-        if (!valid_at(B.key_valid, r)) {
-            nk |= 1u << j;
-            continue;
-        }
-        key[j] = load_int(B.key, key_type, r);
-        if (key[j] == kEmptyKey) nk |= 1u << j;
-    }
+    for (int j = 0; j < R; j++)
+        if (((keep & kvalid) >> j) & 1u && key[j] == kEmptyKey) nk |= 1u << j;
     *nullkey = nk;  // kept rows whose key is NULL or INT64_MIN
     return keep & ~nk;
 }
@@ -2759,8 +2778,13 @@ __global__ void __launch_bounds__(kScanThreads) part_scan_kernel(const __grid_co
     for (int i = threadIdx.x; i < kHllRegs + kFine; i += blockDim.x) scan_smem[i] = 0;
     __syncthreads();
     unsigned n = 0;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const BatchCols& B = batches[batch_of_tile(batches, nb, t)];
+    // A contiguous range of tiles a CTA, stepping from batch to batch (no
+    // search per tile).
+    const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int bi = t0 < t1 ? batch_of_tile(batches, nb, t0) : 0;
+    for (long long t = t0; t < t1; t++) {
+        while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
+        const BatchCols& B = batches[bi];
         const long long base = (t - B.ptile0) * kPartTile;
         const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
         for (long long r0 = base + threadIdx.x; r0 < end; r0 += (long long)kScanThreads * 4) {
@@ -2825,14 +2849,17 @@ __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_cons
     __shared__ unsigned int hist[kMaxF1];
     __shared__ unsigned long long base1[kMaxF1];
     __shared__ long long s_tile;
+    __shared__ long long s_ptile0[kTileCache];
     const int f1 = pp.nparts >> pp.f2_bits;
+    const int cached = nb < kTileCache ? nb : kTileCache;
+    for (int i = threadIdx.x; i < cached; i += blockDim.x) s_ptile0[i] = batches[i].ptile0;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
         __syncthreads();
         const long long t = s_tile;
         if (t >= ntiles) break;
-        const BatchCols& B = batches[batch_of_tile(batches, nb, t)];
+        const BatchCols& B = batches[batch_of_tile_cached(s_ptile0, cached, batches, nb, t)];
         const long long tbase = (t - B.ptile0) * kPartTile;
         const long long tend = tbase + kPartTile < B.n ? tbase + kPartTile : B.n;
         for (long long sub = tbase; sub < tend; sub += kSplitTile) {

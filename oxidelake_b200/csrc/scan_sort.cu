@@ -58,7 +58,7 @@ __global__ void scan_reduce_kernel(const unsigned int* __restrict__ counts, long
 
 // A short scan (up to kSmallScan counts) in one launch: one block walks the
 // counts a chunk at a time, carrying the running total, and stores it at [n].
-constexpr long long kSmallScan = 16 * kScanChunk;
+constexpr long long kSmallScan = 2 * kScanChunk;
 __global__ void scan_small_kernel(const unsigned int* __restrict__ counts, long long n,
                                   unsigned long long* __restrict__ offsets) {
     __shared__ unsigned long long warp_sums[32];
