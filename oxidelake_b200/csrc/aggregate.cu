@@ -2510,7 +2510,7 @@ bool plan_stream(const AggProgram& P, const DevPredicate& pred, const void* key_
 // GpuAggregateExec folds every RecordBatch of a partition into one result
 // (compute/src/exec/aggregate.rs:35-321); the reference runs one device
 // aggregate per batch and merges on the host.  Here every batch's columns
-// are described once in HBM and a persistent kernel takes 1024-row tiles of
+// are described once in HBM and a persistent kernel takes 4096-row tiles of
 // all batches from one work queue (uneven batch sizes cost nothing extra),
 // folding into one HBM table sized from a HyperLogLog count of the keys.
 
@@ -2526,7 +2526,7 @@ struct BatchCols {
     const uint8_t* lvalid[kMaxLeaves];
 };
 
-constexpr int kBatchTile = 1024;
+constexpr int kBatchTile = 4096;
 
 template <int MAXACC>
 __global__ void __launch_bounds__(kThreads) agg_batches_kernel(const __grid_constant__ AggProgram P,
@@ -2536,14 +2536,22 @@ __global__ void __launch_bounds__(kThreads) agg_batches_kernel(const __grid_cons
                                                                unsigned long long* __restrict__ queue) {
     __shared__ long long s_tile;
     __shared__ int s_b;
+    // The first tiles of the first kTile0Cache batches, searched in shared
+    // memory (the descriptors are large: a search in HBM costs a round trip
+    // a step); a tile of a later batch searches HBM.
+    constexpr int kTile0Cache = 2048;
+    __shared__ long long s_tile0[kTile0Cache];
+    const int cached = nb < kTile0Cache ? nb : kTile0Cache;
+    for (int i = threadIdx.x; i < cached; i += blockDim.x) s_tile0[i] = batches[i].tile0;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const long long t = (long long)atomicAdd(queue, 1ull);
-            int lo = 0, hi = nb - 1;  // the last batch whose first tile is <= t
+            const bool far = cached < nb && batches[cached].tile0 <= t;
+            int lo = far ? cached : 0, hi = far ? nb - 1 : cached - 1;  // the last batch whose first tile is <= t
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (batches[mid].tile0 <= t) lo = mid;
+                if ((far ? batches[mid].tile0 : s_tile0[mid]) <= t) lo = mid;
                 else hi = mid - 1;
             }
             s_tile = t;
