@@ -3329,10 +3329,11 @@ oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan
                                                                                         skeys.get(), sslots.get());
         OXB_CUDA(cudaGetLastError());
         unsigned long long span = h.hi - h.lo;
-        // Group keys are distinct: a narrow span is ordered in one launch.
+        // Group keys are distinct: a narrow or well-filled span is ordered
+        // by rank, without a sort.
         ukeys = Scratch<unsigned long long>(s, G + 1);
         uslots = Scratch<unsigned int>(s, G + 1);
-        if (order_distinct_small(s, skeys.get(), sslots.get(), G, span, ukeys.get(), uslots.get())) {
+        if (order_distinct_keys(s, b, skeys.get(), sslots.get(), G, span, ukeys.get(), uslots.get())) {
             okeys = ukeys.get();
             oslots = uslots.get();
         } else {

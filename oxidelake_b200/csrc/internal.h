@@ -223,12 +223,14 @@ void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsign
 // Stable LSD radix sort of (key, value) pairs on bits [0, bits) of the key.
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,
                       unsigned int* values, long long n, int bits);
-// Orders n distinct keys below `span_limit` (span_limit <= 32768) and their
-// values by key in one launch (a presence bitmap and its ranks in shared
-// memory), into keys_out / values_out.  False, with nothing launched, when
-// the keys' span is too wide for it.
-bool order_distinct_small(const StreamRef& s, const unsigned long long* keys, const unsigned int* values, long long n,
-                          unsigned long long span, unsigned long long* keys_out, unsigned int* values_out);
+// Orders n distinct keys in [0, span] and their values by key, into
+// keys_out / values_out, without a sort: a span under 32768 in one launch (a
+// presence bitmap and its ranks in shared memory), a span the keys fill to
+// at least a quarter by presence flags in HBM and their scan.  False, with
+// nothing launched, for a wider span.
+bool order_distinct_keys(const StreamRef& s, const Backend& b, const unsigned long long* keys,
+                          const unsigned int* values, long long n, unsigned long long span,
+                          unsigned long long* keys_out, unsigned int* values_out);
 
 // Minimum and maximum valid int key (as int64) of a column; false when none.
 bool key_range(const StreamRef& s, const Backend& b, const Column& key, long long n,

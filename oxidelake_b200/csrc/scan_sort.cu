@@ -302,16 +302,49 @@ __global__ void __launch_bounds__(1024) order_distinct_small_kernel(const unsign
     }
 }
 
+__global__ void order_dense_flags_kernel(const unsigned long long* __restrict__ keys, long long n,
+                                         unsigned int* __restrict__ present) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        present[keys[i]] = 1u;
+}
+
+__global__ void order_dense_place_kernel(const unsigned long long* __restrict__ keys,
+                                         const unsigned int* __restrict__ values, long long n,
+                                         const unsigned long long* __restrict__ pos,
+                                         unsigned long long* __restrict__ keys_out, unsigned int* __restrict__ values_out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long d = keys[i];
+        const unsigned long long p = pos[d];
+        keys_out[p] = d;
+        values_out[p] = values[i];
+    }
+}
+
 }  // namespace
 
-bool order_distinct_small(const StreamRef& s, const unsigned long long* keys, const unsigned int* values, long long n,
-                          unsigned long long span, unsigned long long* keys_out, unsigned int* values_out) {
-    if (span >= 32ull * kOrderWords) return false;
-    if (n > 0) {
-        note_launch(), order_distinct_small_kernel<<<1, kOrderWords, 0, s->stream>>>(keys, values, n, keys_out,
-                                                                                     values_out);
-        OXB_CUDA(cudaGetLastError());
+bool order_distinct_keys(const StreamRef& s, const Backend& b, const unsigned long long* keys,
+                          const unsigned int* values, long long n, unsigned long long span,
+                          unsigned long long* keys_out, unsigned int* values_out) {
+    if (span < 32ull * kOrderWords) {
+        if (n > 0) {
+            note_launch(), order_distinct_small_kernel<<<1, kOrderWords, 0, s->stream>>>(keys, values, n, keys_out,
+                                                                                         values_out);
+            OXB_CUDA(cudaGetLastError());
+        }
+        return true;
     }
+    // Keys that fill at least a quarter of their span (under 2^28): a key's
+    // rank is the count of present offsets below it.
+    if (span >= (1ull << 28) || (long long)span >= 4 * n + 4096) return false;
+    const long long m = (long long)span + 1;
+    Scratch<unsigned int> present(s, m, true);
+    Scratch<unsigned long long> pos(s, m + 1);
+    const int grid = grid_for(b, n, 256, 8);
+    note_launch(), order_dense_flags_kernel<<<grid, 256, 0, s->stream>>>(keys, n, present.get());
+    scan_u32_to_u64(s, b, present.get(), pos.get(), m);
+    note_launch(), order_dense_place_kernel<<<grid, 256, 0, s->stream>>>(keys, values, n, pos.get(), keys_out,
+                                                                        values_out);
+    OXB_CUDA(cudaGetLastError());
     return true;
 }
 
