@@ -2876,6 +2876,21 @@ __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_cons
             long long key[kSplitRows];
             unsigned nk;
             const unsigned m = kept_keys<kSplitRows>(pred, B, key_type, sub + threadIdx.x, tend, key, &nk);
+            // One Int32 column (16-byte records): its values and validity
+            // are loaded now, while the partition cursors are reserved.
+            int xv[kSplitRows];
+            unsigned xvalid = 0;
+            if (pp.compact) {
+                const int q = pp.src_of_col[0];
+#pragma unroll
+                for (int j = 0; j < kSplitRows; j++) {
+                    const long long r = sub + threadIdx.x + (long long)j * kThreads;
+                    xv[j] = 0;
+                    if (!((m >> j) & 1u) || !valid_at(B.valid[q], r)) continue;
+                    xvalid |= 1u << j;
+                    xv[j] = __ldg((const int*)B.vals[q] + r);
+                }
+            }
             unsigned rank[kSplitRows];
 #pragma unroll
             for (int j = 0; j < kSplitRows; j++) {
@@ -2897,6 +2912,10 @@ __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_cons
                 const long long r = sub + threadIdx.x + (long long)j * kThreads;
                 if (nn & 1u) {
                     part_null_row_to_hbm<MAXACC>(P, B, r);
+                } else if ((mm & 1u) && pp.compact) {
+                    const unsigned long long pos = base1[rank[0] >> 24] + (rank[0] & 0xFFFFFFu);
+                    pp.recs[pos] = make_uint4((unsigned)key[0], (unsigned)((unsigned long long)key[0] >> 32),
+                                              (unsigned)xv[0], xvalid & 1u);
                 } else if (mm & 1u) {
                     const unsigned long long pos = base1[rank[0] >> 24] + (rank[0] & 0xFFFFFFu);
                     unsigned long long w[MAXACC + 2];  // key, columns, validity
@@ -2914,27 +2933,25 @@ __global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_cons
                             w[1 + c] = pp.width[c] == 4 ? (unsigned long long)(long long)__ldg((const int*)B.vals[q] + r)
                                                         : (unsigned long long)__ldg((const long long*)B.vals[q] + r);
                     }
-                    if (pp.compact) {
-                        pp.recs[pos] = make_uint4((unsigned)w[0], (unsigned)(w[0] >> 32), (unsigned)w[1], (unsigned)flags);
-                    } else {
 #pragma unroll
-                        for (int i = 1; i < MAXACC + 2; i++)
-                            if (i == 1 + pp.ncols) w[i] = flags;
-                        const int units = (pp.ncols + 3) >> 1;
-                        uint4* o = pp.recs + pos * units;
+                    for (int i = 1; i < MAXACC + 2; i++)
+                        if (i == 1 + pp.ncols) w[i] = flags;
+                    const int units = (pp.ncols + 3) >> 1;
+                    uint4* o = pp.recs + pos * units;
 #pragma unroll
-                        for (int u = 0; u < (MAXACC + 2) / 2; u++)
-                            if (u < units)
-                                o[u] = make_uint4((unsigned)w[2 * u], (unsigned)(w[2 * u] >> 32), (unsigned)w[2 * u + 1],
-                                                  (unsigned)(w[2 * u + 1] >> 32));
-                    }
+                    for (int u = 0; u < (MAXACC + 2) / 2; u++)
+                        if (u < units)
+                            o[u] = make_uint4((unsigned)w[2 * u], (unsigned)(w[2 * u] >> 32), (unsigned)w[2 * u + 1],
+                                              (unsigned)(w[2 * u + 1] >> 32));
                 }
                 mm >>= 1;
                 nn >>= 1;
+                xvalid >>= 1;
 #pragma unroll
                 for (int t = 0; t + 1 < kSplitRows; t++) {
                     key[t] = key[t + 1];
                     rank[t] = rank[t + 1];
+                    xv[t] = xv[t + 1];
                 }
             }
         }
