@@ -1,10 +1,13 @@
 """Vector top-k at the configured shape: N rows x 768 FP32 (L2-normalised,
 seeded on the device), an int64 filter column uniform in [0, 100), 256 queries
 from the same distribution, top-10 under WHERE f < 30, l2 and cosine.
-Prints one JSON line per metric: the scan's CUDA-event time and TFLOP/s
-(2 x queries x rows x dim over all rows: the filter is applied in the
-scan's epilogue), the whole call's time, how many queries took the exact
-path, and the BF16 score error against FP64 over the re-ranked candidates.
+Prints one JSON line per metric:
+- the scan's CUDA-event time: the copy of the kept rows to a compacted table
+  (a WHERE that keeps at most half the rows) plus the tcgen05 scan;
+- TFLOP/s: 2 x queries x kept rows x dim, the algorithmic flops (the rows
+  the WHERE drops need no distance);
+- the whole call's time, how many queries took the exact path, and the BF16
+  score error against FP64 over the re-ranked candidates.
 
     python -m oxidelake_b200.bench_topk [--rows N] [--repeats R]
 """
@@ -46,6 +49,7 @@ def main() -> int:
     x = torch.randn(n, d, device="cuda", generator=g)
     x /= x.norm(dim=1, keepdim=True)
     f = torch.randint(0, 100, (n,), device="cuda", generator=g, dtype=torch.int64)
+    kept = int((f < 30).sum().item())
     torch.cuda.synchronize()
     schema = pa.schema([pa.field("f", pa.int64()), pa.field("emb", pa.list_(pa.float32(), d))])
     batch = b.batch_from_device(
@@ -67,10 +71,11 @@ def main() -> int:
             call.append((time.perf_counter() - t0) * 1e3)
             scan.append(b.last_kernel_time()[1])
         ms = min(scan)
-        flops = 2.0 * args.queries * n * d
+        flops = 2.0 * args.queries * kept * d
         print(json.dumps({
-            "workload": "vector top-k", "metric": metric.name.lower(), "rows": n, "dim": d, "queries": args.queries,
-            "k": args.k, "filter": "f < 30 (30%)", "scan_ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 1),
+            "workload": "vector top-k", "metric": metric.name.lower(), "rows": n, "kept_rows": kept, "dim": d,
+            "queries": args.queries, "k": args.k, "filter": "f < 30 (30%)", "scan_ms": round(ms, 3),
+            "tflops": round(flops / ms / 1e9, 1),
             "call_ms": round(min(call), 3), "index_build_s": round(build_s, 3), "exact_queries": st["exact_queries"],
             "reranked": st["reranked"], "bf16_score_error_max": st["max_score_error"],
             "bf16_score_error_mean": st["mean_score_error"], "data": "synthetic",

@@ -513,6 +513,7 @@ struct FinalParams {
     const unsigned* counts;
     const unsigned long long* bounds;
     const float* table;   // FP32 vectors, row-major
+    const unsigned* rowmap;  // candidate index -> row (a compacted scan), or null
     const float* queries; // FP32, nq x dim
     const float* qnorm;   // per query ||q|| (FP32, folded in order)
     float xmax;
@@ -587,7 +588,9 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
     unsigned long long ecount = 0;
     for (int iter = 0; iter < 32; iter++) {
         for (int i = done + threadIdx.x; i < R; i += blockDim.x) {
-            const unsigned row = (unsigned)(pool[i] & 0xFFFFFFFFu);
+            const unsigned idx = (unsigned)(pool[i] & 0xFFFFFFFFu);
+            // compacted indices keep row order, so (score, index) sorts as (score, row)
+            const unsigned row = p.rowmap ? __ldg(p.rowmap + idx) : idx;
             const float* x = p.table + (size_t)row * p.dim;
             const unsigned d = exact_distance_bits(x, qv, p.dim, p.metric, qn);
             ex[i] = ((unsigned long long)f32_order(d) << 32) | row;
@@ -746,6 +749,65 @@ EncodeTiled encode_tiled() {
     return fn;
 }
 
+// Compaction of the rows a query batch can return (a WHERE that keeps few
+// rows): per 32-row word, the rows the shared WHERE keeps with a valid
+// vector and, when there is a per-query leaf, a valid leaf operand (a NULL
+// operand fails every query); and its count.
+__global__ void topk_compact_words_kernel(const unsigned* __restrict__ sel, const uint8_t* __restrict__ valid,
+                                          const uint8_t* __restrict__ qvalid, long long n, unsigned* __restrict__ words,
+                                          unsigned* __restrict__ counts) {
+    const long long nwords = (n + 31) >> 5, nbytes = (n + 7) >> 3;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nwords;
+         w += (long long)gridDim.x * blockDim.x) {
+        const long long row0 = w << 5, b0 = row0 >> 3;
+        unsigned m = sel ? __ldg(sel + w) : ~0u;
+        for (int bm = 0; bm < 2; bm++) {
+            const uint8_t* vb = bm == 0 ? valid : qvalid;
+            if (!vb) continue;
+            unsigned v = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (b0 + i < nbytes) v |= (unsigned)__ldg(vb + b0 + i) << (8 * i);
+            m &= v;
+        }
+        if (row0 + 32 > n) m &= (1u << (n - row0)) - 1u;
+        words[w] = m;
+        counts[w] = (unsigned)__popc(m);
+    }
+}
+
+// Copies the kept rows, in row order, to the compacted table: BF16 row,
+// norms, row id and (with a per-query leaf) the operand's order key.  One
+// warp per 32-row word.
+__global__ void topk_compact_gather_kernel(const unsigned* __restrict__ words, const unsigned long long* __restrict__ offs,
+                                           long long nwords, const uint4* __restrict__ bf16, int row_u4,
+                                           const float* __restrict__ norm2, const float* __restrict__ inv,
+                                           const void* __restrict__ qcol, int qtype, uint4* __restrict__ cb,
+                                           float* __restrict__ cn2, float* __restrict__ cinv,
+                                           unsigned* __restrict__ rowmap, long long* __restrict__ cqkey) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); w < nwords; w += warps) {
+        unsigned m = words[w];
+        unsigned long long pos = offs[w];
+        while (m) {
+            const unsigned r = (unsigned)(w << 5) + (unsigned)(__ffs(m) - 1);
+            m &= m - 1u;
+            for (int i = lane; i < row_u4; i += 32) cb[pos * row_u4 + i] = __ldg(bf16 + (size_t)r * row_u4 + i);
+            if (lane == 0) {
+                cn2[pos] = __ldg(norm2 + r);
+                cinv[pos] = __ldg(inv + r);
+                rowmap[pos] = r;
+                if (cqkey)
+                    cqkey[pos] = qtype == kFloat64 ? filter_order_key(__ldg((const double*)qcol + r))
+                                 : qtype == kInt64 ? __ldg((const long long*)qcol + r)
+                                                   : (long long)__ldg((const int*)qcol + r);
+            }
+            pos++;
+        }
+    }
+}
+
 void encode_bf16_map(CUtensorMap* map, const void* base, long long rows, int dp, int box_rows) {
     cuuint64_t dims[2] = {(cuuint64_t)dp, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)dp * 2};
@@ -877,6 +939,54 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     }
     const bool fast = !a.exact && n > 0 && C > 0;
     std::vector<int> host_fb(nq, 1);
+    // A WHERE (or NULL vectors) that keeps at most half the rows: the kept
+    // rows are copied, in row order, to a compacted BF16 table and only those
+    // are scanned; the re-rank maps each candidate back to its row.
+    bool compact = false;
+    long long nsel = n;
+    AllocRef cb_mem, cn2_mem, cinv_mem, rowmap_mem, cq_mem;
+    CUtensorMap cmap;
+    // Timed: the compaction and the scan (the host's read of the kept count
+    // between them is not).
+    KernelTimer timer(b, s, "topk_scan_kernel");
+    Scratch<unsigned> words, wcounts;
+    Scratch<unsigned long long> woffs;
+    if (fast && (selp || ix.vec.validity || qleaf.validity)) {
+        const long long nwords = (n + 31) / 32;
+        words = Scratch<unsigned>(s, nwords);
+        wcounts = Scratch<unsigned>(s, nwords);
+        woffs = Scratch<unsigned long long>(s, nwords + 1);
+        timer.begin();
+        note_launch(), topk_compact_words_kernel<<<grid_for(b, nwords, 256, 8), 256, 0, s->stream>>>(
+            selp, ix.vec.validity, qleaf.validity, n, words.get(), wcounts.get());
+        OXB_CUDA(cudaGetLastError());
+        scan_u32_to_u64(s, b, wcounts.get(), woffs.get(), nwords);
+        timer.end();
+        unsigned long long hn = 0;
+        OXB_CUDA(cudaMemcpyAsync(&hn, woffs.get() + nwords, 8, cudaMemcpyDeviceToHost, s->stream));
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+        if ((long long)hn * 2 <= n) {
+            compact = true;
+            nsel = (long long)hn;
+            const long long crows = nsel > kRTile ? nsel : kRTile;  // the tensor map's box fits
+            const long long m1 = nsel > 0 ? nsel : 1;
+            cb_mem = dev_alloc(s, (size_t)crows * dp * 2, nsel < kRTile);
+            cn2_mem = dev_alloc(s, (size_t)m1 * 4, false);
+            cinv_mem = dev_alloc(s, (size_t)m1 * 4, false);
+            rowmap_mem = dev_alloc(s, (size_t)m1 * 4, false);
+            if (qleaf.values) cq_mem = dev_alloc(s, (size_t)m1 * 8, false);
+            timer.begin();
+            if (nsel > 0) {
+                note_launch(), topk_compact_gather_kernel<<<grid_for(b, nwords * 32, 256, 8), 256, 0, s->stream>>>(
+                    words.get(), woffs.get(), nwords, (const uint4*)ix.bf16->ptr, dp * 2 / 16,
+                    (const float*)ix.norm2->ptr, (const float*)ix.inv->ptr, qleaf.values, qleaf.type,
+                    (uint4*)cb_mem->ptr, (float*)cn2_mem->ptr, (float*)cinv_mem->ptr, (unsigned*)rowmap_mem->ptr,
+                    qleaf.values ? (long long*)cq_mem->ptr : nullptr);
+                OXB_CUDA(cudaGetLastError());
+            }
+            encode_bf16_map(&cmap, cb_mem->ptr, crows, dp, kRTile);
+        }
+    }
     if (fast) {
         const int cap = L;
         Scratch<unsigned long long> lists(s, (size_t)grid * kQTile * cap);
@@ -886,7 +996,7 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         CUtensorMap qmap;
         encode_bf16_map(&qmap, qb.get(), qp, dp, kQTile);
         ScanParams sp{};
-        sp.n = n;
+        sp.n = nsel;
         sp.kblocks = dp / kKBlock;
         sp.groups = groups;
         sp.nq = nq;
@@ -894,13 +1004,13 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.L = L;
         sp.C = C;
         sp.stages = stages;
-        sp.sel = selp;
-        sp.valid = ix.vec.validity;
-        sp.norm2 = (const float*)ix.norm2->ptr;
-        sp.inv = (const float*)ix.inv->ptr;
-        sp.qcol = qleaf.values;
-        sp.qvalid = qleaf.validity;
-        sp.qtype = qleaf.type;
+        sp.sel = compact ? nullptr : selp;
+        sp.valid = compact ? nullptr : ix.vec.validity;
+        sp.norm2 = compact ? (const float*)cn2_mem->ptr : (const float*)ix.norm2->ptr;
+        sp.inv = compact ? (const float*)cinv_mem->ptr : (const float*)ix.inv->ptr;
+        sp.qcol = compact && qleaf.values ? cq_mem->ptr : qleaf.values;
+        sp.qvalid = compact ? nullptr : qleaf.validity;
+        sp.qtype = compact && qleaf.values ? kInt64 : qleaf.type;
         sp.qop = qleaf.op;
         sp.qlits = qlits.get();
         sp.lists = lists.get();
@@ -909,13 +1019,10 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.status = status.get();
         const size_t smem = scan_smem(stages, C);
         OXB_CUDA(cudaFuncSetAttribute(topk_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        {
-            KernelTimer timer(b, s, "topk_scan_kernel");
-            timer.begin();
-            note_launch(), topk_scan_kernel<<<grid, kScanThreads, smem, s->stream>>>(qmap, ix.xmap, sp);
-            timer.end();
-            OXB_CUDA(cudaGetLastError());
-        }
+        if (!compact) timer.begin();  // a compacted scan's segment began with the copy
+        note_launch(), topk_scan_kernel<<<grid, kScanThreads, smem, s->stream>>>(qmap, compact ? cmap : ix.xmap, sp);
+        timer.end();
+        OXB_CUDA(cudaGetLastError());
         FinalParams fp{};
         fp.k = k;
         fp.overfetch = over;
@@ -929,6 +1036,7 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         fp.counts = counts.get();
         fp.bounds = bounds.get();
         fp.table = (const float*)ix.vec.values;
+        fp.rowmap = compact ? (const unsigned*)rowmap_mem->ptr : nullptr;
         fp.queries = qf.get();
         fp.qnorm = qnorm.get();
         fp.xmax = ix.xmax;

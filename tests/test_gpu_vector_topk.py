@@ -136,3 +136,33 @@ def test_per_query_filter_literals(backend, stream, metric):
         stream, ix, dev, shared, q[:4], 9, metric, exact=True, query_leaf=(1, Cmp.Lt, [Literal.int64(t) for t in lits[:4]])
     )
     check(ide, de, ids[:4], dist[:4])
+
+
+@pytest.mark.parametrize("metric", [DistanceMetric.L2, DistanceMetric.Cosine], ids=["l2", "cosine"])
+def test_selective_where_with_per_query_literals(backend, stream, metric):
+    """A shared WHERE that keeps a fifth of the rows (the scan runs over the
+    kept rows only, copied in row order) together with a per-query leaf over
+    a nullable column: each query's answer is its own top-k; a WHERE that
+    keeps nothing pads every answer with id -1 and NaN."""
+    rng = np.random.default_rng(41)
+    n, dim, nq, k = 50_000, 96, 70, 8
+    v = rng.standard_normal((n, dim)).astype(np.float32)
+    vec = pa.FixedSizeListArray.from_arrays(pa.array(v.reshape(-1)), dim, mask=pa.array(rng.random(n) < 0.02))
+    f = pa.array(rng.integers(0, 100, n), pa.int64())
+    w = pa.array(rng.integers(0, 1000, n), pa.int64(), mask=rng.random(n) < 0.05)
+    batch = pa.RecordBatch.from_arrays([pa.array(np.arange(n, dtype=np.int64)), f, vec, w], names=["id", "f", "emb", "w"])
+    q = rng.standard_normal((nq, dim)).astype(np.float32)
+    lits = [int(t) for t in rng.integers(50, 1000, nq)]
+    shared = compare(1, Cmp.Lt, Literal.int64(20))
+    dev = backend.upload(stream, batch)
+    ix = backend.vector_index(stream, dev, 2)
+    ids, dist, _ = backend.vector_topk(
+        stream, ix, dev, shared, q, k, metric, query_leaf=(3, Cmp.Lt, [Literal.int64(t) for t in lits])
+    )
+    for i in range(nq):
+        pred = compare(3, Cmp.Lt, Literal.int64(lits[i]))
+        wi, wd = oracle.vector_topk(batch, 2, q[i : i + 1], k, int(metric), leaves(shared) + leaves(pred))
+        check(ids[i : i + 1], dist[i : i + 1], wi, wd)
+    none = compare(1, Cmp.Lt, Literal.int64(0))
+    ids0, dist0, _ = backend.vector_topk(stream, ix, dev, none, q[:3], k, metric)
+    assert (ids0 == -1).all() and np.isnan(dist0).all()
