@@ -26,7 +26,10 @@ __global__ void join_insert_kernel(JoinSlot* __restrict__ slots, unsigned int* _
                                    unsigned int capacity, const long long* __restrict__ keys,
                                    const unsigned int* __restrict__ starts, const unsigned int* __restrict__ counts,
                                    long long nruns, const unsigned int* __restrict__ rows,
-                                   unsigned int* __restrict__ status) {
+                                   unsigned int* __restrict__ status, const unsigned int* __restrict__ skip) {
+    // A dense build that met a repeated key placed rows that are not runs:
+    // nothing to insert (the host builds again by sorting).
+    if (skip && *skip) return;
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nruns;
          r += (long long)gridDim.x * blockDim.x) {
         long long key = keys[r];
@@ -249,7 +252,12 @@ unsigned int pow2_capacity(long long distinct) {
 
 }  // namespace
 
-oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const oxb_join_build_args& a) {
+namespace {
+
+// try_dense: place dense unique keys by key offset; returns null when a key
+// repeats (found at the status read), and the caller builds again sorted.
+oxb_join_table* prepare_join_build_impl(const StreamRef& s, const Backend& b, const oxb_join_build_args& a,
+                                        bool try_dense) {
     if (!a.build) fail(OXB_PLAN, "prepare_join_build: build batch is null");
     const oxb_batch& build = *a.build;
     if (a.key < 0 || a.key >= (int)build.cols.size())
@@ -269,6 +277,7 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
 
     Scratch<long long> rkeys;
     Scratch<unsigned int> rstart, rcount;
+    Scratch<unsigned int> dup;  // the dense build's repeated-key flag
     long long nruns = 0;
 
     if (a.index) {
@@ -326,18 +335,17 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
         // key order, the order the sort below gives, without the sort.
         bool placed = false;
         const unsigned long long dspan = (unsigned long long)hi - (unsigned long long)lo;
-        if (any && lo != kEmptyKey && dspan < (1ull << 26) && (long long)dspan < 4 * nvalid + 4096) {
+        // Placed optimistically: a repeated key, seen by the count, stops the
+        // insert and is read with the status at the end.
+        if (try_dense && any && lo != kEmptyKey && dspan < (1ull << 26) && (long long)dspan < 4 * nvalid + 4096) {
             const long long m = (long long)dspan + 1;
             Scratch<unsigned int> cnt(s, m, true);
-            Scratch<unsigned int> dup(s, 1, true);
+            dup = Scratch<unsigned int>(s, 1, true);
             const int grid = grid_for(b, n, 256, 8);
             note_launch(), join_dense_count_kernel<<<grid, 256, 0, s->stream>>>(key.values, key.validity, key.type, n, lo,
                                                                                cnt.get(), dup.get());
             OXB_CUDA(cudaGetLastError());
-            unsigned int hdup = 0;
-            OXB_CUDA(cudaMemcpyAsync(&hdup, dup.get(), 4, cudaMemcpyDeviceToHost, s->stream));
-            OXB_CUDA(cudaStreamSynchronize(s->stream));
-            if (!hdup) {
+            {
                 Scratch<unsigned long long> pos(s, m + 1);
                 scan_u32_to_u64(s, b, cnt.get(), pos.get(), m);
                 nruns = nvalid;
@@ -420,13 +428,23 @@ oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const o
     note_launch(), join_init_slots_kernel<<<grid_for(b, t.capacity + 1, 256, 8), 256, 0, s->stream>>>(t.slots, t.capacity + 1);
     if (nruns > 0)
         note_launch(), join_insert_kernel<<<grid_for(b, nruns, 256, 8), 256, 0, s->stream>>>(
-            t.slots, t.first_row, t.capacity, rkeys.get(), rstart.get(), rcount.get(), nruns, t.rows, status.get());
+            t.slots, t.first_row, t.capacity, rkeys.get(), rstart.get(), rcount.get(), nruns, t.rows, status.get(),
+            dup.get());
     OXB_CUDA(cudaGetLastError());
-    uint32_t st = 0;
+    uint32_t st = 0, hdup = 0;
     OXB_CUDA(cudaMemcpyAsync(&st, status.get(), 4, cudaMemcpyDeviceToHost, s->stream));
+    if (dup.get()) OXB_CUDA(cudaMemcpyAsync(&hdup, dup.get(), 4, cudaMemcpyDeviceToHost, s->stream));
     OXB_CUDA(cudaStreamSynchronize(s->stream));
+    if (hdup) return nullptr;
     check_status_word(st, "prepare_join_build");
     return out.release();
+}
+
+}  // namespace
+
+oxb_join_table* prepare_join_build(const StreamRef& s, const Backend& b, const oxb_join_build_args& a) {
+    oxb_join_table* t = prepare_join_build_impl(s, b, a, true);
+    return t ? t : prepare_join_build_impl(s, b, a, false);
 }
 
 oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_join_probe_args& a) {
