@@ -3079,6 +3079,12 @@ __device__ __noinline__ void part_rec_to_hbm(const AggProgram& P, const PartPlan
     if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
 }
 
+// The fold's accumulator operations (kind and input type together).
+enum : unsigned {
+    kFoldCount = 0, kFoldSumInt, kFoldSumF64, kFoldSumF64Int, kFoldMin32, kFoldMax32, kFoldMin64, kFoldMax64,
+    kFoldMinF, kFoldMaxF
+};
+
 // Fold: one final partition at a time (records offs[p * fstride] ..
 // offs[(p + 1) * fstride] of recs2) in a shared table of its keys.  Each
 // thread loads kFoldRows records at once, then folds them one at a time from
@@ -3104,6 +3110,22 @@ __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_consta
     for (int q = 0; q < P.nacc; q++)
         if (P.acc[q].in_type == kInt32 && (P.acc[q].kind == kAccMin || P.acc[q].kind == kAccMax))
             narrow |= 1u << P.acc[q].arr;
+    // The accumulator program as one word per accumulator: operation (kind
+    // and input type together), stored column, array.  Every operation skips
+    // a NULL input.
+    __shared__ unsigned ops[kMaxAccs];
+    if (threadIdx.x < P.nacc) {
+        const DevAcc& a = P.acc[threadIdx.x];
+        unsigned op;
+        switch (a.kind) {
+            case kAccCount: op = kFoldCount; break;
+            case kAccSumInt: op = kFoldSumInt; break;
+            case kAccSumF64: op = a.in_type == kFloat64 ? kFoldSumF64 : kFoldSumF64Int; break;
+            case kAccMin: op = a.in_type == kInt32 ? kFoldMin32 : (a.in_type == kFloat64 ? kFoldMinF : kFoldMin64); break;
+            default: op = a.in_type == kInt32 ? kFoldMax32 : (a.in_type == kFloat64 ? kFoldMaxF : kFoldMax64); break;
+        }
+        ops[threadIdx.x] = op | (unsigned)pp.col_of_acc[threadIdx.x] << 4 | (unsigned)a.arr << 8;
+    }
     for (int part = blockIdx.x; part < pp.nparts; part += gridDim.x) {
         for (int i = threadIdx.x; i < S; i += blockDim.x) {
             keys[i] = kEmptyKey;
@@ -3165,42 +3187,39 @@ __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_consta
                     atomicAdd(&rows[slot], 1u);
 #pragma unroll 1
                     for (int q = 0; q < P.nacc; q++) {
-                        const DevAcc& a = P.acc[q];
-                        const int c = pp.col_of_acc[q];
-                        const unsigned long long v =
-                            contribution_raw(a.kind, a.in_type, (flags >> c) & 1u, rec_raw<UNITS>(r0, c));
-                        unsigned long long* p = tab + a.arr * S + slot;
+                        const unsigned o = ops[q];
+                        const int c = (o >> 4) & 15;
+                        if (!((flags >> c) & 1u)) continue;
+                        const long long raw = rec_raw<UNITS>(r0, c);
+                        unsigned long long* p = tab + (o >> 8) * S + slot;
                         unsigned* w32 = (unsigned*)p;  // little-endian: [0] the low word
-                        switch (a.kind) {
-                            case kAccCount:  // at most 2^32 rows a partition
-                                if (v) atomicAdd(w32, 1u);
+                        switch (o & 15) {
+                            case kFoldCount:  // at most 2^32 rows a partition
+                                atomicAdd(w32, 1u);
                                 break;
-                            case kAccSumInt: {
+                            case kFoldSumInt: {
                                 // 64-bit wrapping add as a 32-bit add and its carry
-                                const unsigned vlo = (unsigned)v, vhi = (unsigned)(v >> 32);
+                                const unsigned vlo = (unsigned)raw, vhi = (unsigned)((unsigned long long)raw >> 32);
                                 const unsigned old = vlo ? atomicAdd(w32, vlo) : 0u;
                                 const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
                                 if (up) atomicAdd(w32 + 1, up);
                                 break;
                             }
-                            case kAccSumF64: {
-                                const double x = as_f64(v);
+                            case kFoldSumF64:
+                            case kFoldSumF64Int: {
+                                const double x = (o & 15) == kFoldSumF64 ? __longlong_as_double(raw) : (double)raw;
                                 const double old = atomicAdd((double*)p, x);
                                 double cc = 0.0;
                                 two_sum_into(old, x, &cc);
                                 if (cc != 0.0) atomicAdd((double*)(p + S), cc);
                                 break;
                             }
-                            case kAccMin:
-                                if (v == 0x7fffffffffffffffull) break;
-                                if ((narrow >> a.arr) & 1u) atomicMin((int*)w32, (int)v);
-                                else atomicMin((long long*)p, (long long)v);
-                                break;
-                            default:
-                                if (v == 0x8000000000000000ull) break;
-                                if ((narrow >> a.arr) & 1u) atomicMax((int*)w32, (int)v);
-                                else atomicMax((long long*)p, (long long)v);
-                                break;
+                            case kFoldMin32: atomicMin((int*)w32, (int)raw); break;
+                            case kFoldMax32: atomicMax((int*)w32, (int)raw); break;
+                            case kFoldMin64: atomicMin((long long*)p, raw); break;
+                            case kFoldMax64: atomicMax((long long*)p, raw); break;
+                            case kFoldMinF: atomicMin((long long*)p, total_order_key(__longlong_as_double(raw))); break;
+                            default: atomicMax((long long*)p, total_order_key(__longlong_as_double(raw))); break;
                         }
                     }
                 }
