@@ -3,7 +3,7 @@ seeded on the device), an int64 filter column uniform in [0, 100), 256 queries
 from the same distribution, top-10 under WHERE f < 30, l2 and cosine.
 Prints one JSON line per metric:
 - the scan's CUDA-event time: the copy of the kept rows to a compacted table
-  (a WHERE that keeps at most half the rows) plus the tcgen05 scan;
+  (a WHERE that keeps at most 40 % of the rows) plus the tcgen05 scan;
 - TFLOP/s: 2 x queries x kept rows x dim, the algorithmic flops (the rows
   the WHERE drops need no distance);
 - the whole call's time, how many queries took the exact path, and the BF16

@@ -939,7 +939,7 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
     }
     const bool fast = !a.exact && n > 0 && C > 0;
     std::vector<int> host_fb(nq, 1);
-    // A WHERE (or NULL vectors) that keeps at most half the rows: the kept
+    // A WHERE (or NULL vectors) that keeps at most 40 % of the rows: the kept
     // rows are copied, in row order, to a compacted BF16 table and only those
     // are scanned; the re-rank maps each candidate back to its row.
     bool compact = false;
@@ -965,7 +965,10 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         unsigned long long hn = 0;
         OXB_CUDA(cudaMemcpyAsync(&hn, woffs.get() + nwords, 8, cudaMemcpyDeviceToHost, s->stream));
         OXB_CUDA(cudaStreamSynchronize(s->stream));
-        if ((long long)hn * 2 <= n) {
+        // Measured on B200: a full scan costs about 0.72 ns a row, a compacted
+        // one about 0.57 ns (copy) + 1.14 ns (scan) a kept row: compaction
+        // pays below about 42 % kept.
+        if ((long long)hn * 5 <= n * 2) {
             compact = true;
             nsel = (long long)hn;
             const long long crows = nsel > kRTile ? nsel : kRTile;  // the tensor map's box fits
