@@ -139,3 +139,43 @@ def test_partitioned_int32_key_and_sums(backend, stream):
         backend.set_agg_variant(-1, 0)
     _, w = want(batches, spec, None)
     assert_batches_equal(got, w)
+
+
+@pytest.mark.parametrize("ncols", [2, 3], ids=["32-byte-records", "48-byte-records"])
+def test_partitioned_wide_records(backend, stream, ncols):
+    """Two or three stored columns (32- or 48-byte partition records):
+    AVG of a nullable Int32 (a Float64 sum of integers), MAX of a Float64
+    with NaN and signed zeros (totalOrder), MAX and MIN of an Int64, through
+    the partitioned passes; Float64 results to the stated tolerance, the
+    rest bit-exact."""
+    rng = np.random.default_rng(90 + ncols)
+    batches = []
+    for n in (150_000, 7, 333_333, 0, 90_000):
+        g = rng.integers(0, 250_000, n).astype(np.int64)
+        x = rng.integers(-2_000_000_000, 2_000_000_000, n).astype(np.int32)
+        v = rng.standard_normal(n) * 1e3
+        if n > 10:
+            v[:4] = [np.nan, -0.0, 0.0, -np.inf]
+        y = rng.integers(np.iinfo(np.int64).min // 4, np.iinfo(np.int64).max // 4, n, dtype=np.int64)
+        batches.append(
+            pa.RecordBatch.from_arrays(
+                [pa.array(g, mask=rng.random(n) < 0.01), pa.array(x, mask=rng.random(n) < 0.04), pa.array(v),
+                 pa.array(y)],
+                names=["g", "x", "v", "y"],
+            )
+        )
+    aggs = [(F.Avg, 1), (F.Max, 2), (F.Min, 1)] if ncols == 2 else [(F.Avg, 1), (F.Max, 2), (F.Max, 3)]
+    spec = AggregateSpec(0, aggs)
+    backend.set_agg_variant(9, 0)
+    backend.set_kernel_timing(True)
+    try:
+        got = fold(backend, stream, batches, spec, None)
+        name = backend.last_kernel_time()[0]
+    finally:
+        backend.set_agg_variant(-1, 0)
+        backend.set_kernel_timing(False)
+    assert "partitioned" in name, name
+    whole, w = want(batches, spec, None)
+    scale = oracle.aggregate(abs_columns(whole, {1}), 0, [(int(f), c) for f, c in spec.aggregates], [])
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w, float_sum_cols=(1,), scale=scale)
