@@ -463,24 +463,64 @@ __global__ void __launch_bounds__(kScanThreads, 1) topk_scan_kernel(const __grid
     }
 }
 
-// The bits of the reference's FP32 distance of one row
-// (cpu/kernels.rs:909-927): folded in index order from -0.0, one correctly
-// rounded operation per step; a zero norm gives the NaN 0x7fc00000.
-__device__ unsigned exact_distance_bits(const float* x, const float* q, int dim, int metric, float qnorm) {
-    if (metric == 0) {
-        float s = -0.0f;
-        for (int i = 0; i < dim; i++) {
-            const float d = __fsub_rn(__ldg(x + i), q[i]);
-            s = __fadd_rn(s, __fmul_rn(d, d));
-        }
-        return __float_as_uint(__fsqrt_rn(s));
-    }
+// The reference's FP32 distance of row x (l2 = sqrt of the sum of squared
+// differences, cosine = 1 - dot / (|x| |q|)), its sums taken in index order
+// (cpu/kernels.rs:909-927), by a whole warp: the lanes load the row 32
+// values at a time and form each term; the terms are added in index order
+// from -0.0, one correctly rounded operation per step (the same additions as
+// a serial loop, so the same bits); a zero norm gives the NaN 0x7fc00000.  Also the
+// FP64 dot product and squared norm, summed in any order (a report only).
+// Every lane returns the distance's bits.
+__device__ unsigned exact_distance_warp(const float* x, const float* q, int dim, int metric, float qnorm,
+                                        double* dot64, double* xx64) {
+    const int lane = threadIdx.x & 31;
     float s0 = -0.0f, s1 = -0.0f;
-    for (int i = 0; i < dim; i++) {
-        const float a = __ldg(x + i);
-        s0 = __fadd_rn(s0, __fmul_rn(a, q[i]));
-        s1 = __fadd_rn(s1, __fmul_rn(a, a));
+    double dd = 0.0, xd = 0.0;
+    constexpr int kChunks = 8;  // 32-value chunks whose loads are in flight together
+    for (int base = 0; base < dim; base += 32 * kChunks) {
+        float a[kChunks];
+#pragma unroll
+        for (int c = 0; c < kChunks; c++) {
+            const int i = base + c * 32 + lane;
+            a[c] = i < dim ? __ldg(x + i) : 0.0f;
+        }
+#pragma unroll
+        for (int c = 0; c < kChunks; c++) {
+            const int b0 = base + c * 32;
+            if (b0 >= dim) break;
+            const int i = b0 + lane;
+            float t0 = 0.0f, t1 = 0.0f;
+            if (i < dim) {
+                dd += (double)a[c] * (double)q[i];
+                xd += (double)a[c] * (double)a[c];
+                if (metric == 0) {
+                    const float d = __fsub_rn(a[c], q[i]);
+                    t0 = __fmul_rn(d, d);
+                } else {
+                    t0 = __fmul_rn(a[c], q[i]);
+                    t1 = __fmul_rn(a[c], a[c]);
+                }
+            }
+            const int cnt = dim - b0 < 32 ? dim - b0 : 32;
+            for (int l = 0; l < 32; l++) {
+                const float v0 = __shfl_sync(0xffffffffu, t0, l);
+                const float v1 = __shfl_sync(0xffffffffu, t1, l);
+                if (l < cnt) {
+                    s0 = __fadd_rn(s0, v0);
+                    s1 = __fadd_rn(s1, v1);
+                }
+            }
+        }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dd += __shfl_xor_sync(0xffffffffu, dd, o);
+        xd += __shfl_xor_sync(0xffffffffu, xd, o);
+    }
+    *dot64 = dd;
+    *xx64 = xd;
+    // every lane added the same values in the same order: s0, s1 agree
+    if (metric == 0) return __float_as_uint(__fsqrt_rn(s0));
     const float na = __fsqrt_rn(s1);
     if (na == 0.0f || qnorm == 0.0f) return 0x7fc00000u;
     return __float_as_uint(__fsub_rn(1.0f, __fdiv_rn(s0, __fmul_rn(na, qnorm))));
@@ -509,6 +549,8 @@ __device__ void bitonic_sort(unsigned long long* a, int m) {
 
 struct FinalParams {
     int k, overfetch, groups, cpg, cap, nq, dim, metric;
+    int pool_cap;  // merged candidates a query can have: a power of two >= cpg * cap, <= kPoolMax
+    int ex_cap;    // re-ranked candidates at most: min(pool_cap, kExactMax)
     const unsigned long long* lists;
     const unsigned* counts;
     const unsigned long long* bounds;
@@ -542,9 +584,9 @@ __device__ float distance_floor(int metric, float sb, float qn, float xmax) {
 
 __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_constant__ FinalParams p) {
     extern __shared__ __align__(16) unsigned char sm[];
-    unsigned long long* pool = (unsigned long long*)sm;         // kPoolMax
-    unsigned long long* ex = pool + kPoolMax;                   // kExactMax
-    float* qv = (float*)(ex + kExactMax);                       // dim
+    unsigned long long* pool = (unsigned long long*)sm;         // pool_cap
+    unsigned long long* ex = pool + p.pool_cap;                 // ex_cap
+    float* qv = (float*)(ex + p.ex_cap);                        // dim
     __shared__ int offs[1024], cnts[1024];
     __shared__ int total_s, R_s, state_s;  // state: 0 go on, 1 done, 2 exact path
     __shared__ unsigned long long bmin_s;
@@ -563,7 +605,7 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
         }
         total_s = total;
         bmin_s = bmin;
-        state_s = total > kPoolMax ? 2 : 0;
+        state_s = total > p.pool_cap ? 2 : 0;
     }
     __syncthreads();
     if (state_s == 2) {
@@ -582,25 +624,23 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
 
     const float qn = p.qnorm[q];
     int R = min(p.overfetch * p.k, total);
-    if (R > kExactMax) R = kExactMax;
+    if (R > p.ex_cap) R = p.ex_cap;
     int done = 0;
     double emax = 0.0, esum = 0.0;
     unsigned long long ecount = 0;
     for (int iter = 0; iter < 32; iter++) {
-        for (int i = done + threadIdx.x; i < R; i += blockDim.x) {
+        // One warp per candidate: coalesced row loads, the terms added in
+        // index order.
+        for (int i = done + (threadIdx.x >> 5); i < R; i += blockDim.x >> 5) {
             const unsigned idx = (unsigned)(pool[i] & 0xFFFFFFFFu);
             // compacted indices keep row order, so (score, index) sorts as (score, row)
             const unsigned row = p.rowmap ? __ldg(p.rowmap + idx) : idx;
             const float* x = p.table + (size_t)row * p.dim;
-            const unsigned d = exact_distance_bits(x, qv, p.dim, p.metric, qn);
+            double dot, xx;
+            const unsigned d = exact_distance_warp(x, qv, p.dim, p.metric, qn, &dot, &xx);
+            if ((threadIdx.x & 31) != 0) continue;
             ex[i] = ((unsigned long long)f32_order(d) << 32) | row;
             // The BF16 score against the FP64 one, for the report.
-            double dot = 0.0, xx = 0.0;
-            for (int t = 0; t < p.dim; t++) {
-                const double a = __ldg(x + t);
-                dot += a * (double)qv[t];
-                xx += a * a;
-            }
             const double s64 = p.metric == 0 ? xx - 2.0 * dot : (xx > 0.0 ? -dot / sqrt(xx) : 0.0);
             const float sa = __uint_as_float(f32_unorder((unsigned)(pool[i] >> 32)));
             const double e = fabs((double)sa - s64);
@@ -630,8 +670,8 @@ __global__ void __launch_bounds__(kFinalThreads) topk_final_kernel(const __grid_
                 if (isfinite(dk) && lb - delta > dk) st = 1;
             }
             if (st == 0) {
-                if (R < total && R < kExactMax) {
-                    R_s = min(min(2 * R, total), kExactMax);
+                if (R < total && R < p.ex_cap) {
+                    R_s = min(min(2 * R, total), p.ex_cap);
                 } else {
                     st = 2;
                 }
@@ -1049,7 +1089,14 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         fp.err_max = err.get();
         fp.err_sum = (double*)(err.get() + 1);
         fp.err_count = err.get() + 2;
-        const size_t fsmem = (size_t)(kPoolMax + kExactMax) * 8 + (size_t)dim * 4;
+        // Sized by the lists' capacity (not the largest one allowed), so
+        // that several queries share an SM.
+        int pool_cap = 2;
+        while (pool_cap < cpg * cap) pool_cap <<= 1;
+        pool_cap = std::min(pool_cap, kPoolMax);
+        fp.pool_cap = pool_cap;
+        fp.ex_cap = std::min(pool_cap, kExactMax);
+        const size_t fsmem = (size_t)(fp.pool_cap + fp.ex_cap) * 8 + (size_t)dim * 4;
         if (fsmem + 12 * 1024 > b.smem_optin) fail(OXB_UNSUPPORTED, "vector dimension too large for the re-rank kernel");
         OXB_CUDA(cudaFuncSetAttribute(topk_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
         note_launch(), topk_final_kernel<<<nq, kFinalThreads, fsmem, s->stream>>>(fp);
