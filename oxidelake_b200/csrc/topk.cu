@@ -762,10 +762,24 @@ __global__ void query_prep_kernel(const float* __restrict__ q, int nq, int dim, 
         const int r = (int)(i / dp), c = (int)(i % dp);
         out[i] = __float2bfloat16_rn(r < nq && c < dim ? q[(size_t)r * dim + c] : 0.0f);
     }
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nq; r += gridDim.x * blockDim.x) {
+    // ||q|| folded in index order from -0.0 (the reference's FP32 norm), one
+    // warp a query: coalesced loads, each lane's squares added in order.
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < nq; r += warps) {
+        const float* row = q + (size_t)r * dim;
         float s = -0.0f;
-        for (int c = 0; c < dim; c++) s = __fadd_rn(s, __fmul_rn(q[(size_t)r * dim + c], q[(size_t)r * dim + c]));
-        qnorm[r] = __fsqrt_rn(s);
+        for (int base = 0; base < dim; base += 32) {
+            const int c = base + lane;
+            const float v = c < dim ? row[c] : 0.0f;
+            const float t = __fmul_rn(v, v);
+            const int cnt = dim - base < 32 ? dim - base : 32;
+            for (int l = 0; l < 32; l++) {
+                const float u = __shfl_sync(0xffffffffu, t, l);
+                if (l < cnt) s = __fadd_rn(s, u);
+            }
+        }
+        if (lane == 0) qnorm[r] = __fsqrt_rn(s);
     }
 }
 
