@@ -229,3 +229,25 @@ def test_float_sums_are_exact_to_1e12_under_cancellation(backend, stream, varian
     assert rel.max() <= 1e-12, (rel.max(), int(rel.argmax()))
     counts = out.column(3).to_numpy()
     assert np.allclose(out.column(2).to_numpy(), exact / counts, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize(
+    "lo,span,distinct",
+    [(-5, 32_767, 32_768), (1_000, 32_768, 20_000), (0, 200_000, 120_000), (-(1 << 40), 1 << 41, 5_000)],
+    ids=["bitmap-edge", "dense-edge", "dense", "sparse-sort"],
+)
+def test_group_order_paths(backend, stream, lo, span, distinct):
+    """The emitted groups in key order whichever way they are ordered: a key
+    span below 32768 by a shared-memory bitmap, a span the keys fill to a
+    quarter by presence flags in HBM, a wider one by the radix sort; the
+    smallest and largest keys of the span always present, NULL keys last."""
+    rng = np.random.default_rng(span % 997)
+    keys = np.unique(np.concatenate([[lo, lo + span], rng.integers(lo, lo + span + 1, distinct)]))
+    n = 300_000
+    g = np.concatenate([keys, rng.choice(keys, n - len(keys))]).astype(np.int64)
+    rng.shuffle(g)
+    batch = pa.RecordBatch.from_arrays(
+        [pa.array(g, mask=rng.random(n) < 0.01), pa.array(rng.integers(-9, 10, n).astype(np.int64))], names=["g", "x"]
+    )
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.CountStar, 0), (F.Min, 1)])
+    assert_batches_equal(run(backend, stream, batch, spec), want(batch, spec))
