@@ -2705,18 +2705,6 @@ __device__ __forceinline__ int batch_of_tile_cached(const long long* ptile0, int
     return lo;
 }
 
-__device__ __forceinline__ bool keep_row(const DevPredicate& pred, const BatchCols& B, long long r) {
-    for (int l = 0; l < pred.nleaves; l++) {
-        const DevLeaf& lf = pred.leaves[l];
-        if (!valid_at(B.lvalid[l], r)) return false;
-        const long long a = lf.type == kFloat64 ? filter_order_key(__ldg((const double*)B.lvals[l] + r))
-                            : lf.type == kInt64 ? __ldg((const long long*)B.lvals[l] + r)
-                                                : (long long)__ldg((const int*)B.lvals[l] + r);
-        if (!cmp_holds(lf.op, a, lf.lit)) return false;
-    }
-    return true;
-}
-
 // Rows r0 + j * T (j < R, below `end`) that pass the WHERE and have a
 // valid key, with their keys.  The keys are loaded with the first leaf's
 // values, before any test: one memory round trip instead of two, for
