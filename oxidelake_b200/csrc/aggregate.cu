@@ -35,7 +35,6 @@ namespace {
 constexpr int kMaxOuts = OXB_MAX_AGGREGATES;
 constexpr int kMaxAccs = OXB_MAX_AGGREGATES;
 constexpr int kMaxArrays = 1 + 2 * kMaxAccs;
-constexpr int kCombineAccs = 8;  // warp combining for up to this many accumulators
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemProbes = 16;
@@ -150,32 +149,6 @@ __device__ __forceinline__ unsigned long long contribution(const DevAcc& a, long
             if (!v) return 0x8000000000000000ull;
             return (unsigned long long)(a.in_type == kFloat64 ? total_order_key(__ldg((const double*)a.values + row))
                                                               : load_int(a.values, a.in_type, row));
-    }
-}
-
-// Folds one row into the arrays at `slot`.
-__device__ __forceinline__ void apply_row(const AggProgram& P, unsigned long long* arr, long long stride, long long slot,
-                                          long long row_p, long long row_b) {
-    atomicAdd(&arr[slot], 1ull);  // array 0: rows of the group
-    for (int j = 0; j < P.nacc; j++) {
-        const DevAcc& a = P.acc[j];
-        const unsigned long long v = contribution(a, row_p, row_b);
-        unsigned long long* p = arr + a.arr * stride + slot;
-        switch (a.kind) {
-            case kAccCount:
-            case kAccSumInt:
-                if (v) atomicAdd(p, v);
-                break;
-            case kAccSumF64:
-                add_f64_comp((double*)p, (double*)(p + stride), as_f64(v));
-                break;
-            case kAccMin:
-                if (v != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)v);
-                break;
-            default:
-                if (v != 0x8000000000000000ull) atomicMax((long long*)p, (long long)v);
-                break;
-        }
     }
 }
 
@@ -501,7 +474,7 @@ template <int MAXACC, bool COMBINE, int RPT>
 __global__ void __launch_bounds__(kThreads) agg_rows_kernel(const __grid_constant__ AggProgram P,
                                                             const __grid_constant__ DevPredicate pred,
                                                             const __grid_constant__ AggKey key, long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const SmemView v = smem_view(P, smem);
     if (P.smem_slots || P.wslots) smem_init(P, v);
     const long long step = (long long)gridDim.x * blockDim.x * RPT;
@@ -560,7 +533,7 @@ __global__ void __launch_bounds__(kThreads) agg_join_kernel(const __grid_constan
                                                             const void* __restrict__ pk, const uint8_t* __restrict__ pkv,
                                                             int pk_type, const __grid_constant__ JoinTableDev jt,
                                                             long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const SmemView v = smem_view(P, smem);
     if (P.smem_slots || P.wslots) smem_init(P, v);
     const long long step = (long long)gridDim.x * blockDim.x * RPT;
@@ -826,7 +799,7 @@ template <int MAXACC>
 __global__ void __launch_bounds__(kThreads) agg_tile_rows_kernel(const __grid_constant__ AggProgram P,
                                                                  const __grid_constant__ DevPredicate pred,
                                                                  const __grid_constant__ AggKey key, long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const TileView t = tile_view(P, smem, MAXACC);
     tile_init<MAXACC>(P, t);
     for (long long base = blockIdx.x * (long long)kTileRows; base < n; base += (long long)gridDim.x * kTileRows) {
@@ -853,7 +826,7 @@ __global__ void __launch_bounds__(kThreads) agg_tile_join_kernel(const __grid_co
                                                                  const void* __restrict__ pk,
                                                                  const uint8_t* __restrict__ pkv, int pk_type,
                                                                  const __grid_constant__ JoinTableDev jt, long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const TileView t = tile_view(P, smem, MAXACC);
     tile_init<MAXACC>(P, t);
     for (long long base = blockIdx.x * (long long)kTileRows; base < n; base += (long long)gridDim.x * kTileRows) {
@@ -1865,7 +1838,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
     const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
     const __grid_constant__ FusedTab ft, long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int S = P.smem_slots;
     unsigned int* rows = (unsigned int*)smem;
     unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;  // array a at tab + a * S
@@ -1982,7 +1955,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
     const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
     const __grid_constant__ FusedTab ft, long long n) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int S = P.smem_slots;
     unsigned int* rows = (unsigned int*)smem;
     unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;  // array a at tab + a * S
@@ -3084,7 +3057,7 @@ template <int MAXACC, int UNITS>
 __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_constant__ AggProgram P,
                                                              const __grid_constant__ PartPlan pp,
                                                              const unsigned long long* __restrict__ offs) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int S = kPartSlots;
     long long* keys = (long long*)smem;
     unsigned int* rows = (unsigned int*)(keys + S);
@@ -3564,7 +3537,6 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
         if (c == 0 && maxacc <= 4 && cp.S == 0) continue;
         for (int r = 1; r <= 2; r++) candidates.push_back(AggVariant{maxacc, c == 1, r, false});
     }
-    const int S = tp.S > 0 ? tp.S : cp.S;
     int cap_class = 0;
     while ((1u << cap_class) < cap) cap_class++;
     const std::string shape = std::string(kernel_name) + "/" + std::to_string(maxacc) + "/" +
