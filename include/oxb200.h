@@ -185,7 +185,8 @@ OXB_API oxb_status oxb_copy_d2h(oxb_backend* backend, oxb_stream* stream, const 
 
 /* GpuBackend::upload: copies `ncols` host columns of `rows` rows to the
  * device.  Queued on `stream`; the host buffers must stay alive until the
- * stream is synchronized. */
+ * stream is synchronized (large pageable buffers are staged and released
+ * earlier: oxb_set_upload_staging). */
 OXB_API oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column* columns,
                       int32_t ncols, int64_t rows, oxb_batch** out);
 /* A batch over columns already in device memory (no copy; the caller keeps
@@ -514,6 +515,15 @@ OXB_API oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_
                                         float* ms);
 /* Kernels this library has launched in this process. */
 OXB_API uint64_t oxb_kernel_launches(void);
+/* Ingest of pageable host memory by oxb_upload: a column buffer of at least
+ * 4 MiB that is not page-locked is copied by `threads` host threads (the
+ * calling thread included) into a ring of four page-locked 8 MiB chunks, and
+ * each chunk's host-to-device copy overlaps the filling of the next.  Such a
+ * buffer is no longer read when oxb_upload returns.  0 = off: the driver
+ * copies pageable memory itself.  Default: half the host's cores, at most
+ * 8; the setter takes at most 32.  The ring (32 MiB
+ * page-locked) is allocated on the first staged upload. */
+OXB_API oxb_status oxb_set_upload_staging(oxb_backend* backend, int32_t threads);
 /* When enabled, the first call of each query shape times every compiled
  * variant of its main kernel (warp combining on/off, rows per thread) on
  * that call's data and keeps the fastest for later calls in this process. */

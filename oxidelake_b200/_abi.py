@@ -296,6 +296,7 @@ PROTOTYPES = {
     "oxb_last_kernel_time": (_S, [_P, C.c_char_p, C.c_int32, C.POINTER(C.c_float)]),
     "oxb_kernel_launches": (C.c_uint64, []),
     "oxb_set_autotune": (_S, [_P, C.c_int32]),
+    "oxb_set_upload_staging": (_S, [_P, C.c_int32]),
     "oxb_set_agg_variant": (_S, [_P, C.c_int32, C.c_int32]),
     "oxb_supports_predicate": (C.c_int32, [_P, C.POINTER(Leaf), C.c_int32]),
     "oxb_supports_hash_join": (C.c_int32, [_P]),

@@ -587,6 +587,11 @@ class CudaBackend:
         """First call per query shape times every kernel variant and keeps the fastest."""
         _abi.check(_L().oxb_set_autotune(self.handle, 1 if enabled else 0))
 
+    def set_upload_staging(self, threads: int) -> None:
+        """Host threads that stage large pageable columns through page-locked
+        chunks in upload (0: one driver copy per buffer)."""
+        _abi.check(_L().oxb_set_upload_staging(self.handle, threads))
+
     def set_agg_variant(self, combine: int = -1, rows_per_thread: int = 0) -> None:
         """Pins the aggregation kernel variant (-1 / 0: automatic)."""
         _abi.check(_L().oxb_set_agg_variant(self.handle, combine, rows_per_thread))

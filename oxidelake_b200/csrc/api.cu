@@ -5,6 +5,7 @@
 // and nothing falls back to the CPU.
 #include <cstdio>
 #include <new>
+#include <thread>
 
 #include "internal.h"
 
@@ -175,6 +176,9 @@ oxb_status oxb_backend_create(int32_t device, oxb_backend** out) {
     b->b.sms = prop.multiProcessorCount;
     b->b.smem_optin = prop.sharedMemPerBlockOptin;
     b->b.name = prop.name;
+    // Half the host's cores, at most 8: 8 threads fill the staging ring at
+    // about the copy engine's rate from page-locked memory.
+    b->b.stage_threads = std::clamp(int(std::thread::hardware_concurrency() / 2), 1, 8);
     *out = b;
     OXB_CATCH
 }
@@ -346,12 +350,12 @@ oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column
             size_t bytes = (size_t)rows * d.width();
             d.owner_values = dev_alloc(s, bytes, false);
             d.values = d.owner_values->ptr;
-            OXB_CUDA(cudaMemcpyAsync(d.values, c.values, bytes, cudaMemcpyHostToDevice, s->stream));
+            upload_bytes(backend->b, s, d.values, c.values, bytes);
             if (c.validity) {
                 size_t vb = ((size_t)rows + 7) / 8;
                 d.owner_validity = dev_alloc(s, vb, false);
                 d.validity = (uint8_t*)d.owner_validity->ptr;
-                OXB_CUDA(cudaMemcpyAsync(d.validity, c.validity, vb, cudaMemcpyHostToDevice, s->stream));
+                upload_bytes(backend->b, s, d.validity, c.validity, vb);
             }
         }
         b->cols.push_back(std::move(d));
@@ -624,6 +628,13 @@ oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t ro
         fail(OXB_UNSUPPORTED, "rows per thread must be 0 (automatic), 1, 2 or 4");
     backend->b.force_combine = combine;
     backend->b.force_rpt = rows_per_thread;
+    OXB_CATCH
+}
+
+oxb_status oxb_set_upload_staging(oxb_backend* backend, int32_t threads) {
+    OXB_TRY
+    use_device(backend);
+    set_upload_staging(backend->b, threads);
     OXB_CATCH
 }
 

@@ -70,6 +70,8 @@ struct Scratch {
     T* get() const { return ptr; }
 };
 
+class Stager;  // page-locked staging ring for pageable uploads (ingest.cu)
+
 struct Backend {
     int device = 0;
     int sms = 148;
@@ -79,7 +81,15 @@ struct Backend {
     bool autotune = false;  // oxb_set_autotune
     int force_combine = -1;  // oxb_set_agg_variant: -1 = tuned/default
     int force_rpt = 0;
+    int stage_threads = 8;            // oxb_set_upload_staging: 0 = off
+    std::shared_ptr<Stager> stager;   // made on the first staged upload
 };
+
+// Queues the copy of n host bytes to device memory on s.  A large pageable
+// source goes through the backend's page-locked staging ring (and is no
+// longer read on return); any other source is one cudaMemcpyAsync.
+void upload_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, size_t n);
+void set_upload_staging(Backend& b, int threads);
 
 // Counts every kernel this library launches (oxb_kernel_launches).
 void note_launch();

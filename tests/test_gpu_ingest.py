@@ -1,0 +1,83 @@
+"""Upload of pageable host columns through the page-locked staging ring
+(oxb_set_upload_staging) against the driver's own pageable copy: the device
+holds the same bytes either way, for ragged chunk counts, every column type,
+validity bitmaps, and any number of staging threads."""
+import ctypes as C
+import os
+
+import numpy as np
+import pyarrow as pa
+import pytest
+
+from oxidelake_b200 import _abi
+from oxidelake_b200.backend import DeviceBatch
+from oxidelake_b200.errors import Plan
+
+pytestmark = pytest.mark.gpu
+
+# 8 MiB slots: 2_100_003 rows give 3 chunks of Int64 (the last one ragged),
+# 2 of Int32 and 9 of an 8-wide vector; the validity bitmaps stay below the
+# 4 MiB threshold and take the single copy.
+ROWS = 2_100_003
+DEFAULT_THREADS = max(1, min(8, (os.cpu_count() or 2) // 2))
+
+
+def make_batch(rows: int, seed: int) -> pa.RecordBatch:
+    rng = np.random.default_rng(seed)
+    i64 = rng.integers(-(2**62), 2**62, size=rows, dtype=np.int64)
+    f64 = rng.standard_normal(rows)
+    null = rng.random(rows) < 0.1
+    i32 = rng.integers(-(2**31), 2**31 - 1, size=rows, dtype=np.int32)
+    vec = rng.standard_normal(rows * 8).astype(np.float32)
+    emb = pa.FixedSizeListArray.from_arrays(pa.array(vec), 8)
+    return pa.record_batch(
+        [pa.array(i64), pa.array(f64, mask=null), pa.array(i32), emb], names=["a", "b", "c", "emb"]
+    )
+
+
+@pytest.mark.parametrize("threads", [0, 1, 4, 7, 8])
+def test_staged_upload_is_byte_exact(backend, stream, threads):
+    batch = make_batch(ROWS, 11 + threads)
+    backend.set_upload_staging(threads)
+    try:
+        dev = backend.upload(stream, batch)
+        out = backend.download(stream, dev)
+    finally:
+        backend.set_upload_staging(DEFAULT_THREADS)
+    assert out.num_rows == ROWS
+    for i in range(batch.num_columns):
+        assert out.column(i).equals(batch.column(i)), batch.schema.field(i).name
+
+
+@pytest.mark.parametrize("rows", [1, 524_287, 524_288, 1_048_577])
+def test_sizes_around_the_threshold_and_one_chunk(backend, stream, rows):
+    # Int64: 4 MiB is exactly 524_288 rows, 8 MiB (one slot) 1_048_576 rows.
+    data = np.arange(rows, dtype=np.int64) * 7919 - 3
+    batch = pa.record_batch([pa.array(data)], names=["a"])
+    out = backend.download(stream, backend.upload(stream, batch))
+    assert out.column(0).equals(batch.column(0))
+
+
+def test_staged_source_may_change_once_upload_returns(backend, stream):
+    # A staged buffer is fully in page-locked slots or on the device when
+    # oxb_upload returns, so the caller may overwrite it before the stream
+    # is synchronized.
+    rows = 3_000_001
+    src = np.arange(rows, dtype=np.int64) * 3 + 1
+    keep = src.copy()
+    schema = pa.schema([("a", pa.int64())])
+    desc = (_abi.Column * 1)(_abi.Column(_abi.TYPE_INT64, 1, rows, src.ctypes.data, None))
+    h = C.c_void_p()
+    _abi.check(_abi.lib().oxb_upload(backend.handle, stream.handle, desc, 1, rows, C.byref(h)))
+    src[:] = -1
+    backend.synchronize(stream)
+    out = backend.download(stream, DeviceBatch(h.value, schema))
+    assert np.array_equal(out.column(0).to_numpy(), keep)
+
+
+def test_staging_threads_out_of_range(backend):
+    with pytest.raises(Plan):
+        backend.set_upload_staging(-1)
+    with pytest.raises(Plan):
+        backend.set_upload_staging(33)
+    backend.set_upload_staging(DEFAULT_THREADS)
