@@ -515,14 +515,16 @@ OXB_API oxb_status oxb_last_kernel_time(oxb_backend* backend, char* name, int32_
                                         float* ms);
 /* Kernels this library has launched in this process. */
 OXB_API uint64_t oxb_kernel_launches(void);
-/* Ingest of pageable host memory by oxb_upload: a column buffer of at least
+/* Ingest of pageable host memory by oxb_upload, and oxb_download_column into
+ * pageable memory: a column buffer of at least
  * 4 MiB that is not page-locked is copied by `threads` host threads (the
  * calling thread included) into a ring of four page-locked 8 MiB chunks, and
- * each chunk's host-to-device copy overlaps the filling of the next.  Such a
+ * each chunk's host-to-device copy overlaps the filling of the next (a
+ * download drains one chunk while the next ones are copied).  Such a
  * buffer is no longer read when oxb_upload returns.  0 = off: the driver
  * copies pageable memory itself.  Default: half the host's cores, at most
  * 8; the setter takes at most 32.  The ring (32 MiB
- * page-locked) is allocated on the first staged upload. */
+ * page-locked) is allocated on the first staged copy. */
 OXB_API oxb_status oxb_set_upload_staging(oxb_backend* backend, int32_t threads);
 /* When enabled, the first call of each query shape times every compiled
  * variant of its main kernel (warp combining on/off, rows per thread) on

@@ -7,7 +7,9 @@ clock around oxb_upload and the stream synchronize):
   pageable memory, staged by the driver itself;
 - "pageable, staged T threads": the page-locked ring filled by T host threads;
 - "page-locked source": the same columns in page-locked memory, one copy per
-  column (the copy engine's own rate, the ceiling of the two above).
+  column (the copy engine's own rate, the ceiling of the two above);
+- the same three cases the other way, from HBM into host memory
+  (oxb_download_column, which returns once the bytes are on the host).
 
     python -m oxidelake_b200.bench_ingest [--rows N] [--repeats R]
 """
@@ -76,6 +78,36 @@ def main() -> int:
         p[:] = a
         pinned.append((t, p))
     cases.append(("page-locked source", 0, best(pinned)))
+
+    # The way back: the same columns from HBM into host memory.
+    desc = (_abi.Column * 3)(*[_abi.Column(t, 1, n, a.ctypes.data, None) for t, a in pageable])
+    h = C.c_void_p()
+    _abi.check(lib.oxb_upload(b.handle, s.handle, desc, 3, n, C.byref(h)))
+    b.synchronize(s)
+    has = C.c_int32(0)
+
+    def download(outs) -> float:
+        t0 = time.perf_counter()
+        for i, o in enumerate(outs):
+            _abi.check(lib.oxb_download_column(b.handle, s.handle, h, i, o.ctypes.data, None, C.byref(has)))
+        return time.perf_counter() - t0
+
+    def best_down(outs) -> float:
+        download(outs)
+        return min(download(outs) for _ in range(args.repeats))
+
+    outs = [np.empty_like(a) for _, a in pageable]
+    for o in outs:
+        o.fill(0)  # touch every page before timing
+    down = []
+    for t in (0, max(1, min(8, (os.cpu_count() or 2) // 2))):
+        b.set_upload_staging(t)
+        down.append(("download to pageable, driver copy" if t == 0 else f"download to pageable, staged {t} threads", t, best_down(outs)))
+    down.append(("download to page-locked", 0, best_down([p for _, p in pinned])))
+    for o, (_, a) in zip(outs, pageable):
+        assert np.array_equal(o, a)
+    lib.oxb_batch_free(h)
+    cases += down
 
     for name, t, sec in cases:
         print(json.dumps({

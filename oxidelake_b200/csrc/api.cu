@@ -413,7 +413,7 @@ oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const o
     if (has_validity) *has_validity = c.validity ? 1 : 0;
     if (c.length > 0) {
         if (!values) fail(OXB_PLAN, "values buffer is null");
-        OXB_CUDA(cudaMemcpyAsync(values, c.values, (size_t)c.length * c.width(), cudaMemcpyDeviceToHost, s->stream));
+        download_bytes(backend->b, s, values, c.values, (size_t)c.length * c.width());
         if (c.validity && validity)
             OXB_CUDA(cudaMemcpyAsync(validity, c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
                                      s->stream));

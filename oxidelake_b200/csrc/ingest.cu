@@ -1,4 +1,5 @@
-// Ingest of host columns into device memory (oxb_upload).
+// Ingest of host columns into device memory (oxb_upload), and the way back
+// into pageable host memory (oxb_download_column).
 //
 // The reference uploads every batch from pageable memory with one plain copy
 // per buffer (crates/oxidelake-device/src/cuda/mod.rs, `upload`; the
@@ -8,7 +9,9 @@
 // page-locked chunks that a few host threads fill: the host→device copy of
 // chunk i runs while chunk i+1 is being filled, so the copy engine sees
 // page-locked memory all the time.  Page-locked and device sources, and
-// small columns, keep the single copy.
+// small columns, keep the single copy.  A large download into pageable
+// memory runs the ring the other way: the device copies into one slot while
+// the host threads drain the slot before it.
 #include <condition_variable>
 #include <thread>
 
@@ -82,6 +85,35 @@ class Stager {
         }
     }
 
+    // Copies n bytes from device `src` to pageable `dst` through the slots,
+    // draining one slot on the host while the copies into the next ones
+    // run.  Returns once every byte is in `dst`.
+    void download(const StreamRef& s, void* dst, const void* src, size_t n) {
+        std::lock_guard<std::mutex> call(call_);
+        for (int k = 0; k < kStageSlots; k++) {  // slots an upload may still be reading
+            if (pending_[k]) OXB_CUDA(cudaEventSynchronize(done_[k]));
+            pending_[k] = false;
+        }
+        const size_t chunks = (n + kStageChunk - 1) / kStageChunk;
+        auto issue = [&](size_t c) {
+            const int k = int(c % kStageSlots);
+            const size_t off = c * kStageChunk, len = std::min(kStageChunk, n - off);
+            OXB_CUDA(cudaMemcpyAsync(slot_[k], (const char*)src + off, len, cudaMemcpyDeviceToHost, s->stream));
+            OXB_CUDA(cudaEventRecord(done_[k], s->stream));
+            pending_[k] = true;
+        };
+        size_t issued = 0;
+        for (; issued < chunks && issued < size_t(kStageSlots); issued++) issue(issued);
+        for (size_t c = 0; c < chunks; c++) {
+            const int k = int(c % kStageSlots);
+            const size_t off = c * kStageChunk, len = std::min(kStageChunk, n - off);
+            OXB_CUDA(cudaEventSynchronize(done_[k]));
+            pending_[k] = false;
+            fill((char*)dst + off, (const char*)slot_[k], len);
+            if (issued < chunks) issue(issued++);  // chunk c + kStageSlots, into the slot just drained
+        }
+    }
+
   private:
     void release() {
         cudaSetDevice(device_);
@@ -145,7 +177,7 @@ class Stager {
     cudaEvent_t done_[kStageSlots] = {};
     bool pending_[kStageSlots] = {};
     uint64_t next_ = 0;
-    std::mutex call_;  // one staged upload at a time per backend
+    std::mutex call_;  // one staged copy at a time per backend
 
     std::vector<std::thread> workers_;
     std::mutex m_;
@@ -184,6 +216,22 @@ void upload_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, si
         st->upload(s, dst, src, n);
     else
         OXB_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s->stream));
+}
+
+void download_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, size_t n) {
+    if (n == 0) return;
+    std::shared_ptr<Stager> st;
+    if (n >= kStageMin && is_pageable(dst)) {
+        std::lock_guard<std::mutex> l(g_stager_mu);
+        if (b.stage_threads > 0) {
+            if (!b.stager) b.stager = std::make_shared<Stager>(b.device, b.stage_threads);
+            st = b.stager;
+        }
+    }
+    if (st)
+        st->download(s, dst, src, n);
+    else
+        OXB_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s->stream));
 }
 
 }  // namespace oxb

@@ -89,6 +89,9 @@ struct Backend {
 // source goes through the backend's page-locked staging ring (and is no
 // longer read on return); any other source is one cudaMemcpyAsync.
 void upload_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, size_t n);
+// The way back: a large pageable `dst` is filled through the same ring and
+// holds every byte on return; any other `dst` is one queued cudaMemcpyAsync.
+void download_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, size_t n);
 void set_upload_staging(Backend& b, int threads);
 
 // Counts every kernel this library launches (oxb_kernel_launches).

@@ -1,7 +1,8 @@
 """Upload of pageable host columns through the page-locked staging ring
 (oxb_set_upload_staging) against the driver's own pageable copy: the device
 holds the same bytes either way, for ragged chunk counts, every column type,
-validity bitmaps, and any number of staging threads."""
+validity bitmaps, and any number of staging threads.  Downloads into
+pageable memory run the ring the other way and are checked the same way."""
 import ctypes as C
 import os
 
@@ -73,6 +74,31 @@ def test_staged_source_may_change_once_upload_returns(backend, stream):
     backend.synchronize(stream)
     out = backend.download(stream, DeviceBatch(h.value, schema))
     assert np.array_equal(out.column(0).to_numpy(), keep)
+
+
+@pytest.mark.parametrize("threads", [0, 1, 8])
+def test_staged_download_of_a_device_result(backend, stream, threads):
+    # A filter's output is produced on the device and downloaded into
+    # pageable memory: through the ring (threads > 0) or the driver's copy.
+    from oxidelake_b200.params import Comparison as Cmp
+    from oxidelake_b200.params import Literal, compare
+
+    rows = 9_000_001
+    rng = np.random.default_rng(5)
+    a = rng.integers(0, 100, size=rows, dtype=np.int64)
+    v = rng.standard_normal(rows)
+    batch = pa.record_batch([pa.array(a), pa.array(v, mask=rng.random(rows) < 0.05)], names=["a", "v"])
+    keep = a < 90
+    want = batch.filter(pa.array(keep))
+    dev = backend.upload(stream, batch)
+    backend.set_upload_staging(threads)
+    try:
+        out = backend.download(stream, backend.filter_project(stream, dev, compare(0, Cmp.Lt, Literal.int64(90)), [0, 1]))
+    finally:
+        backend.set_upload_staging(DEFAULT_THREADS)
+    assert out.num_rows == want.num_rows
+    for i in range(2):
+        assert out.column(i).equals(want.column(i))
 
 
 def test_staging_threads_out_of_range(backend):
