@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
             "orc_agg_groups": (I64, [P]),
             "orc_agg_finish": (None, [P, P, P, P, P]),
             "orc_agg_free": (None, [P]),
+            "orc_aggregate_parallel": (I32, [P, I32, P, P, I32, I32, C.POINTER(P)]),
             "orc_join_aggregate": (I32, [P, I32, P, I32, P, I32, P, I32, C.POINTER(P)]),
             "orc_vector_distance": (I32, [P, P, I32, P, P]),
             "orc_vector_topk": (I32, [P, I32, I32, P, I32, P, I32, I32, I32, I32, P, P]),
@@ -417,11 +418,28 @@ def _finish(h, schema: pa.Schema, funcs) -> pa.RecordBatch:
     return pa.RecordBatch.from_arrays(arrays, schema=schema)
 
 
-def aggregate(batch: pa.RecordBatch, group_by: int, aggregates, leaves=None) -> pa.RecordBatch:
-    """aggregate, cpu/kernels.rs:814-818 (with an optional WHERE first)."""
+def aggregate(batch: pa.RecordBatch, group_by: int, aggregates, leaves=None, threads: int = 1) -> pa.RecordBatch:
+    """aggregate, cpu/kernels.rs:814-818 (with an optional WHERE first).
+    threads > 1 splits the groups over threads by key hash, each folding its
+    groups' rows in row order: the same bits as one thread, sooner."""
     g = GroupedAggregator(batch.schema, group_by, aggregates)
-    g.update(batch, leaves)
-    return g.finish()
+    if threads <= 1:
+        g.update(batch, leaves)
+        return g.finish()
+    cols = _Cols(batch)
+    lv, nl = _leaves(leaves)
+    spec = _Spec()
+    spec.group_by = group_by
+    spec.naggregates = len(g.aggs)
+    for j, (f, c) in enumerate(g.aggs):
+        spec.funcs[j] = f
+        spec.columns[j] = c
+    h = C.c_void_p()
+    _check(lib().orc_aggregate_parallel(cols.ptr(), cols.n, C.byref(spec), lv, nl, int(threads), C.byref(h)), "aggregate")
+    try:
+        return _finish(h.value, g.output_schema(), [f for f, _ in g.aggs])
+    finally:
+        lib().orc_agg_free(h.value)
 
 
 def join_aggregate(

@@ -709,6 +709,75 @@ static void agg_merge_state(orc_agg* a, const orc_agg* b) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* one aggregate, split by key over threads                                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct kp_task {
+    const orc_column* cols;
+    const orc_leaf* leaves;
+    int32_t nleaves;
+    int32_t part, nparts;
+    orc_agg* agg;
+} kp_task;
+
+/* Thread `part` scans every row in order and folds the selected rows whose
+ * key hashes to it (the NULL key to part 0): each group still sees its rows
+ * in row order, exactly as one sequential update folds them. */
+static void* kp_thread(void* p) {
+    kp_task* t = (kp_task*)p;
+    orc_agg* a = t->agg;
+    const orc_column* k = &t->cols[a->group_by];
+    for (int64_t row = 0; row < k->length; row++) {
+        int v = is_valid(k, row);
+        int64_t key = v ? key_at(k, row) : 0;
+        int32_t owner = v ? (int32_t)(mix64((uint64_t)key) % (uint64_t)t->nparts) : 0;
+        if (owner != t->part) continue;
+        if (!row_selected(t->cols, t->leaves, t->nleaves, row)) continue;
+        agg_update_row(a, t->cols, agg_group(a, v, key), row);
+    }
+    return NULL;
+}
+
+/* GroupedAggregator::new + update + (finish), cpu/kernels.rs:693-772, for
+ * one batch, with the groups split over `threads` by a hash of the key.  The
+ * partitions hold disjoint groups, so joining them changes no value: the
+ * result is bit-identical to a single-threaded update (a faster checker for
+ * large inputs, not another semantics). */
+int32_t orc_aggregate_parallel(const orc_column* cols, int32_t ncols, const orc_agg_spec* spec,
+                               const orc_leaf* leaves, int32_t nleaves, int32_t threads,
+                               orc_agg** out) {
+    int rc = leaf_types_ok(cols, ncols, leaves, nleaves);
+    if (rc != ORC_OK) return rc;
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    kp_task tasks[256];
+    pthread_t tids[256];
+    for (int32_t t = 0; t < threads; t++) {
+        tasks[t].cols = cols;
+        tasks[t].leaves = leaves;
+        tasks[t].nleaves = nleaves;
+        tasks[t].part = t;
+        tasks[t].nparts = threads;
+        rc = orc_agg_new(cols, ncols, spec, &tasks[t].agg);
+        if (rc != ORC_OK) {
+            for (int32_t u = 0; u < t; u++) orc_agg_free(tasks[u].agg);
+            return rc;
+        }
+    }
+    if (threads == 1) kp_thread(&tasks[0]);
+    else {
+        for (int32_t t = 0; t < threads; t++) pthread_create(&tids[t], NULL, kp_thread, &tasks[t]);
+        for (int32_t t = 0; t < threads; t++) pthread_join(tids[t], NULL);
+    }
+    for (int32_t t = 1; t < threads; t++) {
+        agg_merge_state(tasks[0].agg, tasks[t].agg);
+        orc_agg_free(tasks[t].agg);
+    }
+    *out = tasks[0].agg;
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
 /* join + filter + aggregate                                                */
 /* ------------------------------------------------------------------------ */
 

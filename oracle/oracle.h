@@ -101,6 +101,11 @@ int64_t orc_agg_groups(const orc_agg* a);
 void orc_agg_finish(const orc_agg* a, int64_t* keys, uint8_t* key_valid, int64_t* values,
                     uint8_t* valid);
 void orc_agg_free(orc_agg* a);
+/* A new aggregation of one batch (WHERE `leaves`), its groups split over
+ * `threads` by key hash; bit-identical to orc_agg_new + orc_agg_update. */
+int32_t orc_aggregate_parallel(const orc_column* cols, int32_t ncols, const orc_agg_spec* spec,
+                               const orc_leaf* leaves, int32_t nleaves, int32_t threads,
+                               orc_agg** out);
 
 /* ---- join + filter + grouped aggregation over one probe batch ----
  * Inner join probe.key = build.key; `leaves` filter the probe side; the

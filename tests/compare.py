@@ -34,9 +34,34 @@ def _bits(arr: pa.Array) -> list:
     return [int(x) if ok else None for x, ok in zip(v, valid)]
 
 
+def _primitive_equal(got: pa.Array, want: pa.Array, what: str) -> None:
+    """Bit-exact comparison of two integer or float columns in numpy: the
+    same validity, and the same value bits wherever a row is valid."""
+    if isinstance(got, pa.ChunkedArray):
+        got = got.combine_chunks()
+    if isinstance(want, pa.ChunkedArray):
+        want = want.combine_chunks()
+    gv = got.is_valid().to_numpy(zero_copy_only=False)
+    wv = want.is_valid().to_numpy(zero_copy_only=False)
+    bad = gv != wv
+    width = got.type.bit_width // 8
+    view = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width]
+    zero = 0.0 if pa.types.is_floating(got.type) else 0
+    g = got.fill_null(zero).to_numpy(zero_copy_only=False).view(view)
+    w = want.fill_null(zero).to_numpy(zero_copy_only=False).view(view)
+    bad |= gv & wv & (g != w)
+    if bad.any():
+        i = np.nonzero(bad)[0][:5]
+        raise AssertionError(f"{what}: differs at rows {i.tolist()}: got {[got[j].as_py() for j in i]} "
+                             f"want {[want[j].as_py() for j in i]}")
+
+
 def assert_columns_equal(got: pa.Array, want: pa.Array, what: str = "") -> None:
     assert len(got) == len(want), f"{what}: {len(got)} rows, want {len(want)}"
     assert got.type == want.type, f"{what}: type {got.type}, want {want.type}"
+    if pa.types.is_integer(got.type) or pa.types.is_floating(got.type):
+        _primitive_equal(got, want, what)
+        return
     g, w = _bits(got), _bits(want)
     if g != w:
         bad = [i for i, (a, b) in enumerate(zip(g, w)) if a != b][:5]
@@ -53,8 +78,9 @@ def abs_columns(batch: pa.RecordBatch, cols) -> pa.RecordBatch:
 
 def assert_close_f64(got: pa.Array, want: pa.Array, what: str = "", rtol: float = FLOAT_SUM_RTOL, scale=None) -> None:
     assert len(got) == len(want), what
-    gv, wv = got.is_valid().to_pylist(), want.is_valid().to_pylist()
-    assert gv == wv, f"{what}: validity differs"
+    gv = got.is_valid().to_numpy(zero_copy_only=False)
+    wv = want.is_valid().to_numpy(zero_copy_only=False)
+    assert (gv == wv).all(), f"{what}: validity differs"
     g = got.fill_null(0.0).to_numpy(zero_copy_only=False)
     w = want.fill_null(0.0).to_numpy(zero_copy_only=False)
     same_nan = np.isnan(g) & np.isnan(w)

@@ -297,3 +297,33 @@ def test_parallel_join_aggregate_equals_one_pass():
     assert one.column(3).to_pylist() == par.column(3).to_pylist()
     a, b = np.array(one.column(1).to_pylist()), np.array(par.column(1).to_pylist())
     assert np.all(np.abs(a - b) <= 1e-12 * np.abs(a))
+
+
+@pytest.mark.parametrize("threads", [2, 7])
+def test_parallel_aggregate_equals_one_pass(threads):
+    """The oracle's key-partitioned aggregate (the checker for the large
+    configurations) gives the same bits as one sequential update: NULL
+    keys, special floats, wrapping Int64 sums, Int32 widening, AVG."""
+    rng = np.random.default_rng(31)
+    n = 60_000
+    specials = np.array([np.nan, -np.inf, np.inf, 0.0, -0.0, 1e300, -1e300, 3.5], np.float64)
+    v = np.where(rng.random(n) < 0.2, specials[rng.integers(0, len(specials), n)], rng.uniform(-1e6, 1e6, n))
+    big = np.where(rng.random(n) < 0.1, np.iinfo(np.int64).max - rng.integers(0, 5, n), rng.integers(-100, 100, n))
+    batch = pa.RecordBatch.from_arrays(
+        [pa.array(rng.integers(-3000, 3000, n), pa.int64(), mask=rng.random(n) < 0.02),
+         pa.array(v, mask=rng.random(n) < 0.05),
+         pa.array(big.astype(np.int64)),
+         pa.array(rng.integers(-2**31, 2**31, n).astype(np.int32), mask=rng.random(n) < 0.05),
+         pa.array(rng.integers(0, 100, n).astype(np.int32))],
+        names=["g", "v", "big", "x", "f"])
+    aggs = [(0, 1), (2, 1), (3, 1), (4, 1), (0, 2), (0, 3), (2, 3), (3, 3), (4, 3), (1, 3), (5, 0)]
+    leaves = [(4, 1, 3, 70)]
+    one = oracle.aggregate(batch, 0, aggs, leaves)
+    par = oracle.aggregate(batch, 0, aggs, leaves, threads=threads)
+    assert par.schema == one.schema and par.num_rows == one.num_rows
+    for i in range(one.num_columns):
+        a, b = one.column(i), par.column(i)
+        assert a.is_valid().to_pylist() == b.is_valid().to_pylist()
+        av = a.fill_null(0).to_numpy(zero_copy_only=False)
+        bv = b.fill_null(0).to_numpy(zero_copy_only=False)
+        assert (av.view(np.uint8) == bv.view(np.uint8)).all(), one.schema.field(i).name
