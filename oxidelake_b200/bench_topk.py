@@ -6,8 +6,9 @@ Prints one JSON line per metric:
   (a WHERE that keeps at most 40 % of the rows) plus the tcgen05 scan;
 - TFLOP/s: 2 x queries x kept rows x dim, the algorithmic flops (the rows
   the WHERE drops need no distance);
-- the whole call's time, how many queries took the exact path, and the BF16
-  score error against FP64 over the re-ranked candidates.
+- the whole call's time (queries from host memory, ids and distances back
+  to host memory: the end-to-end time), how many queries took the exact
+  path, and the BF16 score error against FP64 over the re-ranked candidates.
 
     python -m oxidelake_b200.bench_topk [--rows N] [--repeats R]
 """
@@ -19,9 +20,24 @@ import sys
 import time
 from pathlib import Path
 
-import numpy as np
-
 sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+
+SEED = 0x0A11CE + 4
+
+
+def measure(backend, stream, ix, batch, queries, k: int, metric, pred, repeats: int = 3) -> dict:
+    """Best scan time (CUDA events) and call time of `repeats` top-k calls;
+    the last call's ids, distances and statistics."""
+    b, s = backend, stream
+    scan, call = [], []
+    ids = dist = st = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        ids, dist, st = b.vector_topk(s, ix, batch, pred, queries, k, metric)
+        call.append((time.perf_counter() - t0) * 1e3)
+        scan.append(b.last_kernel_time()[1])
+    return {"scan_ms": min(scan), "call_ms": min(call), "ids": ids, "dist": dist, "stats": st,
+            "h2d_bytes": int(queries.nbytes), "d2h_bytes": int(ids.nbytes + dist.nbytes)}
 
 
 def main() -> int:
@@ -33,11 +49,10 @@ def main() -> int:
     ap.add_argument("--repeats", type=int, default=3)
     args = ap.parse_args()
 
-    import pyarrow as pa
     import torch
 
-    from oxidelake_b200 import _abi
     from oxidelake_b200.backend import CudaBackend
+    from oxidelake_b200.benchkit import unit_queries, vector_table
     from oxidelake_b200.params import Comparison as Cmp
     from oxidelake_b200.params import DistanceMetric, Literal, compare
 
@@ -45,38 +60,23 @@ def main() -> int:
     b = CudaBackend(0)
     s = b.create_stream()
     b.set_kernel_timing(True)
-    g = torch.Generator(device="cuda").manual_seed(0x0A11CE + 4)
-    x = torch.randn(n, d, device="cuda", generator=g)
-    x /= x.norm(dim=1, keepdim=True)
-    f = torch.randint(0, 100, (n,), device="cuda", generator=g, dtype=torch.int64)
+    batch, x, f = vector_table(b, n, d, SEED, 100)
     kept = int((f < 30).sum().item())
     torch.cuda.synchronize()
-    schema = pa.schema([pa.field("f", pa.int64()), pa.field("emb", pa.list_(pa.float32(), d))])
-    batch = b.batch_from_device(
-        schema,
-        [_abi.Column(_abi.TYPE_INT64, 1, n, f.data_ptr(), None), _abi.Column(_abi.TYPE_VECTOR_F32, d, n, x.data_ptr(), None)],
-        n, keep=(x, f),
-    )
     t0 = time.perf_counter()
     ix = b.vector_index(s, batch, 1)
     build_s = time.perf_counter() - t0
-    q = np.random.default_rng(5).standard_normal((args.queries, d)).astype(np.float32)
-    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q = unit_queries(args.queries, d, 5)
     pred = compare(0, Cmp.Lt, Literal.int64(30))
     for metric in (DistanceMetric.L2, DistanceMetric.Cosine):
-        scan, call = [], []
-        for _ in range(args.repeats):
-            t0 = time.perf_counter()
-            ids, dist, st = b.vector_topk(s, ix, batch, pred, q, args.k, metric)
-            call.append((time.perf_counter() - t0) * 1e3)
-            scan.append(b.last_kernel_time()[1])
-        ms = min(scan)
+        m = measure(b, s, ix, batch, q, args.k, metric, pred, args.repeats)
+        st = m["stats"]
         flops = 2.0 * args.queries * kept * d
         print(json.dumps({
             "workload": "vector top-k", "metric": metric.name.lower(), "rows": n, "kept_rows": kept, "dim": d,
-            "queries": args.queries, "k": args.k, "filter": "f < 30 (30%)", "scan_ms": round(ms, 3),
-            "tflops": round(flops / ms / 1e9, 1),
-            "call_ms": round(min(call), 3), "index_build_s": round(build_s, 3), "exact_queries": st["exact_queries"],
+            "queries": args.queries, "k": args.k, "filter": "f < 30 (30%)", "scan_ms": round(m["scan_ms"], 3),
+            "tflops": round(flops / m["scan_ms"] / 1e9, 1),
+            "call_ms": round(m["call_ms"], 3), "index_build_s": round(build_s, 3), "exact_queries": st["exact_queries"],
             "reranked": st["reranked"], "bf16_score_error_max": st["max_score_error"],
             "bf16_score_error_mean": st["mean_score_error"], "data": "synthetic",
         }), flush=True)

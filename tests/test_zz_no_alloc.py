@@ -1,7 +1,8 @@
 """oxb_filter_project_noalloc: filter + projection into caller buffers with
 its scratch in a static device array.  Each case runs the existing entry
 point (oxb_filter_project) and the allocation-free one on the same batch,
-twice in a row, and requires the same rows bit for bit.  The file is named
+twice in a row, and requires the same rows bit for bit; two cases also hold
+them against the oracle, one at exactly the row limit.  The file is named
 to be collected last, so it also runs after every other GPU test has used
 the device."""
 import ctypes as C
@@ -115,3 +116,37 @@ def test_rejects_more_rows_than_the_scratch_holds(backend, stream):
     buf = backend.alloc_device(4)
     with pytest.raises(Unsupported):
         backend.filter_project_noalloc(stream, dev, None, [0], [buf.device_ptr()], [None], 1)
+
+
+def test_exactly_the_maximum_rows_against_the_oracle(backend, stream):
+    """An input of exactly OXB_NOALLOC_MAX_ROWS rows fills the static mask,
+    tile counts and scan partials to the last word: the rows equal the
+    oracle's filter_project (cpu/kernels.rs:144-152) and the existing entry
+    point's, on two calls in a row."""
+    import oracle
+    from oxidelake_b200.params import leaves
+
+    n = _abi.OXB_NOALLOC_MAX_ROWS
+    pred = and_(compare(0, Cmp.GtEq, Literal.int64(-30)), compare(2, Cmp.Lt, Literal.int32(71)))
+    projection = [1, 2, 0]
+    for call in range(2):
+        batch = _batch(n, seed=500 + call)
+        dev = backend.upload(stream, batch)
+        got = _run_noalloc(backend, stream, dev, batch, pred, projection, capacity=n)
+        want = oracle.filter_project(batch, leaves(pred), projection)
+        assert got.num_rows == want.num_rows > n // 3
+        assert_batches_equal(got, want)
+        assert_batches_equal(got, _existing(backend, stream, dev, pred, projection))
+        del dev
+
+
+def test_vector_projection_against_the_oracle(backend, stream):
+    import oracle
+    from oxidelake_b200.params import leaves
+
+    pred = compare(1, Cmp.Lt, Literal.float64(2.5))
+    for call in range(2):
+        batch = _batch(123_457, seed=900 + call, vector=True)
+        dev = backend.upload(stream, batch)
+        got = _run_noalloc(backend, stream, dev, batch, pred, [3, 1], capacity=batch.num_rows)
+        assert_batches_equal(got, oracle.filter_project(batch, leaves(pred), [3, 1]))
