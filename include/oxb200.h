@@ -545,6 +545,69 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * round to the nearest the kernel has). */
 OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);
 
+/* ---- telemetry: the counters of OperatorStats
+ *      (crates/oxidelake-core/src/telemetry.rs:38-66, 99-190) ------------- */
+
+/* The operator a call counts under.  Uploads and downloads count as
+ * transfers; the fused join-aggregate and the many-batch fold count as
+ * aggregates; top-k and vector distance as vector. */
+typedef enum oxb_operator {
+    OXB_OP_TRANSFER = 0,
+    OXB_OP_FILTER = 1,
+    OXB_OP_JOIN = 2,
+    OXB_OP_AGGREGATE = 3,
+    OXB_OP_VECTOR = 4,
+    OXB_OP_COUNT = 5
+} oxb_operator;
+
+/* One call, as OperatorStats::record_batch / record_transfer take it
+ * (telemetry.rs:140-152): rows in and out (for an aggregate the groups it
+ * emits; for a top-k the queries x k it returns), host wall time of the
+ * call, bytes the call itself moved between host and device memory.
+ * batches: the input batches the call consumed (oxb_aggregate_batches: its
+ * batch count; otherwise 1).  device_ns: the main kernel's CUDA-event time
+ * when oxb_set_kernel_timing is on, else 0.  status: the call's return. */
+typedef struct oxb_call_stats {
+    int32_t op;        /* oxb_operator */
+    int32_t status;    /* oxb_status */
+    uint64_t batches;
+    uint64_t rows_in;
+    uint64_t rows_out;
+    uint64_t elapsed_ns;
+    uint64_t device_ns;
+    uint64_t bytes_h2d;
+    uint64_t bytes_d2h;
+} oxb_call_stats;
+/* The last operator or transfer call made on the calling thread.  Replaces
+ * the Rust-side measurement around a trait call in GpuOperator::record_rows
+ * (crates/oxidelake-compute/src/operator.rs:508-520). */
+OXB_API oxb_status oxb_last_call_stats(oxb_call_stats* out);
+
+/* A backend's totals per operator since it was created (or last reset):
+ * the sums of its calls' counters, plus
+ *   unsupported       calls that returned OXB_UNSUPPORTED (where the
+ *                     reference's operator takes its CPU path and counts a
+ *                     fallback, operator.rs:573-586);
+ *   failed            calls that returned another error;
+ *   fallback_batches  batches this library ran on the CPU: always 0, it has
+ *                     no CPU path (record_fallback, telemetry.rs:162-175). */
+typedef struct oxb_operator_stats {
+    uint64_t calls;
+    uint64_t batches;
+    uint64_t rows_in;
+    uint64_t rows_out;
+    uint64_t elapsed_ns;
+    uint64_t device_ns;
+    uint64_t bytes_h2d;
+    uint64_t bytes_d2h;
+    uint64_t unsupported;
+    uint64_t failed;
+    uint64_t fallback_batches;
+} oxb_operator_stats;
+/* reset: 1 zeroes this operator's totals after reading them. */
+OXB_API oxb_status oxb_operator_stats_get(oxb_backend* backend, int32_t op, oxb_operator_stats* out,
+                                          int32_t reset);
+
 /* GpuBackend::supports_predicate / supports_hash_join / supports_aggregate
  * (backend.rs:182-197): 1 when the call runs on the device. */
 OXB_API int32_t oxb_supports_predicate(const oxb_backend* backend, const oxb_leaf* leaves,

@@ -228,6 +228,39 @@ class JoinAggregateArgs(C.Structure):
     ]
 
 
+OP_TRANSFER, OP_FILTER, OP_JOIN, OP_AGGREGATE, OP_VECTOR = 0, 1, 2, 3, 4
+
+
+class CallStats(C.Structure):
+    _fields_ = [
+        ("op", C.c_int32),
+        ("status", C.c_int32),
+        ("batches", C.c_uint64),
+        ("rows_in", C.c_uint64),
+        ("rows_out", C.c_uint64),
+        ("elapsed_ns", C.c_uint64),
+        ("device_ns", C.c_uint64),
+        ("bytes_h2d", C.c_uint64),
+        ("bytes_d2h", C.c_uint64),
+    ]
+
+
+class OperatorStats(C.Structure):
+    _fields_ = [
+        ("calls", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("rows_in", C.c_uint64),
+        ("rows_out", C.c_uint64),
+        ("elapsed_ns", C.c_uint64),
+        ("device_ns", C.c_uint64),
+        ("bytes_h2d", C.c_uint64),
+        ("bytes_d2h", C.c_uint64),
+        ("unsupported", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("fallback_batches", C.c_uint64),
+    ]
+
+
 _P = C.c_void_p
 _PP = C.POINTER(C.c_void_p)
 _S = C.c_int  # oxb_status
@@ -298,6 +331,8 @@ PROTOTYPES = {
     "oxb_set_autotune": (_S, [_P, C.c_int32]),
     "oxb_set_upload_staging": (_S, [_P, C.c_int32]),
     "oxb_set_agg_variant": (_S, [_P, C.c_int32, C.c_int32]),
+    "oxb_last_call_stats": (_S, [C.POINTER(CallStats)]),
+    "oxb_operator_stats_get": (_S, [_P, C.c_int32, C.POINTER(OperatorStats), C.c_int32]),
     "oxb_supports_predicate": (C.c_int32, [_P, C.POINTER(Leaf), C.c_int32]),
     "oxb_supports_hash_join": (C.c_int32, [_P]),
     "oxb_supports_aggregate": (C.c_int32, [_P]),

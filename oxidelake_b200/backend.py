@@ -583,6 +583,22 @@ class CudaBackend:
         _abi.check(_L().oxb_last_kernel_time(self.handle, buf, 64, C.byref(ms)))
         return buf.value.decode(), ms.value
 
+    @staticmethod
+    def last_call_stats() -> dict:
+        """The counters of the last operator or transfer call on this thread
+        (oxb_last_call_stats): what OperatorStats::record_batch and
+        record_transfer take (core/src/telemetry.rs:140-152)."""
+        st = _abi.CallStats()
+        _abi.check(_L().oxb_last_call_stats(C.byref(st)))
+        return {f: getattr(st, f) for f, _ in _abi.CallStats._fields_}
+
+    def operator_stats(self, op: int, reset: bool = False) -> dict:
+        """This backend's totals for one operator (oxb_operator_stats_get);
+        fallback_batches is always 0: the library has no CPU path."""
+        st = _abi.OperatorStats()
+        _abi.check(_L().oxb_operator_stats_get(self.handle, int(op), C.byref(st), 1 if reset else 0))
+        return {f: getattr(st, f) for f, _ in _abi.OperatorStats._fields_}
+
     def set_autotune(self, enabled: bool) -> None:
         """First call per query shape times every kernel variant and keeps the fastest."""
         _abi.check(_L().oxb_set_autotune(self.handle, 1 if enabled else 0))

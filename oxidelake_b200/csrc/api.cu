@@ -3,6 +3,7 @@
 // catches the runtime's errors at the boundary, records the message for
 // oxb_last_error() and returns the status; nothing throws across the ABI
 // and nothing falls back to the CPU.
+#include <chrono>
 #include <cstdio>
 #include <new>
 #include <thread>
@@ -15,6 +16,8 @@ namespace {
 thread_local std::string g_last_error;
 thread_local std::string g_last_kernel;
 thread_local float g_last_kernel_ms = 0.0f;
+thread_local uint64_t g_kernel_times = 0;  // kernel times recorded on this thread
+thread_local oxb_call_stats g_last_call{};
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
@@ -55,6 +58,7 @@ KernelTimer::~KernelTimer() {
         if (ok) {
             g_last_kernel = name_;
             g_last_kernel_ms = total;
+            g_kernel_times++;
         }
     }
     cudaGetLastError();
@@ -113,6 +117,69 @@ AllocRef dev_alloc(const StreamRef& s, size_t bytes, bool zero) {
 }  // namespace oxb
 
 using namespace oxb;
+
+namespace {
+
+// One entry point's counters: filled in by the call, then kept as the
+// thread's last call and added to the backend's totals for its operator.
+class CallRecord {
+  public:
+    CallRecord(oxb_backend* be, int op) : be_(be), t0_(std::chrono::steady_clock::now()), timed0_(g_kernel_times) {
+        st.op = op;
+        st.batches = 1;
+    }
+    void finish(oxb_status status) {
+        st.status = status;
+        st.elapsed_ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                            std::chrono::steady_clock::now() - t0_)
+                            .count();
+        if (status != OXB_OK) st.rows_out = 0;
+        st.device_ns = status == OXB_OK && g_kernel_times != timed0_ ? (uint64_t)(g_last_kernel_ms * 1e6) : 0;
+        g_last_call = st;
+        if (!be_ || st.op < 0 || st.op >= OXB_OP_COUNT) return;
+        std::atomic<uint64_t>* t = be_->tel.v[st.op];
+        const uint64_t add[Telemetry::kFields] = {
+            1, status == OXB_OK ? st.batches : 0, st.rows_in, st.rows_out, st.elapsed_ns, st.device_ns,
+            st.bytes_h2d, st.bytes_d2h, status == OXB_UNSUPPORTED ? 1u : 0u,
+            status != OXB_OK && status != OXB_UNSUPPORTED ? 1u : 0u, 0u /* no CPU path: never a fallback */};
+        for (int i = 0; i < Telemetry::kFields; i++)
+            if (add[i]) t[i].fetch_add(add[i], std::memory_order_relaxed);
+    }
+    oxb_call_stats st{};
+
+  private:
+    oxb_backend* be_;
+    std::chrono::steady_clock::time_point t0_;
+    uint64_t timed0_;
+};
+
+// Runs an entry point's body, turning the runtime's errors into its status
+// (the message kept for oxb_last_error) and recording the call's counters.
+template <typename F>
+oxb_status counted(oxb_backend* backend, int op, F&& body) {
+    CallRecord rec(backend, op);
+    oxb_status status = OXB_OK;
+    try {
+        body(rec.st);
+    } catch (const Error& e) {
+        g_last_error = e.message;
+        status = e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        status = OXB_ALLOCATION;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        status = OXB_EXECUTION;
+    }
+    rec.finish(status);
+    return status;
+}
+
+uint64_t column_bytes(const Column& c) {
+    return (uint64_t)c.length * c.width() + (c.validity ? ((uint64_t)c.length + 7) / 8 : 0);
+}
+
+}  // namespace
 
 #define OXB_TRY try {
 #define OXB_CATCH                                                                \
@@ -333,35 +400,37 @@ extern "C" {
 
 oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column* columns, int32_t ncols, int64_t rows,
                       oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    const StreamRef& s = stream_of(stream);
-    if (!out || (ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad upload arguments");
-    auto b = std::make_unique<oxb_batch>();
-    b->rows = rows;
-    for (int i = 0; i < ncols; i++) {
-        const oxb_column& c = columns[i];
-        check_column_desc(c, rows, i);
-        Column d;
-        d.type = c.type;
-        d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
-        d.length = rows;
-        if (rows > 0) {
-            size_t bytes = (size_t)rows * d.width();
-            d.owner_values = dev_alloc(s, bytes, false);
-            d.values = d.owner_values->ptr;
-            upload_bytes(backend->b, s, d.values, c.values, bytes);
-            if (c.validity) {
-                size_t vb = ((size_t)rows + 7) / 8;
-                d.owner_validity = dev_alloc(s, vb, false);
-                d.validity = (uint8_t*)d.owner_validity->ptr;
-                upload_bytes(backend->b, s, d.validity, c.validity, vb);
+    return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        const StreamRef& s = stream_of(stream);
+        if (!out || (ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad upload arguments");
+        auto b = std::make_unique<oxb_batch>();
+        b->rows = rows;
+        for (int i = 0; i < ncols; i++) {
+            const oxb_column& c = columns[i];
+            check_column_desc(c, rows, i);
+            Column d;
+            d.type = c.type;
+            d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
+            d.length = rows;
+            if (rows > 0) {
+                size_t bytes = (size_t)rows * d.width();
+                d.owner_values = dev_alloc(s, bytes, false);
+                d.values = d.owner_values->ptr;
+                upload_bytes(backend->b, s, d.values, c.values, bytes);
+                if (c.validity) {
+                    size_t vb = ((size_t)rows + 7) / 8;
+                    d.owner_validity = dev_alloc(s, vb, false);
+                    d.validity = (uint8_t*)d.owner_validity->ptr;
+                    upload_bytes(backend->b, s, d.validity, c.validity, vb);
+                }
             }
+            st.bytes_h2d += column_bytes(d);
+            b->cols.push_back(std::move(d));
         }
-        b->cols.push_back(std::move(d));
-    }
-    *out = b.release();
-    OXB_CATCH
+        st.rows_in = st.rows_out = (uint64_t)rows;
+        *out = b.release();
+    });
 }
 
 oxb_status oxb_batch_from_device(oxb_backend* backend, const oxb_column* columns, int32_t ncols, int64_t rows,
@@ -404,59 +473,68 @@ oxb_status oxb_batch_column(const oxb_batch* batch, int32_t index, oxb_column* o
 
 oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch, int32_t index,
                                void* values, uint8_t* validity, int32_t* has_validity) {
-    OXB_TRY
-    use_device(backend);
-    const StreamRef& s = stream_of(stream);
-    if (!batch) fail(OXB_PLAN, "batch is null");
-    if (index < 0 || index >= (int)batch->cols.size()) fail(OXB_PLAN, "column index out of range");
-    const Column& c = batch->cols[index];
-    if (has_validity) *has_validity = c.validity ? 1 : 0;
-    if (c.length > 0) {
-        if (!values) fail(OXB_PLAN, "values buffer is null");
-        download_bytes(backend->b, s, values, c.values, (size_t)c.length * c.width());
-        if (c.validity && validity)
-            OXB_CUDA(cudaMemcpyAsync(validity, c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
-                                     s->stream));
-    }
-    OXB_CUDA(cudaStreamSynchronize(s->stream));
-    OXB_CATCH
+    return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        const StreamRef& s = stream_of(stream);
+        if (!batch) fail(OXB_PLAN, "batch is null");
+        if (index < 0 || index >= (int)batch->cols.size()) fail(OXB_PLAN, "column index out of range");
+        const Column& c = batch->cols[index];
+        if (has_validity) *has_validity = c.validity ? 1 : 0;
+        if (c.length > 0) {
+            if (!values) fail(OXB_PLAN, "values buffer is null");
+            download_bytes(backend->b, s, values, c.values, (size_t)c.length * c.width());
+            st.bytes_d2h += (uint64_t)c.length * c.width();
+            if (c.validity && validity) {
+                OXB_CUDA(cudaMemcpyAsync(validity, c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
+                                         s->stream));
+                st.bytes_d2h += ((uint64_t)c.length + 7) / 8;
+            }
+        }
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+        st.rows_in = st.rows_out = (uint64_t)c.length;
+    });
 }
 
 void oxb_batch_free(oxb_batch* batch) { delete batch; }
 
 oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream, const oxb_filter_project_args* args,
                               oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = filter_project(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_FILTER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->input ? (uint64_t)args->input->rows : 0;
+        *out = filter_project(stream_of(stream), backend->b, *args);
+        st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_filter_project_noalloc(oxb_backend* backend, oxb_stream* stream, const oxb_filter_project_args* args,
                                       void* const* out_values, uint32_t* const* out_validity, int64_t capacity,
                                       int64_t* out_rows) {
-    OXB_TRY
-    use_device(backend);
-    if (!args) fail(OXB_PLAN, "null argument");
-    long long rows = 0;
-    try {
-        filter_project_noalloc(stream_of(stream), backend->b, *args, out_values, out_validity, capacity, &rows);
-    } catch (...) {
+    return counted(backend, OXB_OP_FILTER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->input ? (uint64_t)args->input->rows : 0;
+        long long rows = 0;
+        try {
+            filter_project_noalloc(stream_of(stream), backend->b, *args, out_values, out_validity, capacity, &rows);
+        } catch (...) {
+            if (out_rows) *out_rows = rows;
+            throw;
+        }
         if (out_rows) *out_rows = rows;
-        throw;
-    }
-    if (out_rows) *out_rows = rows;
-    OXB_CATCH
+        st.rows_out = (uint64_t)rows;
+    });
 }
 
 oxb_status oxb_prepare_join_build(oxb_backend* backend, oxb_stream* stream, const oxb_join_build_args* args,
                                   oxb_join_table** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = prepare_join_build(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_JOIN, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        *out = prepare_join_build(stream_of(stream), backend->b, *args);
+        st.rows_in = (uint64_t)(*out)->build_rows;
+    });
 }
 
 int64_t oxb_join_table_distinct_keys(const oxb_join_table* table) { return table ? table->t.ndistinct : -1; }
@@ -465,11 +543,13 @@ void oxb_join_table_free(oxb_join_table* table) { delete table; }
 
 oxb_status oxb_probe_join(oxb_backend* backend, oxb_stream* stream, const oxb_join_probe_args* args,
                           oxb_join_matches** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = probe_join(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_JOIN, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        *out = probe_join(stream_of(stream), backend->b, *args);
+        st.rows_in = (uint64_t)(*out)->probe_rows;
+        st.rows_out = (*out)->total;
+    });
 }
 
 uint64_t oxb_join_matches_len(const oxb_join_matches* matches) { return matches ? matches->total : 0; }
@@ -477,46 +557,60 @@ int64_t oxb_join_matches_probe_rows(const oxb_join_matches* matches) { return ma
 void oxb_join_matches_free(oxb_join_matches* matches) { delete matches; }
 
 oxb_status oxb_hash_join(oxb_backend* backend, oxb_stream* stream, const oxb_hash_join_args* args, oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = hash_join(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_JOIN, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        *out = hash_join(stream_of(stream), backend->b, *args);
+        st.rows_in = st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_aggregate(oxb_backend* backend, oxb_stream* stream, const oxb_aggregate_args* args, oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = aggregate(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_AGGREGATE, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->input ? (uint64_t)args->input->rows : 0;
+        *out = aggregate(stream_of(stream), backend->b, *args);
+        st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream, const oxb_join_aggregate_args* args,
                               oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = join_aggregate(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_AGGREGATE, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->probe ? (uint64_t)args->probe->rows : 0;
+        *out = join_aggregate(stream_of(stream), backend->b, *args);
+        st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream, const oxb_vector_distance_args* args,
                                oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = vector_distance(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_VECTOR, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->input ? (uint64_t)args->input->rows : 0;
+        st.bytes_h2d = args->dim > 0 ? (uint64_t)args->dim * 4 : 0;  // the query
+        *out = vector_distance(stream_of(stream), backend->b, *args);
+        st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_aggregate_batches(oxb_backend* backend, oxb_stream* stream, const oxb_aggregate_batches_args* args,
                                  oxb_batch** out) {
-    OXB_TRY
-    use_device(backend);
-    if (!args || !out) fail(OXB_PLAN, "null argument");
-    *out = aggregate_batches(stream_of(stream), backend->b, *args);
-    OXB_CATCH
+    return counted(backend, OXB_OP_AGGREGATE, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args || !out) fail(OXB_PLAN, "null argument");
+        if (args->inputs && args->ninputs > 0) {
+            st.batches = (uint64_t)args->ninputs;
+            for (int i = 0; i < args->ninputs; i++)
+                if (args->inputs[i]) st.rows_in += (uint64_t)args->inputs[i]->rows;
+        }
+        *out = aggregate_batches(stream_of(stream), backend->b, *args);
+        st.rows_out = (uint64_t)(*out)->rows;
+    });
 }
 
 oxb_status oxb_server_create(oxb_backend* backend, const oxb_server_config* config, oxb_server** out) {
@@ -582,10 +676,43 @@ void oxb_vector_index_free(oxb_vector_index* index) { delete index; }
 
 oxb_status oxb_vector_topk(oxb_backend* backend, oxb_stream* stream, const oxb_vector_topk_args* args,
                            int64_t* out_ids, float* out_dist, oxb_vector_topk_stats* stats) {
+    return counted(backend, OXB_OP_VECTOR, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (!args) fail(OXB_PLAN, "null argument");
+        st.rows_in = args->index ? (uint64_t)args->index->n : 0;
+        vector_topk(stream_of(stream), backend->b, *args, out_ids, out_dist, stats);
+        const uint64_t nq = (uint64_t)std::max(args->nqueries, 0), k = (uint64_t)std::max(args->k, 0);
+        st.rows_out = nq * k;
+        st.bytes_h2d = nq * (uint64_t)std::max(args->dim, 0) * 4 + (args->qleaf_column >= 0 ? nq * 8 : 0);
+        st.bytes_d2h = nq * k * 12;  // ids and distances
+    });
+}
+
+oxb_status oxb_last_call_stats(oxb_call_stats* out) {
+    if (!out) return OXB_PLAN;
+    *out = g_last_call;
+    return OXB_OK;
+}
+
+oxb_status oxb_operator_stats_get(oxb_backend* backend, int32_t op, oxb_operator_stats* out, int32_t reset) {
     OXB_TRY
-    use_device(backend);
-    if (!args) fail(OXB_PLAN, "null argument");
-    vector_topk(stream_of(stream), backend->b, *args, out_ids, out_dist, stats);
+    if (!backend || !out) fail(OXB_PLAN, "null argument");
+    if (op < 0 || op >= OXB_OP_COUNT) fail(OXB_PLAN, "operator " + std::to_string(op) + " does not exist");
+    std::atomic<uint64_t>* t = backend->tel.v[op];
+    uint64_t v[Telemetry::kFields];
+    for (int i = 0; i < Telemetry::kFields; i++)
+        v[i] = reset ? t[i].exchange(0, std::memory_order_relaxed) : t[i].load(std::memory_order_relaxed);
+    out->calls = v[0];
+    out->batches = v[1];
+    out->rows_in = v[2];
+    out->rows_out = v[3];
+    out->elapsed_ns = v[4];
+    out->device_ns = v[5];
+    out->bytes_h2d = v[6];
+    out->bytes_d2h = v[7];
+    out->unsupported = v[8];
+    out->failed = v[9];
+    out->fallback_batches = v[10];
     OXB_CATCH
 }
 

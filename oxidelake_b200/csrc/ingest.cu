@@ -55,16 +55,21 @@ class Stager {
             slot_[i] = p;
             done_[i] = e;
         }
-        for (int i = 1; i < threads; i++) workers_.emplace_back([this, i] { work(i); });
+        // A thread that cannot start leaves the ones already running to be
+        // stopped and joined here: the destructor does not run for a
+        // constructor that throws, and a joinable std::thread must not be
+        // destroyed.
+        try {
+            for (int i = 1; i < threads; i++) workers_.emplace_back([this, i] { work(i); });
+        } catch (const std::exception& e) {
+            stop_workers();
+            release();
+            fail(OXB_ALLOCATION, std::string("staging threads could not be started: ") + e.what());
+        }
     }
 
     ~Stager() {
-        {
-            std::lock_guard<std::mutex> l(m_);
-            stop_ = true;
-        }
-        go_.notify_all();
-        for (auto& t : workers_) t.join();
+        stop_workers();
         release();
     }
 
@@ -115,7 +120,25 @@ class Stager {
     }
 
   private:
+    void stop_workers() {
+        {
+            std::lock_guard<std::mutex> l(m_);
+            stop_ = true;
+        }
+        go_.notify_all();
+        for (auto& t : workers_) t.join();
+        workers_.clear();
+    }
+
+    // Frees the slots and events on the stager's device, then makes the
+    // calling thread's previous device current again: the last reference
+    // may be dropped on any thread, which must not find its device changed.
     void release() {
+        int prev = -1;
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
         cudaSetDevice(device_);
         for (int i = 0; i < kStageSlots; i++) {
             if (done_[i]) {
@@ -126,6 +149,7 @@ class Stager {
             if (slot_[i]) cudaFreeHost(slot_[i]);
             slot_[i] = nullptr;
         }
+        if (prev >= 0 && prev != device_) cudaSetDevice(prev);
     }
 
     // Host copy of n bytes split over the workers and the calling thread,

@@ -133,8 +133,22 @@ struct Column {
 
 }  // namespace oxb
 
+namespace oxb {
+// Per-operator totals of a backend (oxb_operator_stats), one atomic word per
+// field, added to by every call that names the backend.
+struct Telemetry {
+    static constexpr int kFields = 11;
+    std::atomic<uint64_t> v[OXB_OP_COUNT][kFields];
+    Telemetry() {
+        for (auto& op : v)
+            for (auto& f : op) f.store(0, std::memory_order_relaxed);
+    }
+};
+}  // namespace oxb
+
 struct oxb_backend {
     oxb::Backend b;
+    oxb::Telemetry tel;
 };
 struct oxb_stream {
     oxb::StreamRef s;

@@ -57,7 +57,8 @@ int main(void) {
   S(oxb_column) S(oxb_leaf) S(oxb_memory_info) S(oxb_filter_project_args) S(oxb_join_index)
   S(oxb_join_build_args) S(oxb_join_probe_args) S(oxb_hash_join_args) S(oxb_aggregate_spec)
   S(oxb_aggregate_args) S(oxb_vector_distance_args) S(oxb_join_aggregate_args)
-  O(oxb_leaf, lit) O(oxb_hash_join_args, projection) O(oxb_join_aggregate_args, funcs)
+  S(oxb_call_stats) S(oxb_operator_stats)
+  O(oxb_leaf, lit) O(oxb_call_stats, batches) O(oxb_operator_stats, fallback_batches) O(oxb_hash_join_args, projection) O(oxb_join_aggregate_args, funcs)
   O(oxb_join_aggregate_args, columns) O(oxb_vector_distance_args, query)
   return 0;
 }
@@ -87,6 +88,8 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
         "oxb_aggregate_args": _abi.AggregateArgs,
         "oxb_vector_distance_args": _abi.VectorDistanceArgs,
         "oxb_join_aggregate_args": _abi.JoinAggregateArgs,
+        "oxb_call_stats": _abi.CallStats,
+        "oxb_operator_stats": _abi.OperatorStats,
     }
     for name, cls in py.items():
         assert int(got[name]) == C.sizeof(cls), name
@@ -95,6 +98,30 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
     assert int(got["oxb_join_aggregate_args.funcs"]) == _abi.JoinAggregateArgs.funcs.offset
     assert int(got["oxb_join_aggregate_args.columns"]) == _abi.JoinAggregateArgs.columns.offset
     assert int(got["oxb_vector_distance_args.query"]) == _abi.VectorDistanceArgs.query.offset
+    assert int(got["oxb_call_stats.batches"]) == _abi.CallStats.batches.offset
+    assert int(got["oxb_operator_stats.fallback_batches"]) == _abi.OperatorStats.fallback_batches.offset
+
+
+def test_call_stats_record_refused_calls_without_a_device():
+    """Each operator entry point leaves its counters for
+    oxb_last_call_stats even when it fails before any device work: a filter
+    and a join given no backend are recorded under their operator with the
+    PLAN status and no rows."""
+    from oxidelake_b200 import _abi
+
+    lib = _abi.lib()
+    out = C.c_void_p()
+    args = _abi.FilterProjectArgs(None, None, 0, None, 0)
+    assert lib.oxb_filter_project(None, None, C.byref(args), C.byref(out)) == 4
+    st = _abi.CallStats()
+    assert lib.oxb_last_call_stats(C.byref(st)) == 0
+    assert (st.op, st.status, st.rows_out, st.bytes_h2d) == (_abi.OP_FILTER, 4, 0, 0)
+    jargs = _abi.JoinProbeArgs()
+    assert lib.oxb_probe_join(None, None, C.byref(jargs), C.byref(out)) == 4
+    assert lib.oxb_last_call_stats(C.byref(st)) == 0
+    assert (st.op, st.status) == (_abi.OP_JOIN, 4)
+    ops = _abi.OperatorStats()
+    assert lib.oxb_operator_stats_get(None, _abi.OP_FILTER, C.byref(ops), 0) == 4
 
 
 def test_backend_create_fails_loudly_without_a_gpu():

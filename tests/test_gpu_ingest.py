@@ -107,3 +107,40 @@ def test_staging_threads_out_of_range(backend):
     with pytest.raises(Plan):
         backend.set_upload_staging(33)
     backend.set_upload_staging(DEFAULT_THREADS)
+
+
+def test_concurrent_staged_uploads_and_downloads_on_two_streams(backend):
+    """Two host threads stage pageable columns of at least 40 MiB on their
+    own streams at the same time, each downloading into pageable memory
+    right after its upload, while one of them swaps the staging pool
+    between its rounds: every device buffer and every downloaded column is
+    byte-exact."""
+    import threading
+
+    rows = 5_500_007  # 42 MiB of Int64, 44 MiB of Float64: six slots each
+    errors = []
+
+    def worker(seed, swap):
+        try:
+            s = backend.create_stream()
+            for round_ in range(3):
+                rng = np.random.default_rng(seed * 10 + round_)
+                a = rng.integers(-(2**62), 2**62, size=rows, dtype=np.int64)
+                v = rng.standard_normal(rows)
+                batch = pa.record_batch([pa.array(a), pa.array(v)], names=["a", "v"])
+                dev = backend.upload(s, batch)
+                out = backend.download(s, dev)
+                if not (out.column(0).equals(batch.column(0)) and out.column(1).equals(batch.column(1))):
+                    errors.append(f"thread {seed} round {round_}: bytes differ")
+                if swap:
+                    backend.set_upload_staging(3 if round_ % 2 == 0 else DEFAULT_THREADS)
+        except Exception as e:  # reported below
+            errors.append(f"thread {seed}: {e!r}")
+
+    threads = [threading.Thread(target=worker, args=(1, True)), threading.Thread(target=worker, args=(2, False))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    backend.set_upload_staging(DEFAULT_THREADS)
+    assert not errors, errors
