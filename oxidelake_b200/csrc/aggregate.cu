@@ -23,6 +23,7 @@
 // is sum + compensation, O(eps) relative whatever order atomics land in.
 // Int64 SUM wraps (unsigned add); MIN/MAX over Float64 follow totalOrder via
 // integer keys, exactly as the reference.
+#include <climits>
 #include <map>
 
 #include "async_copy.cuh"
@@ -53,6 +54,12 @@ struct DevAcc {
     int in_type;
     int side;  // 0: the input (probe) row, 1: the build row
     int arr;   // its array (a Float64 sum uses arr and arr + 1)
+    // A Float64 sum whose CTA-table words hold a fixed-point window (the
+    // fused join kernels only): fix = 1, the window's unit 2^fix_lo, and
+    // fix_scale = 2^-fix_lo.
+    int fix;
+    int fix_lo;
+    double fix_scale;
 };
 
 // One output column: the function, and where its value and count live.
@@ -1774,19 +1781,112 @@ __device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const Jo
     (void)i;
 }
 
+// ---- Float64 sums as fixed-point integers in a CTA table ------------------
+// A 32-bit shared atomic add is a single instruction that settles lanes of a
+// warp on one address in hardware; a 64-bit or Float64 one is a retried
+// compare-and-swap, several times slower and far slower when lanes of a warp
+// meet on a hot group.  So a fused join kernel folds a Float64 SUM as an
+// exact integer: x = X * 2^lo with X an integer, |X| < 2^63, added into a
+// 128-bit two's-complement accumulator of four 32-bit words (limb k of slot
+// i at limbs[k * S + i]) by 32-bit atomics with their carries.  Integer
+// addition is exact and order-free, so the CTA's partial is the exact sum of
+// the values it folded.  A value that is no such integer (outside the
+// window, or with bits below 2^lo, NaN, infinity) folds into the HBM
+// accumulator with the compensated Float64 add instead.
+
+// X for x when x is an integer multiple of 2^lo with |X| < 2^63 (scale =
+// 2^-lo: the product is exact for a power of two).
+__device__ __forceinline__ bool fixed_of(double x, double scale, long long* X) {
+    const double y = __dmul_rn(x, scale);
+    if (!(fabs(y) < 9223372036854775808.0)) return false;  // also NaN
+    const long long t = __double2ll_rz(y);
+    if ((double)t != y) return false;
+    *X = t;
+    return true;
+}
+
+// Adds X (sign-extended to 128 bits) into the four limbs: each limb's add,
+// then the carry it produced into the next; what carries out of the top limb
+// is dropped (arithmetic modulo 2^128).
+__device__ __forceinline__ void shared_add_i128(unsigned* limbs, int S, int slot, long long X) {
+    const unsigned long long u = (unsigned long long)X;
+    const unsigned long long ext = X < 0 ? 0xffffffffull : 0ull;
+    unsigned long long carry = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        // at most 2^32: a limb's word plus the carry from below
+        const unsigned long long add = (k == 0 ? (u & 0xffffffffull) : k == 1 ? (u >> 32) : ext) + carry;
+        carry = add >> 32;
+        const unsigned a = (unsigned)add;
+        if (a) {
+            const unsigned old = atomicAdd(limbs + k * S + slot, a);
+            carry += old + a < old ? 1u : 0u;
+        }
+    }
+}
+
+// The exact 128-bit value of a slot's limbs, as up to three doubles whose sum
+// is value * 2^lo, each exact (52-bit chunks of the magnitude, scaled by
+// powers of two the host keeps in range); returns how many.
+__device__ __forceinline__ int fixed_chunks(const unsigned* limbs, int S, int slot, int lo, double* out) {
+    unsigned long long l = ((unsigned long long)limbs[S + slot] << 32) | limbs[slot];
+    unsigned long long h = ((unsigned long long)limbs[3 * S + slot] << 32) | limbs[2 * S + slot];
+    const bool neg = (long long)h < 0;
+    if (neg) {  // magnitude: two's complement negation of (h, l)
+        l = ~l + 1ull;
+        h = ~h + (l == 0 ? 1ull : 0ull);
+    }
+    const unsigned long long m52 = (1ull << 52) - 1ull;
+    const unsigned long long c0 = l & m52;
+    const unsigned long long c1 = ((l >> 52) | (h << 12)) & m52;
+    const unsigned long long c2 = h >> 40;
+    int n = 0;
+    const double sg = neg ? -1.0 : 1.0;
+    if (c2) out[n++] = sg * scalbn((double)c2, lo + 104);
+    if (c1) out[n++] = sg * scalbn((double)c1, lo + 52);
+    if (c0) out[n++] = sg * scalbn((double)c0, lo);
+    return n;
+}
+
+// A Float64 value outside its sum's fixed-point window: straight into the
+// group's HBM accumulator, with its rounding error into the compensation.
+__device__ __noinline__ void fused_f64_to_hbm(const AggProgram& P, const DevAcc& a, int cslot, double x) {
+    const long long g = global_slot(P, true, P.direct_lo + cslot);
+    if (g < 0) return;
+    double* d = (double*)(P.arr + a.arr * P.stride + g);
+    add_f64_comp(d, d + P.stride, x);
+}
+
 // Adds a fused kernel's CTA table into the HBM table: each occupied slot's
 // rows and arrays, Float64 sums with their compensation.
 // `keys` (shared memory) names each slot's key; null: slot i holds key
 // direct_lo + i.
 // `narrow`: bit a set when array a holds a 32-bit MIN/MAX in its low word.
+// A Float64 sum in fixed point (DevAcc::fix) holds its four limbs in arrays
+// arr and arr + 1; it reaches HBM as its exact chunks, each added with its
+// rounding error into the compensation.
 __device__ void fused_flush(const AggProgram& P, const unsigned int* rows, const unsigned long long* tab, int S,
                             const long long* keys = nullptr, unsigned narrow = 0) {
+    unsigned long long fixed = 0;  // bit a: arrays a, a + 1 hold limbs
+    for (int j = 0; j < P.nacc; j++)
+        if (P.acc[j].fix) fixed |= 1ull << P.acc[j].arr;
     for (int i = threadIdx.x; i < S; i += blockDim.x) {
         if (rows[i] == 0) continue;
         const long long g = global_slot(P, true, keys ? keys[i] : P.direct_lo + i);
         if (g < 0) continue;
         atomicAdd(&P.arr[g], (unsigned long long)rows[i]);
         for (int a = 1; a < P.narrays; a++) {
+            if ((fixed >> a) & 1ull) {
+                int lo = 0;
+                for (int j = 0; j < P.nacc; j++)
+                    if (P.acc[j].arr == a) lo = P.acc[j].fix_lo;
+                double part[3];
+                const int np = fixed_chunks((const unsigned*)(tab + a * S), S, i, lo, part);
+                double* d = (double*)(P.arr + a * P.stride + g);
+                for (int q = 0; q < np; q++) add_f64_comp(d, d + P.stride, part[q]);
+                a++;  // array a + 1 held the upper limbs
+                continue;
+            }
             unsigned long long x = tab[a * S + i];
             if ((narrow >> a) & 1u) x = (unsigned long long)(long long)(int)(unsigned)x;
             unsigned long long* d = P.arr + a * P.stride + g;
@@ -1833,8 +1933,9 @@ __device__ __forceinline__ void shared_add_u64(unsigned long long* p, unsigned l
     if (up) atomicAdd(w + 1, up);
 }
 
+
 template <int MAXACC, int RPT, bool DENSE>
-__global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
+__global__ void __launch_bounds__(kFusedThreads, 8) agg_fused_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ AggKey gkey,
     const void* __restrict__ pk, const uint8_t* __restrict__ pkv, int pk_type, const __grid_constant__ JoinTableDev jt,
     const __grid_constant__ FusedTab ft, long long n) {
@@ -1922,9 +2023,18 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fused_join_kernel(
                         if (val[j]) shared_add_u64(p, val[j]);
                         break;
                     case kAccSumF64: {
+                        const double x = as_f64(val[j]);
+                        if (a.fix) {
+                            long long X;
+                            if (fixed_of(x, a.fix_scale, &X)) {
+                                if (X) shared_add_i128((unsigned*)(tab + a.arr * S), S, cs, X);
+                            } else {
+                                fused_f64_to_hbm(P, a, cs, x);
+                            }
+                            break;
+                        }
                         // The atomic rounds old + x once; TwoSum recovers that
                         // rounding error exactly, and it joins the compensation.
-                        const double x = as_f64(val[j]);
                         const double old = atomicAdd((double*)p, x);
                         double c = 0.0;
                         two_sum_into(old, x, &c);
@@ -2051,7 +2161,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
             if (a.kind == kAccCount) {
 #pragma unroll
                 for (int r = 0; r < RPT; r++)
-                    if ((vm >> r) & 1u) atomicAdd(&col[cs[r]], 1ull);
+                    if ((vm >> r) & 1u) shared_add_u64(&col[cs[r]], 1ull);
                 continue;
             }
             long long raw[RPT];
@@ -2068,7 +2178,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
                 case kAccSumInt:
 #pragma unroll
                     for (int r = 0; r < RPT; r++)
-                        if ((vm >> r) & 1u) atomicAdd(&col[cs[r]], (unsigned long long)raw[r]);
+                        if (((vm >> r) & 1u) && raw[r]) shared_add_u64(&col[cs[r]], (unsigned long long)raw[r]);
                     break;
                 case kAccSumF64:
 #pragma unroll
@@ -2077,6 +2187,15 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
                         // The atomic rounds old + x once; TwoSum recovers that
                         // rounding error exactly, and it joins the compensation.
                         const double x = a.in_type == kFloat64 ? __longlong_as_double(raw[r]) : (double)raw[r];
+                        if (a.fix) {
+                            long long X;
+                            if (fixed_of(x, a.fix_scale, &X)) {
+                                if (X) shared_add_i128((unsigned*)col, S, cs[r], X);
+                            } else {
+                                fused_f64_to_hbm(P, a, cs[r], x);
+                            }
+                            continue;
+                        }
                         const double old = atomicAdd((double*)&col[cs[r]], x);
                         double c = 0.0;
                         two_sum_into(old, x, &c);
@@ -2273,6 +2392,20 @@ __global__ void agg_sample_kernel(const __grid_constant__ AggKey key, long long 
     }
 }
 
+// The largest finite |x| over a strided sample of a Float64 column, as the
+// bits of a non-negative double (whose integer order is its value order).
+__global__ void f64_absmax_sample_kernel(const double* __restrict__ v, const uint8_t* __restrict__ valid, long long n,
+                                         long long samples, unsigned long long* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < samples;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long row = (long long)((double)i * (double)n / (double)samples);
+        if (row >= n) row = n - 1;
+        if (!valid_at(valid, row)) continue;
+        const double x = fabs(__ldg(v + row));
+        if (isfinite(x) && x != 0.0) atomicMax(out, as_u64(x));
+    }
+}
+
 __global__ void fill_i64_kernel(long long* p, long long n, long long v) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         p[i] = v;
@@ -2298,6 +2431,7 @@ struct AggPlan {
     int acc_index[kMaxAccs];  // each accumulator's column index (-1 when not given)
     std::vector<int> out_types;
     int key_type = kInt64;
+    long long acc_rows = 0;  // rows of the side the accumulators read (fused join kernels)
 };
 
 AggPlan plan_aggregate(const std::vector<int>& funcs, const std::vector<AggInputCol>& inputs, int key_type) {
@@ -2581,6 +2715,12 @@ __global__ void __launch_bounds__(kThreads) agg_batches_kernel(const __grid_cons
 // standard error), to size the table before the fold.
 constexpr int kHllBits = 12;
 constexpr int kHllRegs = 1 << kHllBits;
+
+double as_f64_host(unsigned long long u) {
+    double d;
+    std::memcpy(&d, &u, sizeof d);
+    return d;
+}
 
 double hll_estimate(const std::vector<unsigned>& regs) {
     double sum = 0.0;
@@ -3397,22 +3537,44 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     // level further out.
     unsigned int cap;
     long long sampled_distinct = 0;
+    int fix_lo[kMaxAccs];
     unsigned long long span = ~0ull;
     long long span_lo = 0;
     {
         long long samples = sample_rows < 8192 ? sample_rows : 8192;
-        unsigned long long h[3] = {0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
+        // h[3 + j]: the sampled largest |x| of accumulator j's Float64 input,
+        // which places its fixed-point window in the fused join kernels.
+        unsigned long long h[3 + kMaxAccs] = {0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
+        const long long fsamples = plan.acc_rows < 8192 ? plan.acc_rows : 8192;
+        auto windowed = [&](int j) {
+            const DevAcc& a = P.acc[j];
+            return fusable && fsamples > 0 && a.kind == kAccSumF64 && a.in_type == kFloat64 && a.side == 0;
+        };
         if (samples > 0) {
             const unsigned int tcap = 16384;
             Scratch<long long> t(s, tcap);
-            Scratch<unsigned long long> out(s, 3);
+            Scratch<unsigned long long> out(s, 3 + kMaxAccs);
             OXB_CUDA(cudaMemcpyAsync(out.get(), h, sizeof h, cudaMemcpyHostToDevice, s->stream));
             note_launch(), fill_i64_kernel<<<16, 256, 0, s->stream>>>(t.get(), tcap, kEmptyKey);
             note_launch(), agg_sample_kernel<<<grid_for(b, samples, 256, 2), 256, 0, s->stream>>>(
                 key_for_sample, sample_rows, samples, t.get(), tcap, out.get());
+            for (int j = 0; j < P.nacc; j++)
+                if (windowed(j))
+                    note_launch(), f64_absmax_sample_kernel<<<grid_for(b, fsamples, 256, 2), 256, 0, s->stream>>>(
+                        (const double*)P.acc[j].values, P.acc[j].validity, plan.acc_rows, fsamples, out.get() + 3 + j);
             OXB_CUDA(cudaGetLastError());
             OXB_CUDA(cudaMemcpyAsync(h, out.get(), sizeof h, cudaMemcpyDeviceToHost, s->stream));
             OXB_CUDA(cudaStreamSynchronize(s->stream));
+        }
+        // The window: |x| < 2^H with H one bit above the sampled largest
+        // value's exponent (values up to twice it still fit), unit 2^(H - 63).
+        for (int j = 0; j < P.nacc; j++) {
+            fix_lo[j] = INT_MIN;
+            if (!windowed(j) || h[3 + j] == 0) continue;
+            int e = 0;
+            std::frexp(as_f64_host(h[3 + j]), &e);  // |x| < 2^e
+            const int lo = e + 1 - 63;
+            if (lo >= -900 && lo <= 800) fix_lo[j] = lo;
         }
         const long long d = (long long)h[0];
         sampled_distinct = d;
@@ -3506,6 +3668,12 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     }
     auto configure = [&](const AggVariant& v) {
         const SmemPlan& p = v.fused ? fp : (v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp)));
+        for (int j = 0; j < P.nacc; j++) {  // fixed-point Float64 sums: the fused kernels only
+            DevAcc& a = P.acc[j];
+            a.fix = v.fused && fix_lo[j] != INT_MIN;
+            a.fix_lo = a.fix ? fix_lo[j] : 0;
+            a.fix_scale = a.fix ? std::ldexp(1.0, -fix_lo[j]) : 0.0;
+        }
         P.smem_slots = p.S;
         P.wslots = p.Sw;
         P.direct = p.direct;
@@ -3955,6 +4123,7 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
     // The groups are at most the distinct group keys of the side they come
     // from; the sample is taken over that side's column.
     const long long group_rows = a.group_side ? build.rows : probe.rows;
+    plan.acc_rows = probe.rows;
     AggKey sample_key{gk->values, gk->validity, gk->type, 0};
     const JoinTableDev jt = a.table->t;
     StreamPlan SP;

@@ -144,3 +144,60 @@ def test_fused_probe_table_edges(backend, stream, rpt, form):
     finally:
         backend.set_agg_variant(-1, 0)
         backend.set_kernel_timing(False)
+
+
+@pytest.mark.parametrize("form", [5, 6, 7, 8], ids=["dense", "hashed", "dense-vec", "hashed-vec"])
+def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, form):
+    """The fused kernels fold a Float64 SUM as an exact integer in a window
+    placed from a sample of the column, and every other value through the
+    compensated Float64 path: values far above the sampled range (on rows
+    the sample does not read), values below the window's unit, NaN, both
+    infinities, -0.0 alone, negatives that cancel.  Each group's sum equals
+    the oracle's (NaN and infinities bit for bit in kind) and, where finite,
+    the exactly rounded sum to 1e-12 of its magnitude."""
+    import math
+
+    rng = np.random.default_rng(77 + form)
+    nb, npr = 1000, 400_000
+    build = pa.RecordBatch.from_arrays([pa.array(np.arange(nb, dtype=np.int64)),
+                                        pa.array((np.arange(nb) % 50).astype(np.int32))], names=["key", "attr"])
+    fk = rng.integers(0, nb, npr).astype(np.int64)
+    x = rng.uniform(-1000.0, 1000.0, npr)
+    sampled = np.zeros(npr, bool)
+    sampled[np.minimum((np.arange(8192) * npr / 8192).astype(np.int64), npr - 1)] = True
+    free = np.nonzero(~sampled)[0]
+    big = rng.choice(free, 300, replace=False)
+    x[big] = rng.choice([-1.0, 1.0], 300) * rng.uniform(1e9, 1e12, 300)  # above the window
+    tiny = rng.choice(free, 300, replace=False)
+    x[tiny] = rng.uniform(-1e-20, 1e-20, 300)  # below its unit
+    g = fk % 50
+    x[np.nonzero(g == 7)[0][:1]] = np.nan
+    x[np.nonzero(g == 8)[0][:2]] = np.inf
+    i9 = np.nonzero(g == 9)[0]
+    x[i9[:1]], x[i9[1:2]] = np.inf, -np.inf
+    x[g == 10] = -0.0
+    null = rng.random(npr) < 0.02
+    null[~np.isfinite(x)] = False  # the NaN and infinities stay in their groups
+    probe = pa.RecordBatch.from_arrays([pa.array(fk), pa.array(x, mask=null),
+                                        pa.array(rng.integers(1, 51, npr).astype(np.int32))],
+                                       names=["fk", "payload", "qty"])
+    aggs = [(F.Sum, 0, 1), (F.CountStar, 0, 0), (F.Avg, 0, 1)]
+    spec = [(int(f), s, c) for f, s, c in aggs]
+    backend.set_agg_variant(form, 2 if form in (5, 6) else 4)
+    try:
+        got = run(backend, stream, build, probe, None, (1, 1), aggs)
+    finally:
+        backend.set_agg_variant(-1, 0)
+    want = oracle.join_aggregate(probe, build, 0, 0, [], (1, 1), spec)
+    scale = oracle.join_aggregate(abs_columns(probe, {1}), build, 0, 0, [], (1, 1), spec)
+    assert_batches_equal(got, want, float_sum_cols=(1, 3), scale=scale)
+    sums = got.column(1).to_numpy(zero_copy_only=False)
+    assert np.isnan(sums[7]) and sums[8] == np.inf and np.isnan(sums[9])
+    assert sums[10] == 0.0 and not np.signbit(sums[10])
+    valid = probe.column(1).is_valid().to_numpy(zero_copy_only=False)
+    for grp in range(50):
+        if grp in (7, 8, 9):
+            continue
+        vals = x[(g == grp) & valid]
+        exact = math.fsum(vals.tolist())
+        assert abs(sums[grp] - exact) <= 1e-12 * abs(exact) + 1e-300, (grp, sums[grp], exact)
