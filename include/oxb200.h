@@ -539,7 +539,10 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * hashed form), 7 or 8 (5 or 6 interpreted a vector of rows per thread at
  * a time), 9 or 10 (oxb_aggregate_batches only: the hash-partitioned
  * passes with the planned partitions, or with their fewest; there 0..8 pin
- * the single persistent kernel);
+ * the single persistent kernel), 11 or 12 (join-aggregate only: 5 or 6 with
+ * the probe columns streamed into shared memory by bulk copies), 13 or 14
+ * (join-aggregate only: 5 or 6 compiled for the accumulator shape, when the
+ * inputs are at most two sums and no column has a validity bitmap);
  * rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
  * 1 or 2, the fused kernels 2 or 4, the vector ones 4 or 8; other values
  * round to the nearest the kernel has). */

@@ -24,6 +24,15 @@ from .params import AggregateFunction, AggregateSpec, DistanceMetric, Predicate,
 _L = _abi.lib
 
 
+def _release(fn: str, handle) -> None:
+    """Frees a handle from a finaliser.  At interpreter exit the module state
+    may already be gone; the process then returns every resource itself."""
+    try:
+        getattr(_L(), fn)(handle)
+    except Exception:
+        pass
+
+
 @dataclass
 class MemoryInfo:
     """backend.rs:18-33."""
@@ -49,7 +58,7 @@ class DeviceStream:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_stream_destroy(h)
+            _release("oxb_stream_destroy", h)
 
 
 class DeviceBuffer:
@@ -65,7 +74,7 @@ class DeviceBuffer:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_buffer_free(h)
+            _release("oxb_buffer_free", h)
 
 
 class HostBuffer:
@@ -83,7 +92,7 @@ class HostBuffer:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_host_buffer_free(h)
+            _release("oxb_host_buffer_free", h)
 
 
 class DeviceBatch:
@@ -108,7 +117,7 @@ class DeviceBatch:
     def free(self) -> None:
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_batch_free(h)
+            _release("oxb_batch_free", h)
 
     def __del__(self):
         self.free()
@@ -130,7 +139,7 @@ class DeviceJoinTable:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_join_table_free(h)
+            _release("oxb_join_table_free", h)
 
 
 class VectorIndex:
@@ -143,7 +152,7 @@ class VectorIndex:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_vector_index_free(h)
+            _release("oxb_vector_index_free", h)
 
 
 class DeviceJoinMatches:
@@ -165,7 +174,7 @@ class DeviceJoinMatches:
     def __del__(self):
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_join_matches_free(h)
+            _release("oxb_join_matches_free", h)
 
 
 def _leaf_array(pred: Optional[Predicate]) -> Tuple[Optional[C.Array], int]:
@@ -227,7 +236,7 @@ class CudaBackend:
         h, self.handle = getattr(self, "handle", None), None
         self._default_stream = None
         if h:
-            _L().oxb_backend_destroy(h)
+            _release("oxb_backend_destroy", h)
 
     # --- identity and memory (backend.rs:45-59) ---------------------------
     def kind(self) -> str:
@@ -733,7 +742,7 @@ class Server:
     def close(self) -> None:
         h, self.handle = getattr(self, "handle", None), None
         if h:
-            _L().oxb_server_destroy(h)
+            _release("oxb_server_destroy", h)
 
     def __del__(self):
         self.close()

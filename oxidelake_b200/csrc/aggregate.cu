@@ -55,11 +55,9 @@ struct DevAcc {
     int side;  // 0: the input (probe) row, 1: the build row
     int arr;   // its array (a Float64 sum uses arr and arr + 1)
     // A Float64 sum whose CTA-table words hold a fixed-point window (the
-    // fused join kernels only): fix = 1, the window's unit 2^fix_lo, and
-    // fix_scale = 2^-fix_lo.
+    // fused join kernels only): fix = 1 and the window's unit 2^fix_lo.
     int fix;
     int fix_lo;
-    double fix_scale;
 };
 
 // One output column: the function, and where its value and count live.
@@ -1794,14 +1792,31 @@ __device__ void fused_slow_row(const AggProgram& P, const AggKey& gkey, const Jo
 // window, or with bits below 2^lo, NaN, infinity) folds into the HBM
 // accumulator with the compensated Float64 add instead.
 
-// X for x when x is an integer multiple of 2^lo with |X| < 2^63 (scale =
-// 2^-lo: the product is exact for a power of two).
-__device__ __forceinline__ bool fixed_of(double x, double scale, long long* X) {
-    const double y = __dmul_rn(x, scale);
-    if (!(fabs(y) < 9223372036854775808.0)) return false;  // also NaN
-    const long long t = __double2ll_rz(y);
-    if ((double)t != y) return false;
-    *X = t;
+// X for x when x is an integer multiple of 2^lo with |X| < 2^63, read off
+// x's bits with integer operations alone (no conversion instructions): x is
+// m * 2^(e - 1075) with m its 53-bit significand, so X = m * 2^(e - 1075 - lo)
+// when that shift keeps X under 2^63 and drops no set bit of m.  Zero folds
+// as X = 0; subnormals, infinities and NaN are left to the Float64 path.
+__device__ __forceinline__ bool fixed_of(double x, int lo, long long* X) {
+    const long long bits = __double_as_longlong(x);
+    const int e = (int)((bits >> 52) & 0x7ff);
+    const unsigned long long frac = (unsigned long long)bits & ((1ull << 52) - 1ull);
+    if (e == 0) {
+        *X = 0;
+        return frac == 0;
+    }
+    if (e == 0x7ff) return false;
+    const unsigned long long m = frac | (1ull << 52);
+    const int sh = e - 1075 - lo;
+    unsigned long long mag;
+    if (sh >= 0) {
+        if (sh > 10) return false;  // m << sh would reach 2^63
+        mag = m << sh;
+    } else {
+        if (sh < -52 || (m & ((1ull << -sh) - 1ull))) return false;
+        mag = m >> -sh;
+    }
+    *X = bits < 0 ? -(long long)mag : (long long)mag;
     return true;
 }
 
@@ -2026,7 +2041,7 @@ __global__ void __launch_bounds__(kFusedThreads, 8) agg_fused_join_kernel(
                         const double x = as_f64(val[j]);
                         if (a.fix) {
                             long long X;
-                            if (fixed_of(x, a.fix_scale, &X)) {
+                            if (fixed_of(x, a.fix_lo, &X)) {
                                 if (X) shared_add_i128((unsigned*)(tab + a.arr * S), S, cs, X);
                             } else {
                                 fused_f64_to_hbm(P, a, cs, x);
@@ -2189,7 +2204,7 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
                         const double x = a.in_type == kFloat64 ? __longlong_as_double(raw[r]) : (double)raw[r];
                         if (a.fix) {
                             long long X;
-                            if (fixed_of(x, a.fix_scale, &X)) {
+                            if (fixed_of(x, a.fix_lo, &X)) {
                                 if (X) shared_add_i128((unsigned*)col, S, cs[r], X);
                             } else {
                                 fused_f64_to_hbm(P, a, cs[r], x);
@@ -2218,6 +2233,333 @@ __global__ void __launch_bounds__(kFusedThreads) agg_fusedv_join_kernel(
                         atomicMax((long long*)&col[cs[r]], v);
                     }
                     break;
+            }
+        }
+    }
+    __syncthreads();
+    fused_flush(P, rows, tab, S);
+}
+
+// ---- the fused probe table over streamed columns -------------------------
+//
+// agg_fused_join_kernel's fold (the per-join-slot probe table, a CTA table of
+// u32 row counts and fixed-point Float64 sums) fed by the streamed kernels'
+// producer: one warp copies each 1024-row tile of the probe columns into a
+// ring of shared-memory stages with bulk copies, so the consumer warps read
+// every column from shared memory and wait on HBM only through the ring,
+// not once per row and column.  Their only global loads are the probe-table
+// lookups, all of a thread's rows issued together.
+
+struct FStreamView {
+    StreamView sv;          // stages, barriers and abort flag (stream_produce's view)
+    unsigned int* rows;     // S
+    unsigned long long* tab;  // array a at tab + a * S (a >= 1)
+};
+
+size_t fstream_smem_bytes(int S, int stage_bytes, int narrays) {
+    return (size_t)kStages * stage_bytes + 16 * kStages + 16 * kStages + 16 + 128 + fused_smem_bytes(S, narrays);
+}
+
+__device__ __forceinline__ FStreamView fstream_view(const AggProgram& P, const StreamPlan& SP, unsigned char* smem) {
+    FStreamView v;
+    v.sv.stages = smem;
+    unsigned char* p = smem + (size_t)kStages * SP.stage_bytes;
+    v.sv.full = (unsigned long long*)p;
+    v.sv.empty = v.sv.full + kStages;
+    v.sv.direct = (int*)(v.sv.empty + kStages);
+    v.sv.abort = v.sv.direct + 4 * kStages;
+    v.sv.fill = v.sv.abort + 1;
+    v.sv.keys = nullptr;
+    p = (unsigned char*)(((uintptr_t)(v.sv.abort + 2) + 127) & ~(uintptr_t)127);
+    v.rows = (unsigned int*)p;
+    v.tab = (unsigned long long*)(p + fused_counts_bytes(P.smem_slots)) - P.smem_slots;
+    v.sv.tab = v.tab;
+    return v;
+}
+
+// One fast row's fold into CTA slot cs: its row count, then each
+// accumulator from the stage (or, for a direct tile, global row g).
+template <int MAXACC>
+__device__ __forceinline__ void fstream_fold(const AggProgram& P, const StreamPlan& SP, const FStreamView& v,
+                                             const unsigned char* stage, bool direct, long long g, int r, int cs) {
+    const int S = P.smem_slots;
+    atomicAdd(&v.rows[cs], 1u);
+#pragma unroll
+    for (int j = 0; j < MAXACC; j++) {
+        if (j >= P.nacc) break;
+        const DevAcc& a = P.acc[j];
+        const int c = SP.acc_col[j];
+        const bool valid = stream_valid(SP, c, stage, direct, g, r);
+        const long long raw = valid ? stream_raw(SP, c, stage, direct, g, r) : 0;
+        const unsigned long long val = contribution_raw(a.kind, a.in_type, valid, raw);
+        unsigned long long* p = v.tab + a.arr * S + cs;
+        switch (a.kind) {
+            case kAccCount:
+            case kAccSumInt:
+                if (val) shared_add_u64(p, val);
+                break;
+            case kAccSumF64: {
+                const double x = as_f64(val);
+                if (a.fix) {
+                    long long X;
+                    if (fixed_of(x, a.fix_lo, &X)) {
+                        if (X) shared_add_i128((unsigned*)(v.tab + a.arr * S), S, cs, X);
+                    } else {
+                        fused_f64_to_hbm(P, a, cs, x);
+                    }
+                    break;
+                }
+                const double old = atomicAdd((double*)p, x);
+                double comp = 0.0;
+                two_sum_into(old, x, &comp);
+                if (comp != 0.0) atomicAdd((double*)(p + S), comp);
+                break;
+            }
+            case kAccMin:
+                if (val != 0x7fffffffffffffffull) atomicMin((long long*)p, (long long)val);
+                break;
+            default:
+                if (val != 0x8000000000000000ull) atomicMax((long long*)p, (long long)val);
+                break;
+        }
+    }
+}
+
+template <int MAXACC, bool DENSE>
+__global__ void __launch_bounds__(kStreamThreads) agg_fstream_join_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ StreamPlan SP,
+    const __grid_constant__ AggKey gkey, const __grid_constant__ JoinTableDev jt, const __grid_constant__ FusedTab ft) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const FStreamView v = fstream_view(P, SP, smem);
+    const int S = P.smem_slots;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) v.rows[i] = 0;
+    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) v.tab[S + i] = init_value(P.init[1 + i / S]);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&v.sv.full[s], 1);
+            mbar_init(&v.sv.empty[s], kConsumerWarps);
+        }
+        *v.sv.abort = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        if (lane == 0) stream_produce(P, SP, v.sv);
+        __syncwarp();
+    } else {
+        const unsigned long long keep = policy_evict_last();
+        const int ct = threadIdx.x - 32;
+        constexpr int kRows = kStreamT / (32 * kConsumerWarps);
+        const unsigned int cap_mask = jt.capacity - 1u;
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < SP.ntiles; tile += gridDim.x, it++) {
+            const int st = it % kStages;
+            if (!mbar_wait(&v.sv.full[st], (it / kStages) & 1) || *(volatile int*)v.sv.abort) {
+                atomicOr(P.status, kStatusTimeout);
+                *(volatile int*)v.sv.abort = 1;
+                break;
+            }
+            const bool direct = v.sv.direct[st];
+            const unsigned char* stage = v.sv.stages + (size_t)st * SP.stage_bytes;
+            // Every row's WHERE and key from the stage, then all its lookups
+            // at once: kRows independent L2 loads a thread.
+            long long key[kRows];
+            unsigned live = 0;
+#pragma unroll
+            for (int k = 0; k < kRows; k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                key[k] = 0;
+                if (g >= SP.n) continue;
+                if (pred.nleaves && !stream_predicate(pred, SP, stage, direct, g, r)) continue;
+                if (!stream_valid(SP, SP.key_col, stage, direct, g, r)) continue;
+                key[k] = stream_raw(SP, SP.key_col, stage, direct, g, r);
+                live |= 1u << k;
+            }
+            int cs[kRows];  // the CTA slot; kDenseSlow / kDenseNone as in the dense table
+            long long js[kRows];  // the join slot of a slow row (-1: the kEmptyKey run)
+#pragma unroll
+            for (int k = 0; k < kRows; k++) {
+                cs[k] = kDenseNone;
+                js[k] = -2;
+                if (!((live >> k) & 1u)) continue;
+                if (key[k] == kEmptyKey) {
+                    if (jt.special_count) {
+                        cs[k] = kDenseSlow;
+                        js[k] = -1;
+                    }
+                    continue;
+                }
+                if (DENSE) {
+                    const unsigned long long d = (unsigned long long)key[k] - (unsigned long long)ft.dense_lo;
+                    if (d < ft.dense_n) cs[k] = (int)ld_keep_u32(ft.dense + d, keep);
+                } else {
+                    unsigned int sl = (unsigned int)(fmix64((unsigned long long)key[k]) & cap_mask);
+                    for (unsigned int q = 0; q <= cap_mask; q++) {
+                        const int4 e = ld_keep_v4(&ft.slots[sl], keep);
+                        const long long kk = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
+                        if (kk == key[k]) {
+                            if ((unsigned int)e.w == 1u && e.z >= 0) {
+                                cs[k] = e.z;
+                            } else {
+                                cs[k] = kDenseSlow;
+                                js[k] = sl;
+                            }
+                            break;
+                        }
+                        if (kk == kEmptyKey) break;
+                        sl = (sl + 1u) & cap_mask;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kRows; k++) {
+                const int r = ct + k * 32 * kConsumerWarps;
+                const long long g = tile * kStreamT + r;
+                if (cs[k] >= 0) {
+                    fstream_fold<MAXACC>(P, SP, v, stage, direct, g, r, cs[k]);
+                } else if (cs[k] == kDenseSlow) {
+                    fused_slow(P, gkey, jt, js[k] == -2 ? jt_find_slot(jt, key[k]) : js[k], g);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&v.sv.empty[st]);
+        }
+    }
+    __syncthreads();
+    fused_flush(P, v.rows, v.tab, S);
+}
+
+// ---- the fused probe table, compiled per accumulator shape ----------------
+//
+// agg_fused_join_kernel interprets the accumulator program per row (a loop
+// over accumulators, a switch on kind and type each): about 340 instructions
+// a row, which bounds it by instruction issue, not by HBM.  This form fixes
+// the accumulators at compile time (up to two probe-side sums, COUNT(*)
+// being the row count) and takes rows whose WHERE, key and inputs carry no
+// validity bitmaps: each row is its loads, a compare per leaf, one probe-
+// table lookup and its shared adds.  RPT rows a thread issue their loads
+// together.  Anything else keeps the interpreted kernels.
+
+enum : int { kLeanNone = 0, kLeanSumI32 = 1, kLeanSumI64 = 2, kLeanSumF64 = 3 };
+
+struct LeanPlan {
+    int nleaves;  // 0..2, over probe columns without validity
+    int leaf_width[2];
+    int leaf_f64[2];
+    const void* acc_values[2];
+    int acc_arr[2];  // CTA/HBM array of each sum
+    int acc_j[2];    // its accumulator in the program
+};
+
+template <int KIND>
+__device__ __forceinline__ long long lean_load(const void* values, long long i) {
+    if (KIND == kLeanSumI32) return (long long)__ldcs((const int*)values + i);
+    return __ldcs((const long long*)values + i);
+}
+
+template <int KIND>
+__device__ __forceinline__ void lean_fold(const AggProgram& P, const LeanPlan& L, int q, unsigned long long* tab, int S,
+                                          int cs, long long raw) {
+    if (KIND == kLeanNone) return;
+    unsigned long long* col = tab + L.acc_arr[q] * S;
+    if (KIND == kLeanSumF64) {
+        const DevAcc& a = P.acc[L.acc_j[q]];
+        const double x = __longlong_as_double(raw);
+        long long X;
+        if (a.fix && fixed_of(x, a.fix_lo, &X)) {
+            if (X) shared_add_i128((unsigned*)col, S, cs, X);
+        } else if (a.fix) {
+            fused_f64_to_hbm(P, a, cs, x);
+        } else {
+            const double old = atomicAdd((double*)&col[cs], x);
+            double c = 0.0;
+            two_sum_into(old, x, &c);
+            if (c != 0.0) atomicAdd((double*)&col[S + cs], c);
+        }
+    } else if (raw) {
+        shared_add_u64(&col[cs], (unsigned long long)raw);
+    }
+}
+
+template <int A0, int A1, bool DENSE, int RPT>
+__global__ void __launch_bounds__(kFusedThreads, 4) agg_lean_join_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ LeanPlan L,
+    const __grid_constant__ AggKey gkey, const void* __restrict__ pk, int pk_type, const __grid_constant__ JoinTableDev jt,
+    const __grid_constant__ FusedTab ft, long long n) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int S = P.smem_slots;
+    unsigned int* rows = (unsigned int*)smem;
+    unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) rows[i] = 0;
+    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) tab[S + i] = init_value(P.init[1 + i / S]);
+    __syncthreads();
+    const unsigned long long keep = policy_evict_last();
+    const unsigned int cap_mask = jt.capacity - 1u;
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long base = blockIdx.x * (long long)blockDim.x * RPT + threadIdx.x; base < n; base += step) {
+        long long key[RPT], v0[RPT], v1[RPT], lv0[RPT], lv1[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const long long i = base + r * (long long)kFusedThreads;
+            const bool in = i < n;
+            key[r] = !in ? 0 : pk_type == kInt64 ? __ldcs((const long long*)pk + i) : (long long)__ldcs((const int*)pk + i);
+            lv0[r] = lv1[r] = v0[r] = v1[r] = 0;
+            if (!in) continue;
+            if (L.nleaves > 0)
+                lv0[r] = L.leaf_width[0] == 8 ? __ldcs((const long long*)pred.leaves[0].values + i)
+                                              : (long long)__ldcs((const int*)pred.leaves[0].values + i);
+            if (L.nleaves > 1)
+                lv1[r] = L.leaf_width[1] == 8 ? __ldcs((const long long*)pred.leaves[1].values + i)
+                                              : (long long)__ldcs((const int*)pred.leaves[1].values + i);
+            if (A0 != kLeanNone) v0[r] = lean_load<A0>(L.acc_values[0], i);
+            if (A1 != kLeanNone) v1[r] = lean_load<A1>(L.acc_values[1], i);
+        }
+        int cs[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            cs[r] = kDenseNone;
+            const long long i = base + r * (long long)kFusedThreads;
+            if (i >= n) continue;
+            if (L.nleaves > 0) {
+                const long long a = L.leaf_f64[0] ? filter_order_key(__longlong_as_double(lv0[r])) : lv0[r];
+                if (!cmp_holds(pred.leaves[0].op, a, pred.leaves[0].lit)) continue;
+            }
+            if (L.nleaves > 1) {
+                const long long a = L.leaf_f64[1] ? filter_order_key(__longlong_as_double(lv1[r])) : lv1[r];
+                if (!cmp_holds(pred.leaves[1].op, a, pred.leaves[1].lit)) continue;
+            }
+            if (key[r] == kEmptyKey) {
+                if (jt.special_count) cs[r] = kDenseSlow;
+                continue;
+            }
+            if (DENSE) {
+                const unsigned long long d = (unsigned long long)key[r] - (unsigned long long)ft.dense_lo;
+                if (d < ft.dense_n) cs[r] = (int)ld_keep_u32(ft.dense + d, keep);
+            } else {
+                unsigned int sl = (unsigned int)(fmix64((unsigned long long)key[r]) & cap_mask);
+                for (unsigned int q = 0; q <= cap_mask; q++) {
+                    const int4 e = ld_keep_v4(&ft.slots[sl], keep);
+                    const long long kk = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
+                    if (kk == key[r]) {
+                        cs[r] = ((unsigned int)e.w == 1u && e.z >= 0) ? e.z : kDenseSlow;
+                        break;
+                    }
+                    if (kk == kEmptyKey) break;
+                    sl = (sl + 1u) & cap_mask;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            if (cs[r] >= 0) {
+                atomicAdd(&rows[cs[r]], 1u);
+                lean_fold<A0>(P, L, 0, tab, S, cs[r], v0[r]);
+                lean_fold<A1>(P, L, 1, tab, S, cs[r], v1[r]);
+            } else if (cs[r] == kDenseSlow) {
+                const long long i = base + r * (long long)kFusedThreads;
+                fused_slow(P, gkey, jt, key[r] == kEmptyKey ? -1 : jt_find_slot(jt, key[r]), i);
             }
         }
     }
@@ -2543,6 +2885,8 @@ struct AggVariant {
     bool fused = false;   // the fused probe-table join kernel (rpt used)
     bool dense = false;   // ... with the dense lookup table
     bool vec = false;     // ... interpreted a vector of rows at a time (rpt 4 or 8)
+    bool fstream = false; // ... fed by streamed columns (agg_fstream_join_kernel)
+    bool lean = false;    // ... compiled per accumulator shape (agg_lean_join_kernel)
 };
 
 // The streamed kernels' plan: the probe-side columns (deduplicated) with
@@ -3412,7 +3756,81 @@ FusedKernel fused_kernel_for(const AggVariant& v) {
     fail(OXB_EXECUTION, "no fused join kernel for this variant");
 }
 
+using FStreamKernel = void (*)(const AggProgram, const DevPredicate, const StreamPlan, const AggKey,
+                               const JoinTableDev, const FusedTab);
+FStreamKernel fstream_kernel_for(const AggVariant& v) {
+    if (v.maxacc == 2) return v.dense ? agg_fstream_join_kernel<2, true> : agg_fstream_join_kernel<2, false>;
+    return v.dense ? agg_fstream_join_kernel<4, true> : agg_fstream_join_kernel<4, false>;
+}
+
+// The lean kernels' accumulator shape for a program, or false when the
+// program or its columns need the interpreted kernels.
+bool lean_shape(const AggProgram& P, const DevPredicate& pred, const uint8_t* key_validity, int* a0, int* a1) {
+    if (key_validity || P.nacc > 2 || pred.nleaves > 2) return false;
+    for (int l = 0; l < pred.nleaves; l++)
+        if (pred.leaves[l].validity) return false;
+    int k[2] = {kLeanNone, kLeanNone};
+    for (int j = 0; j < P.nacc; j++) {
+        const DevAcc& a = P.acc[j];
+        if (a.side != 0 || a.validity) return false;
+        if (a.kind == kAccSumInt) k[j] = a.in_type == kInt32 ? kLeanSumI32 : kLeanSumI64;
+        else if (a.kind == kAccSumF64 && a.in_type == kFloat64) k[j] = kLeanSumF64;
+        else return false;
+    }
+    *a0 = k[0];
+    *a1 = k[1];
+    return true;
+}
+
+LeanPlan lean_plan(const AggProgram& P, const DevPredicate& pred) {
+    LeanPlan L{};
+    L.nleaves = pred.nleaves;
+    for (int l = 0; l < pred.nleaves; l++) {
+        L.leaf_width[l] = pred.leaves[l].type == kInt32 ? 4 : 8;
+        L.leaf_f64[l] = pred.leaves[l].type == kFloat64;
+    }
+    for (int j = 0; j < P.nacc; j++) {
+        L.acc_values[j] = P.acc[j].values;
+        L.acc_arr[j] = P.acc[j].arr;
+        L.acc_j[j] = j;
+    }
+    return L;
+}
+
+using LeanKernel = void (*)(const AggProgram, const DevPredicate, const LeanPlan, const AggKey, const void*, int,
+                            const JoinTableDev, const FusedTab, long long);
+
+template <int A0, int A1>
+LeanKernel lean_kernel_pick(bool dense, int rpt) {
+    if (dense) return rpt >= 4 ? agg_lean_join_kernel<A0, A1, true, 4> : agg_lean_join_kernel<A0, A1, true, 2>;
+    return rpt >= 4 ? agg_lean_join_kernel<A0, A1, false, 4> : agg_lean_join_kernel<A0, A1, false, 2>;
+}
+
+template <int A0>
+LeanKernel lean_kernel_a1(int a1, bool dense, int rpt) {
+    switch (a1) {
+        case kLeanSumI32: return lean_kernel_pick<A0, kLeanSumI32>(dense, rpt);
+        case kLeanSumI64: return lean_kernel_pick<A0, kLeanSumI64>(dense, rpt);
+        case kLeanSumF64: return lean_kernel_pick<A0, kLeanSumF64>(dense, rpt);
+        default: return lean_kernel_pick<A0, kLeanNone>(dense, rpt);
+    }
+}
+
+LeanKernel lean_kernel_for(int a0, int a1, bool dense, int rpt) {
+    switch (a0) {
+        case kLeanSumI32: return lean_kernel_a1<kLeanSumI32>(a1, dense, rpt);
+        case kLeanSumI64: return lean_kernel_a1<kLeanSumI64>(a1, dense, rpt);
+        case kLeanSumF64: return lean_kernel_a1<kLeanSumF64>(a1, dense, rpt);
+        default: return lean_kernel_pick<kLeanNone, kLeanNone>(dense, rpt);
+    }
+}
+
 std::string variant_name(const char* base, const AggVariant& v) {
+    if (v.fused && v.lean)
+        return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") + "lean," +
+               std::to_string(v.rpt) + ">";
+    if (v.fused && v.fstream)
+        return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") + "stream>";
     if (v.fused)
         return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") +
                (v.vec ? "vec," : "") + std::to_string(v.rpt) + ">";
@@ -3666,13 +4084,22 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
             fp.bytes = bytes;
         }
     }
+    // ... and over streamed columns: the same table beside the stage ring.
+    SmemPlan fsp;
+    if (fp.S > 0 && SP && SP->n >= 4ll * kStreamT) {
+        const size_t bytes = fstream_smem_bytes(fp.S, SP->stage_bytes, P.narrays);
+        if (bytes <= 200 * 1024) {
+            fsp = fp;
+            fsp.bytes = bytes;
+        }
+    }
     auto configure = [&](const AggVariant& v) {
-        const SmemPlan& p = v.fused ? fp : (v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp)));
+        const SmemPlan& p =
+            v.fused ? (v.fstream ? fsp : fp) : (v.stile ? stp : (v.stream ? sp : (v.tile ? tp : cp)));
         for (int j = 0; j < P.nacc; j++) {  // fixed-point Float64 sums: the fused kernels only
             DevAcc& a = P.acc[j];
             a.fix = v.fused && fix_lo[j] != INT_MIN;
             a.fix_lo = a.fix ? fix_lo[j] : 0;
-            a.fix_scale = a.fix ? std::ldexp(1.0, -fix_lo[j]) : 0.0;
         }
         P.smem_slots = p.S;
         P.wslots = p.Sw;
@@ -3688,7 +4115,18 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     // Warp caches need combining; without a CTA table the atomic-only path
     // would send every row to HBM, so it is no candidate then either.
     std::vector<AggVariant> candidates;
-    for (int d = fusable == 2 ? 1 : 0; d >= 0 && fp.S > 0; d--)
+    // fusable: 1 the hashed probe table, 2 its dense form; bit 4 the lean
+    // (compiled) kernels apply as well.
+    const bool lean_ok = (fusable & 4) != 0;
+    const bool dense_ok = (fusable & 3) == 2;
+    for (int d = dense_ok ? 1 : 0; d >= 0 && fp.S > 0 && lean_ok; d--)
+        for (int r = 2; r <= 4; r *= 2) {
+            AggVariant f{maxacc, false, r, false};
+            f.fused = f.lean = true;
+            f.dense = d == 1;
+            candidates.push_back(f);
+        }
+    for (int d = dense_ok ? 1 : 0; d >= 0 && fp.S > 0; d--)
         for (int r = 2; r <= 8; r *= 2)
             for (int vec = 0; vec < 2; vec++) {
                 if ((vec == 0 && r == 8) || (vec == 1 && r == 2)) continue;
@@ -3698,6 +4136,12 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
                 f.dense = d == 1;
                 candidates.push_back(f);
             }
+    for (int d = dense_ok ? 1 : 0; d >= 0 && fsp.S > 0; d--) {
+        AggVariant f{maxacc, false, 1, false};
+        f.fused = f.fstream = true;
+        f.dense = d == 1;
+        candidates.push_back(f);
+    }
     if (stp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, false, true});
     if (sp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, false, true});
     if (tp.S > 0) candidates.push_back(AggVariant{maxacc, false, 1, true});
@@ -3715,21 +4159,30 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
     if (fp.S > 0) {
         chosen = AggVariant{maxacc, false, 2, false};
         chosen.fused = true;
-        chosen.dense = fusable == 2;
+        chosen.dense = dense_ok;
+        chosen.lean = lean_ok;
     }
     bool tune = false;
     if (b.force_combine >= 0 || b.force_rpt > 0) {
         if (b.force_combine >= 0) {
-            chosen.fused = b.force_combine >= 5 && b.force_combine <= 8 && fp.S > 0;
-            chosen.vec = b.force_combine >= 7;
-            chosen.dense = (b.force_combine == 5 || b.force_combine == 7) && fusable == 2;
+            chosen.fused = ((b.force_combine >= 5 && b.force_combine <= 8) && fp.S > 0) ||
+                           ((b.force_combine == 11 || b.force_combine == 12) && fsp.S > 0) ||
+                           ((b.force_combine == 13 || b.force_combine == 14) && fp.S > 0);
+            chosen.fstream = b.force_combine == 11 || b.force_combine == 12;
+            chosen.lean = (b.force_combine == 13 || b.force_combine == 14) && lean_ok;
+            chosen.vec = b.force_combine == 7 || b.force_combine == 8;
+            chosen.dense = (b.force_combine == 5 || b.force_combine == 7 || b.force_combine == 11 ||
+                            b.force_combine == 13) &&
+                           dense_ok;
             chosen.stile = b.force_combine == 4 && stp.S > 0;
             chosen.stream = b.force_combine == 3 && sp.S > 0;
             chosen.tile = b.force_combine == 2 && tp.S > 0;
             chosen.combine = b.force_combine == 1 && maxacc <= 4;
         }
         if (b.force_rpt > 0) chosen.rpt = b.force_rpt;
-        if (chosen.fused && chosen.vec) chosen.rpt = chosen.rpt <= 4 ? 4 : 8;
+        if (chosen.fstream) chosen.rpt = 1;
+        else if (chosen.lean) chosen.rpt = chosen.rpt <= 2 ? 2 : 4;
+        else if (chosen.fused && chosen.vec) chosen.rpt = chosen.rpt <= 4 ? 4 : 8;
         else if (chosen.fused) chosen.rpt = chosen.rpt <= 2 ? 2 : 4;
         else if (chosen.rpt > 2) chosen.rpt = 2;
     } else {
@@ -4139,8 +4592,11 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
     const unsigned long long key_span = (unsigned long long)jt.key_hi - (unsigned long long)jt.key_lo;
     const bool dense = jt.key_lo <= jt.key_hi && key_span < (1ull << 26) &&
                        (long long)key_span < 4 * jt.ndistinct + 4096;
+    int la0 = kLeanNone, la1 = kLeanNone;
+    const bool lean = fusable && lean_shape(plan.P, pred, pk.validity, &la0, &la1);
     return run_aggregate(s, b, plan, sample_key, group_rows, group_rows, "agg_join_kernel", streamable ? &SP : nullptr,
-                         fusable ? (dense ? 2 : 1) : 0, [&](AggProgram& P, size_t smem, const AggVariant& v) {
+                         fusable ? (dense ? 2 : 1) | (lean ? 4 : 0) : 0,
+                         [&](AggProgram& P, size_t smem, const AggVariant& v) {
                              if (n == 0) return;
                              if (v.fused) {
                                  FusedTab ft{};
@@ -4159,6 +4615,26 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
                                      ft.slots = (const FusedSlot*)fs->ptr;
                                      note_launch(), fuse_table_kernel<<<grid, 256, 0, s->stream>>>(
                                          jt, k, P.direct_lo, P.smem_slots, (FusedSlot*)fs->ptr);
+                                 }
+                                 if (v.lean) {
+                                     LeanKernel kern = lean_kernel_for(la0, la1, v.dense, v.rpt);
+                                     set_smem(kern, smem);
+                                     note_launch(), kern<<<resident_grid(b, kern, smem, (n + v.rpt - 1) / v.rpt),
+                                                           kFusedThreads, smem, s->stream>>>(
+                                         P, pred, lean_plan(P, pred), k, pk.values, pk.type, jt, ft, n);
+                                     return;
+                                 }
+                                 if (v.fstream) {
+                                     FStreamKernel kern = fstream_kernel_for(v);
+                                     set_smem(kern, smem);
+                                     int per_sm = 0;
+                                     OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStreamThreads,
+                                                                                            smem));
+                                     const long long grid =
+                                         std::min<long long>(SP.ntiles, (long long)b.sms * std::max(per_sm, 1));
+                                     note_launch(), kern<<<(unsigned)grid, kStreamThreads, smem, s->stream>>>(P, pred, SP, k,
+                                                                                                             jt, ft);
+                                     return;
                                  }
                                  FusedKernel kern = fused_kernel_for(v);
                                  set_smem(kern, smem);
