@@ -204,6 +204,13 @@ OXB_API oxb_status oxb_batch_column(const oxb_batch* batch, int32_t index, oxb_c
 OXB_API oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch,
                                int32_t index, void* values, uint8_t* validity,
                                int32_t* has_validity);
+/* GpuBackend::download (backend.rs:91-95), the whole batch in one call:
+ * column i into values[i] (length * width bytes) and, when it has a bitmap
+ * (has_validity[i] = 1), validity[i] (ceil(length / 8) bytes; may be NULL
+ * for a column without one).  The copies are queued together and the stream
+ * is synchronized once, at the end.  ncols must equal the batch's. */
+OXB_API oxb_status oxb_download(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch, int32_t ncols,
+                                void* const* values, uint8_t* const* validity, int32_t* has_validity);
 OXB_API void oxb_batch_free(oxb_batch* batch);
 
 /* ---- operators --------------------------------------------------------- */

@@ -296,6 +296,7 @@ PROTOTYPES = {
     "oxb_batch_num_columns": (C.c_int32, [_P]),
     "oxb_batch_column": (_S, [_P, C.c_int32, C.POINTER(Column)]),
     "oxb_download_column": (_S, [_P, _P, _P, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "oxb_download": (_S, [_P, _P, _P, C.c_int32, _PP, _PP, C.POINTER(C.c_int32)]),
     "oxb_batch_free": (None, [_P]),
     "oxb_filter_project": (_S, [_P, _P, C.POINTER(FilterProjectArgs), _PP]),
     "oxb_filter_project_noalloc": (

@@ -302,27 +302,38 @@ class CudaBackend:
         return DeviceBatch(h.value, schema, keep=keep)
 
     def download(self, stream: DeviceStream, batch: DeviceBatch) -> pa.RecordBatch:
-        arrays = []
-        for i, field in enumerate(batch.schema):
+        """backend.rs:91-95: every column into host memory, one call and one
+        stream synchronization (oxb_download)."""
+        ncols = len(batch.schema)
+        vals, bits, lens = [], [], []
+        for i in range(ncols):
             c = batch.column(i)
             n = c.length
-            dtype = columns.numpy_dtype(c.type)
-            values = np.empty(n * (c.dim if c.type == _abi.TYPE_VECTOR_F32 else 1), dtype=dtype)
-            validity = np.empty((n + 7) // 8, dtype=np.uint8)
-            has = C.c_int32(0)
-            _abi.check(
-                _L().oxb_download_column(
-                    self.handle,
-                    stream.handle,
-                    batch.handle,
-                    i,
-                    values.ctypes.data if n else None,
-                    validity.ctypes.data if n else None,
-                    C.byref(has),
-                )
-            )
-            arrays.append(columns.rebuild(field.type, values, validity if has.value and n else None, n))
+            lens.append(n)
+            vals.append(np.empty(n * (c.dim if c.type == _abi.TYPE_VECTOR_F32 else 1), dtype=columns.numpy_dtype(c.type)))
+            bits.append(np.empty((n + 7) // 8, dtype=np.uint8))
+        k = max(1, ncols)
+        vp = (C.c_void_p * k)(*[v.ctypes.data if v.size else None for v in vals])
+        bp = (C.c_void_p * k)(*[b.ctypes.data if b.size else None for b in bits])
+        has = (C.c_int32 * k)()
+        _abi.check(_L().oxb_download(self.handle, stream.handle, batch.handle, ncols, vp, bp, has))
+        arrays = []
+        for i, field in enumerate(batch.schema):
+            n = lens[i]
+            arrays.append(columns.rebuild(field.type, vals[i], bits[i] if has[i] and n else None, n))
         return pa.RecordBatch.from_arrays(arrays, schema=batch.schema)
+
+    def download_column(self, stream: DeviceStream, batch: DeviceBatch, i: int) -> pa.Array:
+        """One column (oxb_download_column)."""
+        c = batch.column(i)
+        n = c.length
+        values = np.empty(n * (c.dim if c.type == _abi.TYPE_VECTOR_F32 else 1), dtype=columns.numpy_dtype(c.type))
+        validity = np.empty((n + 7) // 8, dtype=np.uint8)
+        has = C.c_int32(0)
+        _abi.check(_L().oxb_download_column(self.handle, stream.handle, batch.handle, i,
+                                            values.ctypes.data if n else None, validity.ctypes.data if n else None,
+                                            C.byref(has)))
+        return columns.rebuild(batch.schema.field(i).type, values, validity if has.value and n else None, n)
 
     # --- operators ----------------------------------------------------------
     def filter_project(

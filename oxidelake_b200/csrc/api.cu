@@ -495,6 +495,34 @@ oxb_status oxb_download_column(oxb_backend* backend, oxb_stream* stream, const o
     });
 }
 
+oxb_status oxb_download(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch, int32_t ncols,
+                        void* const* values, uint8_t* const* validity, int32_t* has_validity) {
+    return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        const StreamRef& s = stream_of(stream);
+        if (!batch) fail(OXB_PLAN, "batch is null");
+        if (ncols != (int32_t)batch->cols.size())
+            fail(OXB_PLAN, "the batch has " + std::to_string(batch->cols.size()) + " columns, not " +
+                               std::to_string(ncols));
+        if (ncols > 0 && (!values || !has_validity)) fail(OXB_PLAN, "null output arrays");
+        for (int i = 0; i < ncols; i++) {
+            const Column& c = batch->cols[i];
+            has_validity[i] = c.validity ? 1 : 0;
+            if (c.length == 0) continue;
+            if (!values[i]) fail(OXB_PLAN, "values buffer of column " + std::to_string(i) + " is null");
+            download_bytes(backend->b, s, values[i], c.values, (size_t)c.length * c.width());
+            st.bytes_d2h += (uint64_t)c.length * c.width();
+            if (c.validity && validity && validity[i]) {
+                OXB_CUDA(cudaMemcpyAsync(validity[i], c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
+                                         s->stream));
+                st.bytes_d2h += ((uint64_t)c.length + 7) / 8;
+            }
+        }
+        OXB_CUDA(cudaStreamSynchronize(s->stream));
+        st.rows_in = st.rows_out = (uint64_t)batch->rows;
+    });
+}
+
 void oxb_batch_free(oxb_batch* batch) { delete batch; }
 
 oxb_status oxb_filter_project(oxb_backend* backend, oxb_stream* stream, const oxb_filter_project_args* args,

@@ -117,3 +117,37 @@ def test_admission_refuses_what_never_fits(backend, stream, resident):
         srv.submit_topk(resident["ix"], resident["vdev"], None, q, 10, DistanceMetric.L2)
     assert srv.stats()["rejected"] == 1
     srv.close()
+
+
+def test_admission_defers_until_memory_frees(backend, stream, resident):
+    """A budget with room for two requests' device memory and ten requests
+    submitted at once: the server runs at most two at a time (the others wait
+    in the queue until memory frees, with workers idle), every request
+    completes, and each result equals its direct call."""
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(10):  # distinct WHERE literals: no two share a scan
+        reqs.append((rng.standard_normal(resident["dim"]).astype(np.float32), int(rng.choice([5, 10])), 100 + 83 * i))
+    # One request alone: the server's estimate of its device memory.
+    srv = backend.server(workers=1)
+    q, k, lit = reqs[0]
+    srv.wait_topk(srv.submit_topk(resident["ix"], resident["vdev"], compare(0, Cmp.Lt, Literal.int64(lit)), q, k,
+                                  DistanceMetric.L2), k)
+    one = srv.stats()["peak_bytes"]
+    srv.close()
+    assert one > 0
+    budget = int(2.5 * one)
+    srv = backend.server(memory_budget=budget, workers=6, max_batch=256)
+    tickets = [srv.submit_topk(resident["ix"], resident["vdev"], compare(0, Cmp.Lt, Literal.int64(lit)), q, k,
+                               DistanceMetric.L2) for q, k, lit in reqs]
+    got = [srv.wait_topk(t, k) for t, (_, k, _) in zip(tickets, reqs)]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 10 and st["rejected"] == 0 and st["dispatches"] == 10
+    assert st["peak_bytes"] <= budget and st["peak_bytes"] < 3 * one
+    for (q, k, lit), (ids, dist, _) in zip(reqs, got):
+        want_ids, want_dist, _ = backend.vector_topk(stream, resident["ix"], resident["vdev"],
+                                                     compare(0, Cmp.Lt, Literal.int64(lit)), q[None, :], k,
+                                                     DistanceMetric.L2)
+        assert (ids == want_ids[0]).all()
+        assert (dist.view(np.uint32) == want_dist[0].view(np.uint32)).all()
