@@ -3681,6 +3681,137 @@ __global__ void __launch_bounds__(kThreads) part_fold_kernel(const __grid_consta
     }
 }
 
+// The fold for 16-byte records (one Int32 column) whose accumulators are
+// among COUNT, SUM, MIN and MAX of that column: the program fixed at compile
+// time (OPS: bit 0 COUNT, 1 SUM, 2 MIN, 3 MAX), kFoldRows records a thread
+// loaded together and folded straight from their registers, no interpreter.
+// part_fold_kernel folds every other shape.
+struct CompactOps {
+    int count_arr, sum_arr, min_arr, max_arr;
+};
+
+template <int OPS>
+__global__ void __launch_bounds__(kThreads) part_fold_compact_kernel(const __grid_constant__ AggProgram P,
+                                                                     const __grid_constant__ PartPlan pp,
+                                                                     const __grid_constant__ CompactOps ops,
+                                                                     const unsigned long long* __restrict__ offs) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int S = kPartSlots;
+    long long* keys = (long long*)smem;
+    unsigned int* rows = (unsigned int*)(keys + S);
+    unsigned long long* tab = (unsigned long long*)(rows + S) - S;  // array a at tab + a * S
+    __shared__ int fill;
+    unsigned narrow = 0;  // MIN/MAX of the Int32 column live in their arrays' low words
+    if (OPS & 4) narrow |= 1u << ops.min_arr;
+    if (OPS & 8) narrow |= 1u << ops.max_arr;
+    for (int part = blockIdx.x; part < pp.nparts; part += gridDim.x) {
+        for (int i = threadIdx.x; i < S; i += blockDim.x) {
+            keys[i] = kEmptyKey;
+            rows[i] = 0;
+        }
+        for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) {
+            const int a = 1 + i / S;
+            tab[S + i] = (narrow >> a) & 1u ? (P.init[a] == kInitMax ? 0x7fffffffull : 0x80000000ull)
+                                            : init_value(P.init[a]);
+        }
+        if (threadIdx.x == 0) fill = 0;
+        __syncthreads();
+        const unsigned long long lo = offs[(long long)part * pp.fstride], hi = offs[(long long)(part + 1) * pp.fstride];
+        for (unsigned long long b0 = lo + threadIdx.x; b0 < hi; b0 += (unsigned long long)kThreads * kFoldRows) {
+            uint4 rec[kFoldRows];
+#pragma unroll
+            for (int j = 0; j < kFoldRows; j++) {
+                const unsigned long long i = b0 + (unsigned long long)j * kThreads;
+                rec[j] = i < hi ? __ldcs(pp.recs2 + i) : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int j = 0; j < kFoldRows; j++) {
+                if (b0 + (unsigned long long)j * kThreads >= hi) break;
+                const long long key = (long long)((unsigned long long)rec[j].x | (unsigned long long)rec[j].y << 32);
+                int slot = -1;
+                unsigned int h = (unsigned int)(fmix64((unsigned long long)key) & (unsigned)(S - 1));
+                for (int q = 0; q < 64; q++) {
+                    const long long k = ((volatile long long*)keys)[h];
+                    if (k == key) {
+                        slot = (int)h;
+                        break;
+                    }
+                    if (k == kEmptyKey) {
+                        if (*(volatile int*)&fill >= S * 3 / 4) break;
+                        const unsigned long long old = atomicCAS((unsigned long long*)&keys[h],
+                                                                 (unsigned long long)kEmptyKey, (unsigned long long)key);
+                        if (old == (unsigned long long)kEmptyKey) {
+                            atomicAdd(&fill, 1);
+                            slot = (int)h;
+                            break;
+                        }
+                        if ((long long)old == key) {
+                            slot = (int)h;
+                            break;
+                        }
+                    }
+                    h = (h + 1u) & (unsigned)(S - 1);
+                }
+                if (slot < 0) {
+                    part_rec_to_hbm<4, 1>(P, pp, rec[j], rec[j], rec[j]);
+                    continue;
+                }
+                atomicAdd(&rows[slot], 1u);
+                if (!(rec[j].w & 1u)) continue;  // a NULL value: the row counts, nothing else
+                const int x = (int)rec[j].z;
+                if (OPS & 1) atomicAdd((unsigned*)(tab + ops.count_arr * S + slot), 1u);
+                if (OPS & 2) {
+                    // the Int64 sum as a 32-bit add and its carry (x sign-extended)
+                    unsigned* w32 = (unsigned*)(tab + ops.sum_arr * S + slot);
+                    const unsigned vlo = (unsigned)x, vhi = x < 0 ? 0xffffffffu : 0u;
+                    const unsigned old = vlo ? atomicAdd(w32, vlo) : 0u;
+                    const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
+                    if (up) atomicAdd(w32 + 1, up);
+                }
+                if (OPS & 4) atomicMin((int*)(tab + ops.min_arr * S + slot), x);
+                if (OPS & 8) atomicMax((int*)(tab + ops.max_arr * S + slot), x);
+            }
+        }
+        __syncthreads();
+        fused_flush(P, rows, tab, S, keys, narrow);
+        __syncthreads();
+    }
+}
+
+using CompactFold = void (*)(const AggProgram, const PartPlan, const CompactOps, const unsigned long long*);
+CompactFold compact_fold_for(int ops) {
+    switch (ops) {
+#define OXB_CF(m) \
+    case m: return part_fold_compact_kernel<m>;
+        OXB_CF(1) OXB_CF(2) OXB_CF(3) OXB_CF(4) OXB_CF(5) OXB_CF(6) OXB_CF(7) OXB_CF(8) OXB_CF(9) OXB_CF(10)
+        OXB_CF(11) OXB_CF(12) OXB_CF(13) OXB_CF(14) OXB_CF(15)
+#undef OXB_CF
+        default: return nullptr;
+    }
+}
+
+// The compact fold's program for P (records of one Int32 column), or 0 when
+// an accumulator is outside it.
+int compact_ops_of(const AggProgram& P, CompactOps* ops) {
+    int m = 0;
+    *ops = CompactOps{0, 0, 0, 0};
+    for (int q = 0; q < P.nacc; q++) {
+        const DevAcc& a = P.acc[q];
+        if (a.in_type != kInt32) return 0;
+        int bit;
+        switch (a.kind) {
+            case kAccCount: bit = 1; ops->count_arr = a.arr; break;
+            case kAccSumInt: bit = 2; ops->sum_arr = a.arr; break;
+            case kAccMin: bit = 4; ops->min_arr = a.arr; break;
+            case kAccMax: bit = 8; ops->max_arr = a.arr; break;
+            default: return 0;
+        }
+        if (m & bit) return 0;
+        m |= bit;
+    }
+    return m;
+}
+
 size_t part_fold_smem(int narrays) { return (size_t)kPartSlots * (8 + 4 + 8 * (narrays - 1)); }
 
 int maxacc_for(int nacc) { return nacc <= 2 ? 2 : (nacc <= 4 ? 4 : kMaxAccs); }
@@ -4465,7 +4596,16 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
                 note_launch(), psplit2<<<(unsigned)grid2, kThreads, 0, s->stream>>>(pp, offs.get(), tstart.get(),
                                                                                    queue2.get(), cursor2.get());
             }
-            note_launch(), pfold<<<(unsigned)fgrid, kThreads, fsmem, s->stream>>>(P, pp, offs.get());
+            CompactOps cops;
+            const int cmask = units == 1 ? compact_ops_of(P, &cops) : 0;
+            if (cmask) {
+                CompactFold cf = compact_fold_for(cmask);
+                set_smem(cf, fsmem);
+                note_launch(), cf<<<(unsigned)resident_grid(b, cf, fsmem, (long long)pp.nparts * kThreads), kThreads, fsmem,
+                                    s->stream>>>(P, pp, cops, offs.get());
+            } else {
+                note_launch(), pfold<<<(unsigned)fgrid, kThreads, fsmem, s->stream>>>(P, pp, offs.get());
+            }
             timer.end();
             OXB_CUDA(cudaGetLastError());
         } else {
