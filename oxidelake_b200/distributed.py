@@ -131,3 +131,81 @@ def exchange_and_merge(local: pa.RecordBatch, partial, finish, names, group=None
     dist.all_gather_object(gathered, payload, group=group)
     parts = [pa.ipc.open_stream(b).read_next_batch() for b in gathered]
     return merge_partials(parts, partial, finish, names)
+
+
+# ---- top-k over row shards ------------------------------------------------
+
+def _order_key(dist: np.ndarray) -> np.ndarray:
+    """FP32 distances as signed integers in IEEE totalOrder (NaN last), the
+    order of ORDER BY distance."""
+    k = dist.view(np.int32).astype(np.int64)
+    return np.where(k < 0, k ^ 0x7FFFFFFF, k)
+
+
+def merge_topk(ids: Sequence[np.ndarray], dist: Sequence[np.ndarray], k: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Per query, the k best of several ranks' candidate lists ([Q, m_r] ids
+    with global row numbers, -1 padding) by (distance in totalOrder, row id):
+    the order one pass over the whole table gives.  Each rank's list is its
+    shard's exact top-k, and the global top-k is drawn from their union."""
+    cat_i = np.concatenate(list(ids), axis=1)
+    cat_d = np.concatenate(list(dist), axis=1)
+    pad = cat_i < 0
+    key = _order_key(cat_d)
+    key = np.where(pad, np.iinfo(np.int64).max, key)
+    rid = np.where(pad, np.iinfo(np.int64).max, cat_i)
+    order = np.lexsort((rid, key), axis=1)[:, :k]
+    out_i = np.take_along_axis(cat_i, order, axis=1)
+    out_d = np.take_along_axis(cat_d, order, axis=1)
+    return out_i, out_d
+
+
+def exchange_topk(local_ids: np.ndarray, local_dist: np.ndarray, row_offset: int, k: int,
+                  group=None) -> Tuple[np.ndarray, np.ndarray]:
+    """The top-k of a table sharded by rows over the ranks: each rank's exact
+    local top-k (shard row numbers) made global by its shard's first row,
+    gathered once, and merged; every rank gets the result."""
+    import torch.distributed as dist
+
+    gids = np.where(local_ids >= 0, local_ids + row_offset, -1)
+    gathered: List[Tuple[np.ndarray, np.ndarray]] = [None] * dist.get_world_size(group)
+    dist.all_gather_object(gathered, (gids, local_dist), group=group)
+    return merge_topk([g[0] for g in gathered], [g[1] for g in gathered], k)
+
+
+# ---- many groups: a hash-partitioned exchange -----------------------------
+
+def key_owner(keys: pa.Array, world: int) -> np.ndarray:
+    """The rank that merges each group: a hash of the key (the NULL group to
+    rank 0), the same on every rank."""
+    valid = keys.is_valid().to_numpy(zero_copy_only=False)
+    k = keys.fill_null(0).to_numpy(zero_copy_only=False).astype(np.int64).view(np.uint64)
+    with np.errstate(over="ignore"):
+        z = k * np.uint64(0x9E3779B97F4A7C15)
+        z ^= z >> np.uint64(29)
+    return np.where(valid, (z % np.uint64(world)).astype(np.int64), 0)
+
+
+def exchange_partitioned(local: pa.RecordBatch, partial, finish, names, group=None) -> pa.RecordBatch:
+    """The exchange for many groups: each rank sends every partial group to
+    the rank its key hashes to (an all-to-all of Arrow IPC pieces), merges
+    the groups it owns, and returns them (sorted by key, NULL last).  The
+    ranks' results are disjoint; together they are the query's result.  A
+    rank holds only its share of the groups, where exchange_and_merge
+    gathers all of them everywhere."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    owner = key_owner(local.column(0), world)
+    pieces = []
+    for r in range(world):
+        part = local.filter(pa.array(owner == r))
+        sink = pa.BufferOutputStream()
+        with pa.ipc.new_stream(sink, local.schema) as w:
+            w.write_batch(part)
+        pieces.append(sink.getvalue().to_pybytes())
+    # all-to-all through one gather of every rank's pieces (gloo and NCCL both carry it)
+    gathered: List[List[bytes]] = [None] * world
+    dist.all_gather_object(gathered, pieces, group=group)
+    me = dist.get_rank(group)
+    mine = [pa.ipc.open_stream(g[me]).read_next_batch() for g in gathered]
+    return merge_partials(mine, partial, finish, names)
