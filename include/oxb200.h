@@ -455,6 +455,16 @@ typedef struct oxb_join_aggregate_args {
 } oxb_join_aggregate_args;
 OXB_API oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream,
                               const oxb_join_aggregate_args* args, oxb_batch** out);
+/* Several oxb_join_aggregate requests in one launch, where they differ only
+ * in their probe batch (columns of the same types) and their WHERE literals:
+ * the rows of every request are tiles of one work queue, and each request
+ * folds into its own table.  out[i] is the result of args[i], equal to its
+ * own oxb_join_aggregate call's; requests that cannot share the launch
+ * (another shape, a column with a validity bitmap, more than two inputs)
+ * run one at a time.  No reference counterpart: the reference runs one query
+ * at a time (compute/src/operator.rs). */
+OXB_API oxb_status oxb_join_aggregate_many(oxb_backend* backend, oxb_stream* stream,
+                                           const oxb_join_aggregate_args* args, int32_t n, oxb_batch** out);
 
 /* ---- serving (the request loop the reference lacks; its queries run one at
  *      a time through compute/src/operator.rs) ---------------------------- */
@@ -463,7 +473,8 @@ OXB_API oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream,
  * worker threads (one CUDA stream each) run admitted work concurrently, and
  * top-k requests that queue while others run are stacked into one scan when
  * they share the index, batch, metric and WHERE except for their own query
- * vector, k and per-query literal.  Work is admitted while the estimated
+ * vector, k and per-query literal; join-aggregate requests of one shape
+ * (oxb_join_aggregate_many) share one launch the same way.  Work is admitted while the estimated
  * device memory of what runs stays within the budget; a request that alone
  * exceeds it is refused with OXB_OOM_ADMISSION.  Results equal the direct
  * calls'.  The resident batches, indexes and join tables outlive the server. */
@@ -504,7 +515,7 @@ typedef struct oxb_server_stats {
     int64_t completed;
     int64_t rejected;
     int64_t dispatches;      /* work items run */
-    int64_t batched_queries; /* top-k requests that shared a scan */
+    int64_t batched_queries; /* requests that shared a launch: top-k scans, join-aggregate folds */
     int64_t peak_bytes;      /* largest admitted estimate in flight */
     double p50_us, p99_us;   /* submit-to-result latency */
     double qps;              /* completed / (last completion - first submit) */

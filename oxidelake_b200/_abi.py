@@ -314,6 +314,7 @@ PROTOTYPES = {
     "oxb_hash_join": (_S, [_P, _P, C.POINTER(HashJoinArgs), _PP]),
     "oxb_aggregate": (_S, [_P, _P, C.POINTER(AggregateArgs), _PP]),
     "oxb_join_aggregate": (_S, [_P, _P, C.POINTER(JoinAggregateArgs), _PP]),
+    "oxb_join_aggregate_many": (_S, [_P, _P, C.POINTER(JoinAggregateArgs), C.c_int32, _PP]),
     "oxb_vector_distance": (_S, [_P, _P, C.POINTER(VectorDistanceArgs), _PP]),
     "oxb_aggregate_batches": (_S, [_P, _P, C.POINTER(AggregateBatchesArgs), _PP]),
     "oxb_server_create": (_S, [_P, C.POINTER(ServerConfig), _PP]),

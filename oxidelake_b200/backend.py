@@ -512,6 +512,16 @@ class CudaBackend:
         _abi.check(_L().oxb_join_aggregate(self.handle, stream.handle, C.byref(a), C.byref(h)))
         return DeviceBatch(h.value, schema)
 
+    def join_aggregate_many(self, stream: DeviceStream, requests) -> List[DeviceBatch]:
+        """Several join_aggregate requests, each (probe, probe_key, table,
+        predicate, group, aggregates), in one launch where they share a shape
+        (oxb_join_aggregate_many); results in request order."""
+        built = [_join_aggregate_args(*r) for r in requests]
+        arr = (_abi.JoinAggregateArgs * max(1, len(built)))(*[x[0] for x in built])
+        outs = (C.c_void_p * max(1, len(built)))()
+        _abi.check(_L().oxb_join_aggregate_many(self.handle, stream.handle, arr, len(built), outs))
+        return [DeviceBatch(outs[i], built[i][1]) for i in range(len(built))]
+
     def server(self, memory_budget: int = 0, workers: int = 0, max_batch: int = 0) -> "Server":
         """A serving loop over resident tables (oxb_server_create)."""
         return Server(self, memory_budget, workers, max_batch)

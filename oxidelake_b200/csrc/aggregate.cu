@@ -2483,6 +2483,93 @@ __device__ __forceinline__ void lean_fold(const AggProgram& P, const LeanPlan& L
     }
 }
 
+// One request's columns as the lean kernels read them: the probe key, up to
+// two WHERE columns with their literals (the comparisons are the plan's),
+// and up to two sum inputs.
+struct LeanCols {
+    const void* pk;
+    const void* leaf[2];
+    long long lit[2];
+    const void* acc[2];
+};
+
+// Rows base + r * kFusedThreads (r < RPT, below n) of one request, folded
+// into the CTA table: every load first, then the lookups, then the folds.
+template <int A0, int A1, bool DENSE, int RPT>
+__device__ __forceinline__ void lean_rows(const AggProgram& P, const DevPredicate& pred, const LeanPlan& L,
+                                          const LeanCols& C, const AggKey& gkey, int pk_type, const JoinTableDev& jt,
+                                          const FusedTab& ft, long long base, long long n, unsigned int* rows,
+                                          unsigned long long* tab, int S, unsigned long long keep) {
+    const unsigned int cap_mask = jt.capacity - 1u;
+    long long key[RPT], v0[RPT], v1[RPT], lv0[RPT], lv1[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        const long long i = base + r * (long long)kFusedThreads;
+        const bool in = i < n;
+        key[r] = !in ? 0 : pk_type == kInt64 ? __ldcs((const long long*)C.pk + i) : (long long)__ldcs((const int*)C.pk + i);
+        lv0[r] = lv1[r] = v0[r] = v1[r] = 0;
+        if (!in) continue;
+        if (L.nleaves > 0)
+            lv0[r] = L.leaf_width[0] == 8 ? __ldcs((const long long*)C.leaf[0] + i) : (long long)__ldcs((const int*)C.leaf[0] + i);
+        if (L.nleaves > 1)
+            lv1[r] = L.leaf_width[1] == 8 ? __ldcs((const long long*)C.leaf[1] + i) : (long long)__ldcs((const int*)C.leaf[1] + i);
+        if (A0 != kLeanNone) v0[r] = lean_load<A0>(C.acc[0], i);
+        if (A1 != kLeanNone) v1[r] = lean_load<A1>(C.acc[1], i);
+    }
+    int cs[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        cs[r] = kDenseNone;
+        const long long i = base + r * (long long)kFusedThreads;
+        if (i >= n) continue;
+        if (L.nleaves > 0) {
+            const long long a = L.leaf_f64[0] ? filter_order_key(__longlong_as_double(lv0[r])) : lv0[r];
+            if (!cmp_holds(pred.leaves[0].op, a, C.lit[0])) continue;
+        }
+        if (L.nleaves > 1) {
+            const long long a = L.leaf_f64[1] ? filter_order_key(__longlong_as_double(lv1[r])) : lv1[r];
+            if (!cmp_holds(pred.leaves[1].op, a, C.lit[1])) continue;
+        }
+        if (key[r] == kEmptyKey) {
+            if (jt.special_count) cs[r] = kDenseSlow;
+            continue;
+        }
+        if (DENSE) {
+            const unsigned long long d = (unsigned long long)key[r] - (unsigned long long)ft.dense_lo;
+            if (d < ft.dense_n) cs[r] = (int)ld_keep_u32(ft.dense + d, keep);
+        } else {
+            unsigned int sl = (unsigned int)(fmix64((unsigned long long)key[r]) & cap_mask);
+            for (unsigned int q = 0; q <= cap_mask; q++) {
+                const int4 e = ld_keep_v4(&ft.slots[sl], keep);
+                const long long kk = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
+                if (kk == key[r]) {
+                    cs[r] = ((unsigned int)e.w == 1u && e.z >= 0) ? e.z : kDenseSlow;
+                    break;
+                }
+                if (kk == kEmptyKey) break;
+                sl = (sl + 1u) & cap_mask;
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        if (cs[r] >= 0) {
+            atomicAdd(&rows[cs[r]], 1u);
+            lean_fold<A0>(P, L, 0, tab, S, cs[r], v0[r]);
+            lean_fold<A1>(P, L, 1, tab, S, cs[r], v1[r]);
+        } else if (cs[r] == kDenseSlow) {
+            const long long i = base + r * (long long)kFusedThreads;
+            fused_slow(P, gkey, jt, key[r] == kEmptyKey ? -1 : jt_find_slot(jt, key[r]), i);
+        }
+    }
+}
+
+__device__ __forceinline__ void fused_table_init(const AggProgram& P, unsigned int* rows, unsigned long long* tab,
+                                                 int S) {
+    for (int i = threadIdx.x; i < S; i += blockDim.x) rows[i] = 0;
+    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) tab[S + i] = init_value(P.init[1 + i / S]);
+}
+
 template <int A0, int A1, bool DENSE, int RPT>
 __global__ void __launch_bounds__(kFusedThreads, 4) agg_lean_join_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ LeanPlan L,
@@ -2492,79 +2579,96 @@ __global__ void __launch_bounds__(kFusedThreads, 4) agg_lean_join_kernel(
     const int S = P.smem_slots;
     unsigned int* rows = (unsigned int*)smem;
     unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) rows[i] = 0;
-    for (int i = threadIdx.x; i < S * (P.narrays - 1); i += blockDim.x) tab[S + i] = init_value(P.init[1 + i / S]);
+    fused_table_init(P, rows, tab, S);
     __syncthreads();
-    const unsigned long long keep = policy_evict_last();
-    const unsigned int cap_mask = jt.capacity - 1u;
-    const long long step = (long long)gridDim.x * blockDim.x * RPT;
-    for (long long base = blockIdx.x * (long long)blockDim.x * RPT + threadIdx.x; base < n; base += step) {
-        long long key[RPT], v0[RPT], v1[RPT], lv0[RPT], lv1[RPT];
-#pragma unroll
-        for (int r = 0; r < RPT; r++) {
-            const long long i = base + r * (long long)kFusedThreads;
-            const bool in = i < n;
-            key[r] = !in ? 0 : pk_type == kInt64 ? __ldcs((const long long*)pk + i) : (long long)__ldcs((const int*)pk + i);
-            lv0[r] = lv1[r] = v0[r] = v1[r] = 0;
-            if (!in) continue;
-            if (L.nleaves > 0)
-                lv0[r] = L.leaf_width[0] == 8 ? __ldcs((const long long*)pred.leaves[0].values + i)
-                                              : (long long)__ldcs((const int*)pred.leaves[0].values + i);
-            if (L.nleaves > 1)
-                lv1[r] = L.leaf_width[1] == 8 ? __ldcs((const long long*)pred.leaves[1].values + i)
-                                              : (long long)__ldcs((const int*)pred.leaves[1].values + i);
-            if (A0 != kLeanNone) v0[r] = lean_load<A0>(L.acc_values[0], i);
-            if (A1 != kLeanNone) v1[r] = lean_load<A1>(L.acc_values[1], i);
-        }
-        int cs[RPT];
-#pragma unroll
-        for (int r = 0; r < RPT; r++) {
-            cs[r] = kDenseNone;
-            const long long i = base + r * (long long)kFusedThreads;
-            if (i >= n) continue;
-            if (L.nleaves > 0) {
-                const long long a = L.leaf_f64[0] ? filter_order_key(__longlong_as_double(lv0[r])) : lv0[r];
-                if (!cmp_holds(pred.leaves[0].op, a, pred.leaves[0].lit)) continue;
-            }
-            if (L.nleaves > 1) {
-                const long long a = L.leaf_f64[1] ? filter_order_key(__longlong_as_double(lv1[r])) : lv1[r];
-                if (!cmp_holds(pred.leaves[1].op, a, pred.leaves[1].lit)) continue;
-            }
-            if (key[r] == kEmptyKey) {
-                if (jt.special_count) cs[r] = kDenseSlow;
-                continue;
-            }
-            if (DENSE) {
-                const unsigned long long d = (unsigned long long)key[r] - (unsigned long long)ft.dense_lo;
-                if (d < ft.dense_n) cs[r] = (int)ld_keep_u32(ft.dense + d, keep);
-            } else {
-                unsigned int sl = (unsigned int)(fmix64((unsigned long long)key[r]) & cap_mask);
-                for (unsigned int q = 0; q <= cap_mask; q++) {
-                    const int4 e = ld_keep_v4(&ft.slots[sl], keep);
-                    const long long kk = ((long long)(unsigned int)e.y << 32) | (unsigned int)e.x;
-                    if (kk == key[r]) {
-                        cs[r] = ((unsigned int)e.w == 1u && e.z >= 0) ? e.z : kDenseSlow;
-                        break;
-                    }
-                    if (kk == kEmptyKey) break;
-                    sl = (sl + 1u) & cap_mask;
-                }
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < RPT; r++) {
-            if (cs[r] >= 0) {
-                atomicAdd(&rows[cs[r]], 1u);
-                lean_fold<A0>(P, L, 0, tab, S, cs[r], v0[r]);
-                lean_fold<A1>(P, L, 1, tab, S, cs[r], v1[r]);
-            } else if (cs[r] == kDenseSlow) {
-                const long long i = base + r * (long long)kFusedThreads;
-                fused_slow(P, gkey, jt, key[r] == kEmptyKey ? -1 : jt_find_slot(jt, key[r]), i);
-            }
-        }
+    LeanCols C;
+    C.pk = pk;
+    for (int l = 0; l < 2; l++) {
+        C.leaf[l] = l < L.nleaves ? pred.leaves[l].values : nullptr;
+        C.lit[l] = l < L.nleaves ? pred.leaves[l].lit : 0;
+        C.acc[l] = L.acc_values[l];
     }
+    const unsigned long long keep = policy_evict_last();
+    const long long step = (long long)gridDim.x * blockDim.x * RPT;
+    for (long long base = blockIdx.x * (long long)blockDim.x * RPT + threadIdx.x; base < n; base += step)
+        lean_rows<A0, A1, DENSE, RPT>(P, pred, L, C, gkey, pk_type, jt, ft, base, n, rows, tab, S, keep);
     __syncthreads();
     fused_flush(P, rows, tab, S);
+}
+
+// ---- many join-aggregate requests in one launch ----------------------------
+//
+// Requests that differ only in their probe batch and WHERE literals (the
+// same join table, group key, aggregates and comparisons) share one launch:
+// their rows are cut into kLeanTile-row tiles laid end to end in one work
+// queue, a CTA folds the tiles it takes into its CTA table, and when the
+// next tile belongs to another request it flushes the table into that
+// request's own HBM table first.  Each request's result equals its own call's.
+
+constexpr long long kLeanTile = 8192;
+
+struct LeanReq {
+    LeanCols cols;
+    long long n;
+    long long tile0;  // the request's first tile in the queue
+    long long* keys;  // its HBM table
+    unsigned long long* arr;
+    unsigned* status;
+};
+
+template <int A0, int A1, bool DENSE, int RPT>
+__global__ void __launch_bounds__(kFusedThreads, 4) agg_lean_multi_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DevPredicate pred, const __grid_constant__ LeanPlan L,
+    const __grid_constant__ AggKey gkey, int pk_type, const __grid_constant__ JoinTableDev jt,
+    const __grid_constant__ FusedTab ft, const LeanReq* __restrict__ reqs, int nreq, long long ntiles,
+    unsigned long long* __restrict__ queue) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ AggProgram Ps;  // P with the current request's HBM table
+    __shared__ long long s_tile;
+    const int S = P.smem_slots;
+    unsigned int* rows = (unsigned int*)smem;
+    unsigned long long* tab = (unsigned long long*)(smem + fused_counts_bytes(S)) - S;
+    for (int i = threadIdx.x; i < (int)(sizeof(AggProgram) / 4); i += blockDim.x)
+        ((unsigned*)&Ps)[i] = ((const unsigned*)&P)[i];
+    const unsigned long long keep = policy_evict_last();
+    int cur = -1;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const long long t = s_tile;
+        if (t >= ntiles) break;
+        int lo = 0, hi = nreq - 1;  // the last request whose first tile is <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (reqs[mid].tile0 <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        if (lo != cur) {
+            if (cur >= 0) {
+                fused_flush(Ps, rows, tab, S);
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                Ps.keys = reqs[lo].keys;
+                Ps.arr = reqs[lo].arr;
+                Ps.status = reqs[lo].status;
+                // the slow paths read a row's inputs through the program
+                for (int j = 0; j < Ps.nacc && j < 2; j++) Ps.acc[j].values = reqs[lo].cols.acc[j];
+            }
+            fused_table_init(Ps, rows, tab, S);
+            __syncthreads();
+            cur = lo;
+        }
+        const LeanReq& q = reqs[lo];
+        const long long t0 = (t - q.tile0) * kLeanTile;
+        const long long end = t0 + kLeanTile < q.n ? t0 + kLeanTile : q.n;
+        const LeanCols C = q.cols;
+        for (long long base = t0 + threadIdx.x; base < end; base += (long long)kFusedThreads * RPT)
+            lean_rows<A0, A1, DENSE, RPT>(Ps, pred, L, C, gkey, pk_type, jt, ft, base, end, rows, tab, S, keep);
+    }
+    __syncthreads();
+    if (cur >= 0) fused_flush(Ps, rows, tab, S);
 }
 
 __global__ void agg_init_kernel(const __grid_constant__ AggProgram P) {
@@ -3956,6 +4060,34 @@ LeanKernel lean_kernel_for(int a0, int a1, bool dense, int rpt) {
     }
 }
 
+using LeanMultiKernel = void (*)(const AggProgram, const DevPredicate, const LeanPlan, const AggKey, int,
+                                 const JoinTableDev, const FusedTab, const LeanReq*, int, long long,
+                                 unsigned long long*);
+
+template <int A0, int A1>
+LeanMultiKernel lean_multi_pick(bool dense) {
+    return dense ? agg_lean_multi_kernel<A0, A1, true, 2> : agg_lean_multi_kernel<A0, A1, false, 2>;
+}
+
+template <int A0>
+LeanMultiKernel lean_multi_a1(int a1, bool dense) {
+    switch (a1) {
+        case kLeanSumI32: return lean_multi_pick<A0, kLeanSumI32>(dense);
+        case kLeanSumI64: return lean_multi_pick<A0, kLeanSumI64>(dense);
+        case kLeanSumF64: return lean_multi_pick<A0, kLeanSumF64>(dense);
+        default: return lean_multi_pick<A0, kLeanNone>(dense);
+    }
+}
+
+LeanMultiKernel lean_multi_kernel_for(int a0, int a1, bool dense) {
+    switch (a0) {
+        case kLeanSumI32: return lean_multi_a1<kLeanSumI32>(a1, dense);
+        case kLeanSumI64: return lean_multi_a1<kLeanSumI64>(a1, dense);
+        case kLeanSumF64: return lean_multi_a1<kLeanSumF64>(a1, dense);
+        default: return lean_multi_pick<kLeanNone, kLeanNone>(dense);
+    }
+}
+
 std::string variant_name(const char* base, const AggVariant& v) {
     if (v.fused && v.lean)
         return std::string(base) + "<" + std::to_string(v.maxacc) + (v.dense ? ",fused-dense," : ",fused,") + "lean," +
@@ -4806,5 +4938,244 @@ oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_a
                                                    s->stream>>>(P, pred, k, pk.values, pk.validity, pk.type, jt, n);
                          });
 }
+
+// True when two join-aggregate requests differ at most in their probe batch
+// (same column types) and their WHERE literals.
+bool same_join_shape(const oxb_join_aggregate_args& a, const oxb_join_aggregate_args& z) {
+    if (a.table != z.table || a.build != z.build || a.probe_key != z.probe_key || a.group_side != z.group_side ||
+        a.group_column != z.group_column || a.naggregates != z.naggregates || a.nleaves != z.nleaves || !a.probe ||
+        !z.probe || a.probe->cols.size() != z.probe->cols.size())
+        return false;
+    for (size_t c = 0; c < a.probe->cols.size(); c++)
+        if (a.probe->cols[c].type != z.probe->cols[c].type) return false;
+    for (int j = 0; j < a.naggregates; j++)
+        if (a.funcs[j] != z.funcs[j] || a.sides[j] != z.sides[j] || a.columns[j] != z.columns[j]) return false;
+    for (int l = 0; l < a.nleaves; l++)
+        if (a.leaves[l].column != z.leaves[l].column || a.leaves[l].op != z.leaves[l].op ||
+            a.leaves[l].lit_type != z.leaves[l].lit_type)
+            return false;
+    return true;
+}
+
+// Several join-aggregates of one shape in one launch of the compiled fused
+// kernel (agg_lean_multi_kernel); requests that cannot share it, and one
+// whose small table overflows, run alone through join_aggregate.
+std::vector<oxb_batch*> join_aggregate_many(const StreamRef& s, const Backend& b, const oxb_join_aggregate_args* all,
+                                            int nall) {
+    std::vector<oxb_batch*> res(nall, nullptr);
+    try {
+        // The requests that can share the launch: the compiled kernel's shape,
+        // the first such request's; the others run alone.
+        std::vector<int> idx;
+        std::vector<AggPlan> plans;
+        std::vector<DevPredicate> preds;
+        int la0 = kLeanNone, la1 = kLeanNone;
+        for (int r = 0; r < nall; r++) {
+            const oxb_join_aggregate_args& ar = all[r];
+            bool ok = ar.probe && ar.build && ar.table && ar.group_side == 1 && ar.probe->rows < (1ll << 38) &&
+                      ar.group_column >= 0 && ar.group_column < (int)ar.build->cols.size() && ar.probe_key >= 0 &&
+                      ar.probe_key < (int)ar.probe->cols.size() && ar.table->build_rows == ar.build->rows &&
+                      ar.naggregates >= 0 && ar.naggregates <= kMaxOuts;
+            if (ok && !idx.empty()) ok = same_join_shape(ar, all[idx[0]]);
+            if (ok) {
+                const Column& g = ar.build->cols[ar.group_column];
+                ok = g.type == kInt64 || g.type == kInt32;
+            }
+            std::vector<int> funcs;
+            std::vector<AggInputCol> inputs;
+            for (int j = 0; ok && j < ar.naggregates; j++) {
+                if (ar.funcs[j] != OXB_AGG_COUNT_STAR &&
+                    (ar.sides[j] != 0 || ar.columns[j] < 0 || ar.columns[j] >= (int)ar.probe->cols.size())) {
+                    ok = false;
+                    break;
+                }
+                const Column* c = ar.funcs[j] == OXB_AGG_COUNT_STAR ? nullptr : &ar.probe->cols[ar.columns[j]];
+                if (ar.funcs[j] != OXB_AGG_COUNT_STAR && c->type != kInt64 && c->type != kFloat64 && c->type != kInt32) ok = false;
+                funcs.push_back(ar.funcs[j]);
+                inputs.push_back(AggInputCol{c, 0});
+            }
+            if (ok) {
+                AggPlan pl = plan_aggregate(funcs, inputs, ar.build->cols[ar.group_column].type);
+                DevPredicate pr = make_predicate(*ar.probe, ar.leaves, ar.nleaves);
+                const Column& pk = ar.probe->cols[ar.probe_key];
+                int x0, x1;
+                ok = (pk.type == kInt64 || pk.type == kInt32) && lean_shape(pl.P, pr, pk.validity, &x0, &x1);
+                if (ok && !idx.empty()) ok = x0 == la0 && x1 == la1 && pl.P.narrays == plans[0].P.narrays;
+                if (ok) {
+                    if (idx.empty()) {
+                        la0 = x0;
+                        la1 = x1;
+                    }
+                    idx.push_back(r);
+                    plans.push_back(pl);
+                    preds.push_back(pr);
+                }
+            }
+        }
+        std::vector<bool> shared(nall, false);
+        if (idx.size() > 1)
+            for (int r : idx) shared[r] = true;
+        for (int r = 0; r < nall; r++)
+            if (!shared[r]) res[r] = join_aggregate(s, b, all[r]);
+        if (idx.size() <= 1) return res;
+        std::vector<oxb_join_aggregate_args> a;
+        for (int r : idx) a.push_back(all[r]);
+        const int n = (int)a.size();
+        std::vector<oxb_batch*> out(n, nullptr);
+        auto alone = [&](int q) { out[q] = join_aggregate(s, b, a[q]); };
+        auto finish = [&]() {
+            for (int q = 0; q < n; q++) {
+                res[idx[q]] = out[q];
+                out[q] = nullptr;
+            }
+            return res;
+        };
+        const oxb_join_aggregate_args& a0 = a[0];
+        const Column* gk = &a0.build->cols[a0.group_column];
+        AggPlan plan;
+        DevPredicate pred{};
+        try {
+        plan = plans[0];
+        pred = preds[0];
+        AggProgram& P = plan.P;
+        const JoinTableDev jt = a0.table->t;
+        const long long build_rows = a0.build->rows;
+        // The group key's sample (build side) and the Float64 inputs' largest
+        // values over every request, in one round trip.
+        unsigned long long h[3 + kMaxAccs] = {0, (unsigned long long)LLONG_MAX, (unsigned long long)LLONG_MIN};
+        const long long samples = build_rows < 8192 ? build_rows : 8192;
+        if (samples > 0) {
+            const unsigned int tcap = 16384;
+            Scratch<long long> t(s, tcap);
+            Scratch<unsigned long long> outs(s, 3 + kMaxAccs);
+            OXB_CUDA(cudaMemcpyAsync(outs.get(), h, sizeof h, cudaMemcpyHostToDevice, s->stream));
+            note_launch(), fill_i64_kernel<<<16, 256, 0, s->stream>>>(t.get(), tcap, kEmptyKey);
+            AggKey sk{gk->values, gk->validity, gk->type, 0};
+            note_launch(), agg_sample_kernel<<<grid_for(b, samples, 256, 2), 256, 0, s->stream>>>(sk, build_rows, samples,
+                                                                                                t.get(), tcap, outs.get());
+            for (int r = 0; r < n; r++) {
+                const long long nr = a[r].probe->rows, fs = nr < 8192 ? nr : 8192;
+                for (int j = 0; j < P.nacc && fs > 0; j++)
+                    if (plans[r].P.acc[j].kind == kAccSumF64 && plans[r].P.acc[j].in_type == kFloat64)
+                        note_launch(), f64_absmax_sample_kernel<<<grid_for(b, fs, 256, 2), 256, 0, s->stream>>>(
+                            (const double*)plans[r].P.acc[j].values, plans[r].P.acc[j].validity, nr, fs, outs.get() + 3 + j);
+            }
+            OXB_CUDA(cudaGetLastError());
+            OXB_CUDA(cudaMemcpyAsync(h, outs.get(), sizeof h, cudaMemcpyDeviceToHost, s->stream));
+            OXB_CUDA(cudaStreamSynchronize(s->stream));
+        }
+        const long long d = (long long)h[0];
+        const unsigned long long span = d > 0 ? (unsigned long long)(long long)h[2] - (unsigned long long)(long long)h[1] : ~0ull;
+        if (d == 0 || span >= 4096ull || fused_smem_bytes((int)span + 1, P.narrays) > 48 * 1024) {
+            for (int r = 0; r < n; r++) alone(r);
+            return finish();
+        }
+        const long long full = build_rows < 1 ? 1 : build_rows;
+        const unsigned int cap = d * 8 <= samples ? next_pow2(std::min<long long>(2 * full, 64ll * d + 4096), 4096)
+                                                  : next_pow2(2 * full, 4096);
+        const int S = (int)span + 1;
+        const long long direct_lo = (long long)h[1];
+        // Fixed-point windows (the widest any request needs), as run_aggregate places them.
+        int fix_lo[kMaxAccs];
+        for (int j = 0; j < P.nacc; j++) {
+            fix_lo[j] = INT_MIN;
+            if (P.acc[j].kind != kAccSumF64 || P.acc[j].in_type != kFloat64 || h[3 + j] == 0) continue;
+            int e = 0;
+            std::frexp(as_f64_host(h[3 + j]), &e);
+            const int lo = e + 1 - 63;
+            if (lo >= -900 && lo <= 800) fix_lo[j] = lo;
+        }
+        P.smem_slots = S;
+        P.wslots = 0;
+        P.direct = 1;
+        P.direct_lo = direct_lo;
+        P.capacity = cap;
+        P.probe_limit = kMaxInsertProbes;
+        P.stride = (long long)cap + 2;
+        for (int j = 0; j < P.nacc; j++) {
+            P.acc[j].fix = fix_lo[j] != INT_MIN;
+            P.acc[j].fix_lo = P.acc[j].fix ? fix_lo[j] : 0;
+        }
+        // The probe table, once for every request.
+        AggKey k{gk->values, gk->validity, gk->type, 1};
+        FusedTab ft{};
+        AllocRef fs;
+        const unsigned long long key_span = (unsigned long long)jt.key_hi - (unsigned long long)jt.key_lo;
+        const bool dense = jt.key_lo <= jt.key_hi && key_span < (1ull << 26) && (long long)key_span < 4 * jt.ndistinct + 4096;
+        const int fgrid = grid_for(b, jt.capacity, 256, 8);
+        if (dense) {
+            ft.dense_lo = jt.key_lo;
+            ft.dense_n = key_span + 1;
+            fs = dev_alloc(s, (size_t)ft.dense_n * 4, false);
+            OXB_CUDA(cudaMemsetAsync(fs->ptr, 0xff, (size_t)ft.dense_n * 4, s->stream));
+            ft.dense = (const int*)fs->ptr;
+            note_launch(), fuse_dense_kernel<<<fgrid, 256, 0, s->stream>>>(jt, k, direct_lo, S, (int*)fs->ptr, ft.dense_lo);
+        } else {
+            fs = dev_alloc(s, (size_t)jt.capacity * sizeof(FusedSlot), false);
+            ft.slots = (const FusedSlot*)fs->ptr;
+            note_launch(), fuse_table_kernel<<<fgrid, 256, 0, s->stream>>>(jt, k, direct_lo, S, (FusedSlot*)fs->ptr);
+        }
+        // Each request's HBM table and its work.
+        std::vector<AllocRef> keep;
+        std::vector<LeanReq> hreq(n);
+        std::vector<AggProgram> Pr(n, P);
+        Scratch<unsigned int> status(s, n, true);
+        long long ntiles = 0;
+        for (int r = 0; r < n; r++) {
+            AllocRef km = dev_alloc(s, (size_t)cap * 8, false);
+            AllocRef am = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
+            keep.push_back(km);
+            keep.push_back(am);
+            Pr[r].keys = (long long*)km->ptr;
+            Pr[r].arr = (unsigned long long*)am->ptr;
+            Pr[r].status = status.get() + r;
+            note_launch(), agg_init_kernel<<<grid_for(b, (long long)P.narrays * P.stride, 256, 8), 256, 0, s->stream>>>(Pr[r]);
+            LeanReq& q = hreq[r];
+            const oxb_join_aggregate_args& ar = a[r];
+            q.cols.pk = ar.probe->cols[ar.probe_key].values;
+            for (int l = 0; l < 2; l++) {
+                q.cols.leaf[l] = l < ar.nleaves ? preds[r].leaves[l].values : nullptr;
+                q.cols.lit[l] = l < ar.nleaves ? preds[r].leaves[l].lit : 0;
+                q.cols.acc[l] = l < plans[r].P.nacc ? plans[r].P.acc[l].values : nullptr;
+            }
+            q.n = ar.probe->rows;
+            q.tile0 = ntiles;
+            ntiles += (q.n + kLeanTile - 1) / kLeanTile;
+            q.keys = Pr[r].keys;
+            q.arr = Pr[r].arr;
+            q.status = Pr[r].status;
+        }
+        Scratch<LeanReq> dreq(s, n);
+        Scratch<unsigned long long> queue(s, 1, true);
+        OXB_CUDA(cudaMemcpyAsync(dreq.get(), hreq.data(), n * sizeof(LeanReq), cudaMemcpyHostToDevice, s->stream));
+        const LeanPlan L = lean_plan(P, pred);
+        LeanMultiKernel kern = lean_multi_kernel_for(la0, la1, dense);
+        const size_t smem = fused_smem_bytes(S, P.narrays);
+        set_smem(kern, smem);
+        {
+            KernelTimer timer(b, s, dense ? "agg_join_kernel<fused-dense,lean,many>" : "agg_join_kernel<fused,lean,many>");
+            timer.begin();
+            if (ntiles > 0)
+                note_launch(), kern<<<(unsigned)resident_grid(b, kern, smem, ntiles * kFusedThreads), kFusedThreads, smem,
+                                      s->stream>>>(P, pred, L, k, a0.probe->cols[a0.probe_key].type, jt, ft, dreq.get(), n,
+                                                   ntiles, queue.get());
+            timer.end();
+        }
+        OXB_CUDA(cudaGetLastError());
+        for (int r = 0; r < n; r++) {
+            out[r] = emit_groups(s, b, plans[r], Pr[r], cap, status.get() + r, true);
+            if (!out[r]) alone(r);  // its table overflowed: alone, with its own retry
+        }
+        return finish();
+        } catch (...) {
+            for (oxb_batch* x : out) delete x;
+            throw;
+        }
+    } catch (...) {
+        for (oxb_batch* x : res) delete x;
+        throw;
+    }
+}
+
 
 }  // namespace oxb

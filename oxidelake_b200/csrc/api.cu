@@ -614,6 +614,24 @@ oxb_status oxb_join_aggregate(oxb_backend* backend, oxb_stream* stream, const ox
     });
 }
 
+oxb_status oxb_join_aggregate_many(oxb_backend* backend, oxb_stream* stream, const oxb_join_aggregate_args* args,
+                                   int32_t n, oxb_batch** out) {
+    return counted(backend, OXB_OP_AGGREGATE, [&](oxb_call_stats& st) {
+        use_device(backend);
+        if (n < 0 || (n > 0 && (!args || !out))) fail(OXB_PLAN, "null argument");
+        for (int i = 0; i < n; i++) {
+            if (!args[i].probe || !args[i].table || !args[i].build) fail(OXB_PLAN, "request without probe, build or table");
+            st.rows_in += (uint64_t)args[i].probe->rows;
+        }
+        st.batches = (uint64_t)n;
+        std::vector<oxb_batch*> res = join_aggregate_many(stream_of(stream), backend->b, args, n);
+        for (int i = 0; i < n; i++) {
+            out[i] = res[i];
+            st.rows_out += (uint64_t)res[i]->rows;
+        }
+    });
+}
+
 oxb_status oxb_vector_distance(oxb_backend* backend, oxb_stream* stream, const oxb_vector_distance_args* args,
                                oxb_batch** out) {
     return counted(backend, OXB_OP_VECTOR, [&](oxb_call_stats& st) {

@@ -287,6 +287,11 @@ oxb_batch* aggregate(const StreamRef& s, const Backend& b, const oxb_aggregate_a
 oxb_batch* vector_distance(const StreamRef& s, const Backend& b,
                            const oxb_vector_distance_args& a);
 oxb_batch* join_aggregate(const StreamRef& s, const Backend& b, const oxb_join_aggregate_args& a);
+// Requests of one shape (same_join_shape) in one launch; each result equals
+// its own join_aggregate call's.
+bool same_join_shape(const oxb_join_aggregate_args& a, const oxb_join_aggregate_args& z);
+std::vector<oxb_batch*> join_aggregate_many(const StreamRef& s, const Backend& b, const oxb_join_aggregate_args* a,
+                                            int n);
 void launch_vector_distance(const StreamRef& s, const Backend& b, const Column& vec, long long n,
                             const float* dquery, int metric, float* out);
 

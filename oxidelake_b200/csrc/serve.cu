@@ -6,7 +6,9 @@
 // budget, and batches continuously: while work is on the GPU, new top-k
 // requests queue, and the next free worker stacks every queued request that
 // differs from the oldest one only in its query vector, k and its per-query
-// literal into one tensor-core scan.  Workers own one CUDA stream each, so
+// literal into one tensor-core scan; queued join-aggregates of one shape
+// (same table, group key, aggregates and comparisons) run as one launch of
+// the fused kernel, each into its own table.  Workers own one CUDA stream each, so
 // admitted work items overlap on the device.  Latencies (submit to result)
 // give p50/p99 beside throughput.
 #include <chrono>
@@ -133,7 +135,15 @@ struct Server {
                             for (Request* o : pick) kmax = std::max(kmax, o->k);
                             est = estimate_topk(*r, (int)pick.size(), kmax);
                         } else {
+                            // Join-aggregates of one shape share a launch, each
+                            // with its own table: their estimates add.
                             est = r->est_bytes;
+                            for (Request* o : pending)
+                                if (o != r && (int)pick.size() < max_batch && o->kind == kReqJoinAggregate &&
+                                    same_join_shape(r->ja, o->ja) && in_use + est + o->est_bytes <= budget) {
+                                    pick.push_back(o);
+                                    est += o->est_bytes;
+                                }
                         }
                         // Admission: wait for memory to free up unless nothing
                         // else holds any (a request alone never exceeds the
@@ -209,9 +219,14 @@ struct Server {
                     r.ids.assign(ids.begin() + (size_t)i * kmax, ids.begin() + (size_t)i * kmax + r.k);
                     r.dist.assign(dist.begin() + (size_t)i * kmax, dist.begin() + (size_t)i * kmax + r.k);
                 }
-            } else {
+            } else if (work.size() == 1) {
                 Request& r = *work[0];
                 r.batch = join_aggregate(s, b, r.ja);
+            } else {
+                std::vector<oxb_join_aggregate_args> args;
+                for (Request* r : work) args.push_back(r->ja);
+                std::vector<oxb_batch*> res = join_aggregate_many(s, b, args.data(), (int)args.size());
+                for (size_t i = 0; i < work.size(); i++) work[i]->batch = res[i];
             }
         } catch (const Error& e) {
             for (Request* r : work) {

@@ -212,3 +212,58 @@ def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, 
         vals = x[(g == grp) & valid]
         exact = math.fsum(vals.tolist())
         assert abs(sums[grp] - exact) <= 1e-12 * abs(exact) + 1e-300, (grp, sums[grp], exact)
+
+
+def test_many_requests_in_one_launch(backend, stream):
+    """Join-aggregates that differ in their probe batch and WHERE literal run
+    as one launch (oxb_join_aggregate_many), each into its own table: every
+    result equals its own call's and the oracle's.  Request sizes from 0 rows
+    to several tiles; one request with NULL payloads (which the compiled
+    kernel does not take) runs alone, inside the same call."""
+    build, probe = config2(20_000, 700_000, seed=91)
+    rng = np.random.default_rng(92)
+    bdev = backend.upload(stream, build)
+    table = backend.prepare_join_build(stream, bdev, 0)
+    sizes = [0, 1, 1000, 8191, 8193, 60_000, 250_000, 380_815]
+    reqs, hosts = [], []
+    off = 0
+    for i, n in enumerate(sizes):
+        part = probe.slice(off, n)
+        off += n
+        if i == 3:  # NULL payloads
+            pay = part.column(1).to_numpy(zero_copy_only=False)
+            part = pa.RecordBatch.from_arrays([part.column(0), pa.array(pay, mask=rng.random(n) < 0.1), part.column(2)],
+                                              names=part.schema.names)
+        lit = int(rng.integers(1, 50))
+        hosts.append((part, lit))
+        reqs.append((backend.upload(stream, part), 0, table, compare(2, Cmp.Gt, Literal.int32(lit)), (1, 1), AGGS))
+    backend.set_kernel_timing(True)
+    try:
+        outs = backend.join_aggregate_many(stream, reqs)
+        assert "many" in backend.last_kernel_time()[0]
+    finally:
+        backend.set_kernel_timing(False)
+    spec = [(int(f), s, c) for f, s, c in AGGS]
+    for (part, lit), r, o in zip(hosts, reqs, outs):
+        got = backend.download(stream, o)
+        alone = backend.download(stream, backend.join_aggregate(stream, *r))
+        want = oracle.join_aggregate(part, build, 0, 0, [(2, 3, 3, lit)], (1, 1), spec)
+        assert_batches_equal(got, want, float_sum_cols=(1, 4))
+        assert_batches_equal(got, alone, float_sum_cols=(1, 4))
+
+
+def test_many_requests_of_different_shapes_run_alone(backend, stream):
+    build, probe = config2(5_000, 90_000, seed=93)
+    bdev = backend.upload(stream, build)
+    table = backend.prepare_join_build(stream, bdev, 0)
+    pdev = backend.upload(stream, probe)
+    aggs2 = [(F.Sum, 0, 2), (F.CountStar, 0, 0)]
+    reqs = [(pdev, 0, table, compare(2, Cmp.Gt, Literal.int32(20)), (1, 1), AGGS),
+            (pdev, 0, table, compare(2, Cmp.Lt, Literal.int32(20)), (1, 1), aggs2)]
+    outs = backend.join_aggregate_many(stream, reqs)
+    for r, o in zip(reqs, outs):
+        got = backend.download(stream, o)
+        spec = [(int(f), s, c) for f, s, c in r[5]]
+        lf = r[3]
+        want = oracle.join_aggregate(probe, build, 0, 0, leaves(lf), (1, 1), spec)
+        assert_batches_equal(got, want, float_sum_cols=(1, 4) if len(spec) == 4 else ())

@@ -97,7 +97,7 @@ def test_mixed_stream_equals_alone(backend, stream, resident):
     got, st = served(backend, stream, resident, reqs)
     check_same(reqs, got, want)
     assert st["completed"] == len(reqs)
-    assert st["batched_queries"] > 0, st  # queued top-k requests shared scans
+    assert st["batched_queries"] > 0, st  # queued requests shared launches
     assert st["dispatches"] < len(reqs)
     assert 0 < st["p50_us"] <= st["p99_us"] and st["qps"] > 0
 
@@ -151,3 +151,14 @@ def test_admission_defers_until_memory_frees(backend, stream, resident):
                                                      DistanceMetric.L2)
         assert (ids == want_ids[0]).all()
         assert (dist.view(np.uint32) == want_dist[0].view(np.uint32)).all()
+
+
+def test_join_aggregates_share_launches(backend, stream, resident):
+    """Join-aggregate requests queued together (probe batches of one shape,
+    different WHERE literals) run as shared launches; each result equals its
+    direct call."""
+    reqs = [("ja", 5 + 3 * i) for i in range(12)]
+    want = [direct(backend, stream, resident, r) for r in reqs]
+    got, st = served(backend, stream, resident, reqs, workers=1, max_batch=64)
+    check_same(reqs, got, want)
+    assert st["completed"] == 12 and st["dispatches"] < 12 and st["batched_queries"] > 1, st
