@@ -439,6 +439,8 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--configs", default="1,3,4,5", help="other configurations measured on one GPU ('' for none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--agg-variant", type=int, default=-1,
+                    help="pin the join-aggregate kernel variant as oxb_set_agg_variant does (-1: tuned)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -470,6 +472,8 @@ def main() -> int:
 
     build, probe = gen_data(rank, args.build_rows, args.probe_rows)
     backend = CudaBackend(local)
+    if args.agg_variant >= 0:
+        backend.set_agg_variant(args.agg_variant, 0)
     stream = backend.create_stream()
     tstream = torch.cuda.ExternalStream(stream.cuda_handle())
     bdev = backend.upload(stream, build)

@@ -560,10 +560,12 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * the single persistent kernel), 11 or 12 (join-aggregate only: 5 or 6 with
  * the probe columns streamed into shared memory by bulk copies), 13 or 14
  * (join-aggregate only: 5 or 6 compiled for the accumulator shape, when the
- * inputs are at most two sums and no column has a validity bitmap);
+ * inputs are at most two sums and no column has a validity bitmap), 15 or
+ * 16 (13 or 14 reading each column two rows per vector load, when every
+ * column starts on a 16-byte boundary; otherwise 13 or 14);
  * rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
- * 1 or 2, the fused kernels 2 or 4, the vector ones 4 or 8; other values
- * round to the nearest the kernel has). */
+ * 1 or 2, the fused kernels 2 or 4, the compiled ones 1, 2 or 4, the vector
+ * ones 4 or 8; other values round to the nearest the kernel has). */
 OXB_API oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread);
 
 /* ---- telemetry: the counters of OperatorStats

@@ -57,7 +57,7 @@ def test_duplicates_nulls_and_probe_side_groups(backend, stream):
             assert_batches_equal(got, want, float_sum_cols=(1,))
 
 
-@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4, 5, 6, 7, 8, 11, 12, 13, 14])
+@pytest.mark.parametrize("combine", [0, 1, 2, 3, 4, 5, 6, 7, 8, 11, 12, 13, 14, 15, 16])
 @pytest.mark.parametrize("rpt", [1, 2])
 def test_every_kernel_variant(backend, stream, combine, rpt):
     """Each compiled variant of the row-loop kernels (the autotuner's
@@ -94,9 +94,9 @@ def test_every_kernel_variant(backend, stream, combine, rpt):
 
 
 @pytest.mark.parametrize("rpt", [2, 4, 8])
-@pytest.mark.parametrize("form", [5, 6, 7, 8, 11, 12, 13, 14],
+@pytest.mark.parametrize("form", [5, 6, 7, 8, 11, 12, 13, 14, 15, 16],
                          ids=["dense", "hashed", "dense-vec", "hashed-vec", "dense-stream", "hashed-stream",
-                              "dense-lean", "hashed-lean"])
+                              "dense-lean", "hashed-lean", "dense-lean4", "hashed-lean4"])
 def test_fused_probe_table_edges(backend, stream, rpt, form):
     """The fused probe-table kernel (a build-side group key, probe-side
     inputs) on the cases its fast path hands to the slow one: build keys
@@ -138,8 +138,9 @@ def test_fused_probe_table_edges(backend, stream, rpt, form):
             got = run(backend, stream, build, probe, pred, (1, 1), agg_set)
             name = backend.last_kernel_time()[0]
             # the lean kernels take no validity bitmaps: these columns have
-            # them, so forms 13 and 14 run the interpreted fused kernel
-            assert ("fused" in name) == fused and ("fused-dense" in name) == (fused and form in (5, 7, 11, 13)), name
+            # them, so forms 13 to 16 run the interpreted fused kernel
+            assert ("fused" in name) == fused and ("fused-dense" in name) == (fused and form in (5, 7, 11, 13, 15)), name
+            assert "lean" not in name, name
             assert ("vec" in name) == (fused and form in (7, 8)), name
             assert ("stream" in name) == (fused and form in (11, 12)), name
             spec = [(int(f), s, c) for f, s, c in agg_set]
@@ -151,9 +152,9 @@ def test_fused_probe_table_edges(backend, stream, rpt, form):
         backend.set_kernel_timing(False)
 
 
-@pytest.mark.parametrize("form", [5, 6, 7, 8, 11, 12, 13, 14],
+@pytest.mark.parametrize("form", [5, 6, 7, 8, 11, 12, 13, 14, 15, 16],
                          ids=["dense", "hashed", "dense-vec", "hashed-vec", "dense-stream", "hashed-stream",
-                              "dense-lean", "hashed-lean"])
+                              "dense-lean", "hashed-lean", "dense-lean4", "hashed-lean4"])
 def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, form):
     """The fused kernels fold a Float64 SUM as an exact integer in a window
     placed from a sample of the column, and every other value through the
@@ -183,8 +184,8 @@ def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, 
     i9 = np.nonzero(g == 9)[0]
     x[i9[:1]], x[i9[1:2]] = np.inf, -np.inf
     x[g == 10] = -0.0
-    # the lean kernels (forms 13, 14) take columns without validity bitmaps
-    null = rng.random(npr) < (0.0 if form in (13, 14) else 0.02)
+    # the lean kernels (forms 13 to 16) take columns without validity bitmaps
+    null = rng.random(npr) < (0.0 if form in (13, 14, 15, 16) else 0.02)
     null[~np.isfinite(x)] = False  # the NaN and infinities stay in their groups
     probe = pa.RecordBatch.from_arrays([pa.array(fk), pa.array(x, mask=null),
                                         pa.array(rng.integers(1, 51, npr).astype(np.int32))],
@@ -195,7 +196,8 @@ def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, 
     backend.set_kernel_timing(True)
     try:
         got = run(backend, stream, build, probe, None, (1, 1), aggs)
-        assert ("lean" in backend.last_kernel_time()[0]) == (form in (13, 14))
+        name = backend.last_kernel_time()[0]
+        assert ("lean" in name) == (form in (13, 14, 15, 16)) and ("lean4" in name) == (form in (15, 16)), name
     finally:
         backend.set_agg_variant(-1, 0)
         backend.set_kernel_timing(False)
