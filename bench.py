@@ -21,8 +21,11 @@ oracle on the host cores and a parity check at the measured size:
   config4  top-10 of 256 queries over 10M x 768 FP32 rows, WHERE f < 30 (30 %),
            l2 and cosine (parity on 16 of the 256 queries over every row)
   config5  the served mixed stream against the plain one-query-at-a-time path
+  plain_operators  filter_project, probe_join + hash_join over the headline's
+           100M-row probe, vector_distance over 4M x 768 rows, each against
+           the measured HBM bandwidth (parity: whole results; a distance slice)
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--configs 1,3,4,5]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--configs 1,3,4,5,ops]
 
 N > 1 (one process per GPU under torchrun): weak scaling, each rank its own
 100M-row probe shard and the same build side; the per-rank group partials are
@@ -78,6 +81,22 @@ def profiled_traffic(kernel: str):
                 except ValueError:
                     return None
     return None
+
+
+def profile_kernel(variant_name: str) -> str:
+    """The kernel a join-aggregate variant name (as last_kernel_time reports
+    it) launches, which names its committed ncu summary."""
+    if "lean4" in variant_name:
+        return "agg_lean4_join_kernel"
+    if "lean" in variant_name:
+        return "agg_lean_join_kernel"
+    if "stream" in variant_name:
+        return "agg_fstream_join_kernel"
+    if "vec" in variant_name:
+        return "agg_fusedv_join_kernel"
+    if "fused" in variant_name:
+        return "agg_fused_join_kernel"
+    return "agg_join_kernel"
 
 
 class ClockSampler:
@@ -415,6 +434,21 @@ def config4_block(backend, stream, threads: int, rows: int = 10_000_000, dim: in
     return out
 
 
+def ops_block(backend, stream, build, probe, bdev, pdev) -> dict:
+    """The plain drop-in operators (filter_project, probe_join, hash_join,
+    vector_distance) at HBM-bound sizes, each against the measured HBM
+    copy bandwidth and checked against the oracle."""
+    from oxidelake_b200 import bench_ops
+
+    peak, kind = peaks("hbm")
+    out = {}
+    for line in bench_ops.measure_filter_join(backend, stream, build, probe, bdev, pdev, peak, repeats=5):
+        out[line.pop("op")] = dict(line, peak_kind=kind)
+    line = bench_ops.measure_distance(backend, stream, peak, repeats=5)
+    out[line.pop("op")] = dict(line, peak_kind=kind)
+    return out
+
+
 def config5_block(backend, stream, build, probe, seconds: float = 2.0) -> dict:
     """Config 5: the served mixed stream against the plain path."""
     from oxidelake_b200 import bench_serve
@@ -437,7 +471,8 @@ def main() -> int:
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--configs", default="1,3,4,5", help="other configurations measured on one GPU ('' for none)")
+    ap.add_argument("--configs", default="1,3,4,5,ops",
+                    help="other configurations measured on one GPU ('' for none; 'ops': the plain operators)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--agg-variant", type=int, default=-1,
                     help="pin the join-aggregate kernel variant as oxb_set_agg_variant does (-1: tuned)")
@@ -598,7 +633,8 @@ def main() -> int:
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None,
                 "kernel_ms": round(kms, 4) if kms else None,
-                "traffic": profiled_traffic("agg_fused_join_kernel"),
+                "traffic": profiled_traffic(profile_kernel(kernel_name or "")),
+                "traffic_source": f"profiles/{profile_kernel(kernel_name or '')}_config2.md",
                 "algorithmic_bytes_per_launch": kernel_bytes,
             },
             "e2e": {
@@ -632,6 +668,7 @@ def main() -> int:
                 "3": lambda: config3_block(backend, stream, threads),
                 "4": lambda: config4_block(backend, stream, threads),
                 "5": lambda: config5_block(backend, stream, build, probe),
+                "ops": lambda: ops_block(backend, stream, build, probe, bdev, pdev),
             }
             for c in configs:
                 if c not in blocks:
@@ -642,9 +679,11 @@ def main() -> int:
                 except Exception as e:  # recorded in the line; the headline still prints
                     blk = {"error": repr(e)[:300]}
                 blk["seconds"] = round(time.perf_counter() - t0, 1)
-                per[f"config{c}"] = blk
+                per[f"config{c}" if c != "ops" else "plain_operators"] = blk
                 if c == "1" and "parity" in blk:
                     checks.append(blk["parity"]["result"])
+                if c == "ops":
+                    checks += [v["parity"]["result"] for v in blk.values() if isinstance(v, dict) and "parity" in v]
                 for sub in ("selectivity", "metric"):
                     checks += [v["parity"]["result"] for v in blk.get(sub, {}).values()]
             if per:

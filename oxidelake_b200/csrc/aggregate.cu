@@ -2456,6 +2456,7 @@ struct LeanPlan {
     int acc_off[2];  // acc_arr * S: the sum's CTA array, in 64-bit words from the table's base
     int fix[2];      // the program's DevAcc::fix and fix_lo of each sum
     int fix_lo[2];
+    int acc_leaf[2];  // the WHERE leaf that reads the same column as the sum (its values reused), or -1
 };
 
 // A comparison without branches: which of a < b, a == b, a > b holds picks
@@ -2634,8 +2635,13 @@ __device__ __forceinline__ void lean_rows4(const AggProgram& P, const DevPredica
         load_pairs(C.pk, pk_type == kInt64 ? 8 : 4, i, key);
         if (L.nleaves > 0) load_pairs(C.leaf[0], L.leaf_width[0], i, lv0);
         if (L.nleaves > 1) load_pairs(C.leaf[1], L.leaf_width[1], i, lv1);
-        if (A0 != kLeanNone) load_pairs(C.acc[0], A0 == kLeanSumI32 ? 4 : 8, i, v0);
-        if (A1 != kLeanNone) load_pairs(C.acc[1], A1 == kLeanSumI32 ? 4 : 8, i, v1);
+        if (A0 != kLeanNone && L.acc_leaf[0] < 0) load_pairs(C.acc[0], A0 == kLeanSumI32 ? 4 : 8, i, v0);
+        if (A1 != kLeanNone && L.acc_leaf[1] < 0) load_pairs(C.acc[1], A1 == kLeanSumI32 ? 4 : 8, i, v1);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if (A0 != kLeanNone && L.acc_leaf[0] >= 0) v0[r] = L.acc_leaf[0] == 0 ? lv0[r] : lv1[r];
+            if (A1 != kLeanNone && L.acc_leaf[1] >= 0) v1[r] = L.acc_leaf[1] == 0 ? lv0[r] : lv1[r];
+        }
     } else {
         load_pairs_tail(C.pk, pk_type == kInt64 ? 8 : 4, i, n, key);
         if (L.nleaves > 0) load_pairs_tail(C.leaf[0], L.leaf_width[0], i, n, lv0);
@@ -4204,6 +4210,10 @@ LeanPlan lean_plan(const AggProgram& P, const DevPredicate& pred) {
         L.acc_off[j] = P.acc[j].arr * P.smem_slots;
         L.fix[j] = P.acc[j].fix;
         L.fix_lo[j] = P.acc[j].fix_lo;
+        L.acc_leaf[j] = -1;
+        const int width = P.acc[j].in_type == kInt32 ? 4 : 8;
+        for (int l = 0; l < pred.nleaves && l < 2; l++)
+            if (pred.leaves[l].values == P.acc[j].values && L.leaf_width[l] == width) L.acc_leaf[j] = l;
     }
     return L;
 }
@@ -5371,7 +5381,8 @@ std::vector<oxb_batch*> join_aggregate_many(const StreamRef& s, const Backend& b
         Scratch<LeanReq> dreq(s, n);
         Scratch<unsigned long long> queue(s, 1, true);
         OXB_CUDA(cudaMemcpyAsync(dreq.get(), hreq.data(), n * sizeof(LeanReq), cudaMemcpyHostToDevice, s->stream));
-        const LeanPlan L = lean_plan(P, pred);
+        LeanPlan L = lean_plan(P, pred);
+        L.acc_leaf[0] = L.acc_leaf[1] = -1;  // the requests' columns differ
         LeanMultiKernel kern = lean_multi_kernel_for(la0, la1, dense);
         const size_t smem = fused_smem_bytes(S, P.narrays);
         set_smem(kern, smem);

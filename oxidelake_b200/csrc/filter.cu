@@ -198,14 +198,19 @@ oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter
     unsigned long long total = 0;
     Scratch<unsigned int> mask, tile_counts;
     Scratch<unsigned long long> tile_off;
+    // Device time of the mask pass, its scan and the gather (the host's
+    // read of the row count between them is not counted).
+    KernelTimer timer(b, s, "filter_mask_kernel+filter_gather_kernel");
     if (n > 0) {
         mask = Scratch<unsigned int>(s, (n + 31) / 32);
         tile_counts = Scratch<unsigned int>(s, ntiles);
         tile_off = Scratch<unsigned long long>(s, ntiles + 1);
         int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
+        timer.begin();
         note_launch(), filter_mask_kernel<<<grid, kThreads, 0, s->stream>>>(pred, n, mask.get(), tile_counts.get(), ntiles);
         OXB_CUDA(cudaGetLastError());
         scan_u32_to_u64(s, b, tile_counts.get(), tile_off.get(), ntiles);
+        timer.end();
         OXB_CUDA(cudaMemcpyAsync(&total, tile_off.get() + ntiles, sizeof total, cudaMemcpyDeviceToHost,
                                  s->stream));
         OXB_CUDA(cudaStreamSynchronize(s->stream));
@@ -235,7 +240,6 @@ oxb_batch* filter_project(const StreamRef& s, const Backend& b, const oxb_filter
     }
     if (total > 0 && a.nprojection > 0) {
         int grid = grid_for(b, ntiles * kThreads, kThreads, 8);
-        KernelTimer timer(b, s, "filter_gather_kernel");
         timer.begin();
         note_launch(), filter_gather_kernel<<<grid, kThreads, 0, s->stream>>>(mask.get(), tile_off.get(), n, ntiles, proj);
         timer.end();

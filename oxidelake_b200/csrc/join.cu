@@ -466,13 +466,13 @@ oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_joi
     auto* starts = (unsigned int*)m->starts_mem->ptr;
     if (n > 0) {
         Scratch<unsigned int> counts(s, n);
-        KernelTimer timer(b, s, "join_probe_kernel");
+        KernelTimer timer(b, s, "join_probe_kernel+scan");  // the probe and its offsets' scan
         timer.begin();
         note_launch(), join_probe_kernel<<<grid_for(b, n, 256, 8), 256, 0, s->stream>>>(a.table->t, key.values, key.validity,
                                                                           key.type, n, counts.get(), starts);
-        timer.end();
         OXB_CUDA(cudaGetLastError());
         scan_u32_to_u64(s, b, counts.get(), offsets, n);
+        timer.end();
     } else {
         OXB_CUDA(cudaMemsetAsync(offsets, 0, 8, s->stream));
     }

@@ -216,6 +216,41 @@ def test_fused_float_sums_in_and_out_of_the_fixed_point_window(backend, stream, 
         assert abs(sums[grp] - exact) <= 1e-12 * abs(exact) + 1e-300, (grp, sums[grp], exact)
 
 
+@pytest.mark.parametrize("form", [13, 15])
+def test_sum_of_the_where_column(backend, stream, form):
+    """The compiled kernels reuse a WHERE column's loaded values for a sum
+    over the same column: SUM(qty) under WHERE qty > 10, and SUM(payload)
+    under WHERE payload >= -40.5 AND qty < 45 (a Float64 leaf, compared by
+    its order key, summed as its raw value), each equal to the oracle's."""
+    from oxidelake_b200.params import and_
+
+    build, probe = config2(5_000, 300_001, seed=17 + form)
+    x = probe.column(1).to_numpy(zero_copy_only=False).copy()
+    x[::7] = -x[::7]  # negative payloads too
+    probe = pa.RecordBatch.from_arrays([probe.column(0), pa.array(x), probe.column(2)], names=probe.schema.names)
+    cases = [
+        (compare(2, Cmp.Gt, Literal.int32(10)), [(F.Sum, 0, 2), (F.CountStar, 0, 0)], ()),
+        (and_(compare(1, Cmp.GtEq, Literal.float64(-40.5)), compare(2, Cmp.Lt, Literal.int32(45))),
+         [(F.Sum, 0, 1), (F.Sum, 0, 2), (F.CountStar, 0, 0)], (1,)),
+    ]
+    backend.set_agg_variant(form, 1)
+    backend.set_kernel_timing(True)
+    try:
+        for pred, aggs, fcols in cases:
+            got = run(backend, stream, build, probe, pred, (1, 1), aggs)
+            assert "lean" in backend.last_kernel_time()[0]
+            spec = [(int(f), s, c) for f, s, c in aggs]
+            want = oracle.join_aggregate(probe, build, 0, 0, leaves(pred), (1, 1), spec)
+            # the scale: |x| on the rows the WHERE keeps (they still pass it)
+            xs = np.where(x >= -40.5, np.abs(x), x)
+            sprobe = pa.RecordBatch.from_arrays([probe.column(0), pa.array(xs), probe.column(2)], names=probe.schema.names)
+            scale = oracle.join_aggregate(sprobe, build, 0, 0, leaves(pred), (1, 1), spec)
+            assert_batches_equal(got, want, float_sum_cols=fcols, scale=scale)
+    finally:
+        backend.set_agg_variant(-1, 0)
+        backend.set_kernel_timing(False)
+
+
 def test_many_requests_in_one_launch(backend, stream):
     """Join-aggregates that differ in their probe batch and WHERE literal run
     as one launch (oxb_join_aggregate_many), each into its own table: every
