@@ -213,6 +213,61 @@ OXB_API oxb_status oxb_download(oxb_backend* backend, oxb_stream* stream, const 
                                 void* const* values, uint8_t* const* validity, int32_t* has_validity);
 OXB_API void oxb_batch_free(oxb_batch* batch);
 
+/* ---- Arrow C data interface (columns.rs:192-289 hands the backend the
+ * same buffers) ------------------------------------------------------------
+ * The structs are the Arrow project's stable C ABI ("The Arrow C data
+ * interface"), declared under its own include guard so a program that also
+ * includes Arrow's abi.h sees one definition. */
+#ifndef ARROW_C_DATA_INTERFACE
+#define ARROW_C_DATA_INTERFACE
+#define ARROW_FLAG_DICTIONARY_ORDERED 1
+#define ARROW_FLAG_NULLABLE 2
+#define ARROW_FLAG_MAP_KEYS_SORTED 4
+struct ArrowSchema {
+    const char* format;
+    const char* name;
+    const char* metadata;
+    int64_t flags;
+    int64_t n_children;
+    struct ArrowSchema** children;
+    struct ArrowSchema* dictionary;
+    void (*release)(struct ArrowSchema*);
+    void* private_data;
+};
+struct ArrowArray {
+    int64_t length;
+    int64_t null_count;
+    int64_t offset;
+    int64_t n_buffers;
+    int64_t n_children;
+    const void** buffers;
+    struct ArrowArray** children;
+    struct ArrowArray* dictionary;
+    void (*release)(struct ArrowArray*);
+    void* private_data;
+};
+#endif
+
+/* GpuBackend::upload of a RecordBatch exported through the Arrow C data
+ * interface: a struct array ("+s") whose children are Int64 ("l"), Int32
+ * ("i"), Float64 ("g"), Float32 ("f") or FixedSizeList<Float32, dim>
+ * ("+w:dim" over "f", no nulls inside the lists).  Array and child offsets
+ * are honoured (a validity bitmap at an odd bit offset is re-based on the
+ * host).  The copies finish before the call returns; then `array` and
+ * `schema` are released.  On an error neither is released (the caller
+ * still owns them, e.g. to take its CPU path after OXB_UNSUPPORTED). */
+OXB_API oxb_status oxb_import_arrow(oxb_backend* backend, oxb_stream* stream, struct ArrowArray* array,
+                                    struct ArrowSchema* schema, oxb_batch** out);
+/* GpuBackend::download into a RecordBatch exported through the Arrow C data
+ * interface: `out_array` and `out_schema` (caller-provided structs, filled
+ * here) describe a struct array whose children are the batch's columns,
+ * named names[i] (or "c<i>" when `names` is NULL), in host memory this call
+ * allocates.  The consumer releases them with their release callbacks.
+ * Synchronizes `stream`. */
+OXB_API oxb_status oxb_export_arrow(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch,
+                                    const char* const* names, struct ArrowArray* out_array,
+                                    struct ArrowSchema* out_schema);
+
 /* ---- operators --------------------------------------------------------- */
 
 /* FilterProjectArgs, args.rs:10-15 -> GpuBackend::filter_project

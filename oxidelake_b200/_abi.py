@@ -231,6 +231,30 @@ class JoinAggregateArgs(C.Structure):
 OP_TRANSFER, OP_FILTER, OP_JOIN, OP_AGGREGATE, OP_VECTOR = 0, 1, 2, 3, 4
 
 
+class ArrowSchema(C.Structure):
+    """struct ArrowSchema of the Arrow C data interface."""
+
+
+ArrowSchema._fields_ = [
+    ("format", C.c_char_p), ("name", C.c_char_p), ("metadata", C.c_char_p), ("flags", C.c_int64),
+    ("n_children", C.c_int64), ("children", C.POINTER(C.POINTER(ArrowSchema))),
+    ("dictionary", C.POINTER(ArrowSchema)), ("release", C.CFUNCTYPE(None, C.POINTER(ArrowSchema))),
+    ("private_data", C.c_void_p),
+]
+
+
+class ArrowArray(C.Structure):
+    """struct ArrowArray of the Arrow C data interface."""
+
+
+ArrowArray._fields_ = [
+    ("length", C.c_int64), ("null_count", C.c_int64), ("offset", C.c_int64), ("n_buffers", C.c_int64),
+    ("n_children", C.c_int64), ("buffers", C.POINTER(C.c_void_p)), ("children", C.POINTER(C.POINTER(ArrowArray))),
+    ("dictionary", C.POINTER(ArrowArray)), ("release", C.CFUNCTYPE(None, C.POINTER(ArrowArray))),
+    ("private_data", C.c_void_p),
+]
+
+
 class CallStats(C.Structure):
     _fields_ = [
         ("op", C.c_int32),
@@ -297,6 +321,8 @@ PROTOTYPES = {
     "oxb_batch_column": (_S, [_P, C.c_int32, C.POINTER(Column)]),
     "oxb_download_column": (_S, [_P, _P, _P, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "oxb_download": (_S, [_P, _P, _P, C.c_int32, _PP, _PP, C.POINTER(C.c_int32)]),
+    "oxb_import_arrow": (_S, [_P, _P, C.POINTER(ArrowArray), C.POINTER(ArrowSchema), _PP]),
+    "oxb_export_arrow": (_S, [_P, _P, _P, C.POINTER(C.c_char_p), C.POINTER(ArrowArray), C.POINTER(ArrowSchema)]),
     "oxb_batch_free": (None, [_P]),
     "oxb_filter_project": (_S, [_P, _P, C.POINTER(FilterProjectArgs), _PP]),
     "oxb_filter_project_noalloc": (

@@ -294,6 +294,32 @@ class CudaBackend:
         self.synchronize(stream)  # the host buffers may go once the copies are done
         return DeviceBatch(h.value, batch.schema)
 
+    def upload_arrow(self, stream: DeviceStream, batch: pa.RecordBatch) -> DeviceBatch:
+        """upload through the Arrow C data interface (oxb_import_arrow): the
+        batch is exported as a struct array and its buffers are read in
+        place, offsets included.  On an error the exported structs are
+        released here and the error raised."""
+        arr, sch = _abi.ArrowArray(), _abi.ArrowSchema()
+        batch._export_to_c(C.addressof(arr), C.addressof(sch))
+        h = C.c_void_p()
+        st = _L().oxb_import_arrow(self.handle, stream.handle, C.byref(arr), C.byref(sch), C.byref(h))
+        if st != 0:
+            for x in (arr, sch):
+                if x.release:
+                    x.release(C.byref(x))
+            _abi.check(st)
+        return DeviceBatch(h.value, batch.schema)
+
+    def download_arrow(self, stream: DeviceStream, batch: DeviceBatch) -> pa.RecordBatch:
+        """download through the Arrow C data interface (oxb_export_arrow),
+        imported by pyarrow without a copy."""
+        names = [f.name.encode() for f in batch.schema]
+        carr = (C.c_char_p * max(1, len(names)))(*names)
+        arr, sch = _abi.ArrowArray(), _abi.ArrowSchema()
+        _abi.check(_L().oxb_export_arrow(self.handle, stream.handle, batch.handle, carr, C.byref(arr), C.byref(sch)))
+        out = pa.RecordBatch._import_from_c(C.addressof(arr), C.addressof(sch))
+        return out.cast(batch.schema) if out.schema != batch.schema else out
+
     def batch_from_device(self, schema: pa.Schema, descs: List[_abi.Column], rows: int, keep=None) -> DeviceBatch:
         """A batch over columns already in device memory (no copy)."""
         arr = (_abi.Column * max(1, len(descs)))(*descs)

@@ -3573,8 +3573,11 @@ __device__ __noinline__ void part_null_row_to_hbm(const AggProgram& P, const Bat
     if (g >= 0) apply_vals<MAXACC>(P, P.arr, P.stride, g, 1, val, comp);
 }
 
+#ifndef OXB_SPLIT1_BLOCKS
+#define OXB_SPLIT1_BLOCKS 4  // resident CTAs an SM split1 is compiled for (64 registers)
+#endif
 template <int MAXACC>
-__global__ void __launch_bounds__(kThreads) part_split1_kernel(const __grid_constant__ AggProgram P,
+__global__ void __launch_bounds__(kThreads, OXB_SPLIT1_BLOCKS) part_split1_kernel(const __grid_constant__ AggProgram P,
                                                                const __grid_constant__ DevPredicate pred, int key_type,
                                                                const BatchCols* __restrict__ batches, int nb,
                                                                long long ntiles, unsigned long long* __restrict__ queue,

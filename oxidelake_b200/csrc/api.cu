@@ -398,38 +398,79 @@ void check_column_desc(const oxb_column& c, int64_t rows, int i) {
 
 extern "C" {
 
+}  // extern "C"
+
+namespace oxb {
+
+// The body of oxb_upload (and of the Arrow import): each host column into
+// new device memory, queued on the stream.
+std::unique_ptr<oxb_batch> upload_columns(oxb_backend* backend, const StreamRef& s, const oxb_column* columns,
+                                          int32_t ncols, int64_t rows, oxb_call_stats& st) {
+    if ((ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad upload arguments");
+    auto b = std::make_unique<oxb_batch>();
+    b->rows = rows;
+    for (int i = 0; i < ncols; i++) {
+        const oxb_column& c = columns[i];
+        check_column_desc(c, rows, i);
+        Column d;
+        d.type = c.type;
+        d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
+        d.length = rows;
+        if (rows > 0) {
+            size_t bytes = (size_t)rows * d.width();
+            d.owner_values = dev_alloc(s, bytes, false);
+            d.values = d.owner_values->ptr;
+            upload_bytes(backend->b, s, d.values, c.values, bytes);
+            if (c.validity) {
+                size_t vb = ((size_t)rows + 7) / 8;
+                d.owner_validity = dev_alloc(s, vb, false);
+                d.validity = (uint8_t*)d.owner_validity->ptr;
+                upload_bytes(backend->b, s, d.validity, c.validity, vb);
+            }
+        }
+        st.bytes_h2d += column_bytes(d);
+        b->cols.push_back(std::move(d));
+    }
+    st.rows_in = st.rows_out = (uint64_t)rows;
+    return b;
+}
+
+}  // namespace oxb
+
+extern "C" {
+
 oxb_status oxb_upload(oxb_backend* backend, oxb_stream* stream, const oxb_column* columns, int32_t ncols, int64_t rows,
                       oxb_batch** out) {
     return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
         use_device(backend);
         const StreamRef& s = stream_of(stream);
-        if (!out || (ncols > 0 && !columns) || ncols < 0 || rows < 0) fail(OXB_PLAN, "bad upload arguments");
-        auto b = std::make_unique<oxb_batch>();
-        b->rows = rows;
-        for (int i = 0; i < ncols; i++) {
-            const oxb_column& c = columns[i];
-            check_column_desc(c, rows, i);
-            Column d;
-            d.type = c.type;
-            d.dim = c.type == OXB_TYPE_VECTOR_F32 ? c.dim : 1;
-            d.length = rows;
-            if (rows > 0) {
-                size_t bytes = (size_t)rows * d.width();
-                d.owner_values = dev_alloc(s, bytes, false);
-                d.values = d.owner_values->ptr;
-                upload_bytes(backend->b, s, d.values, c.values, bytes);
-                if (c.validity) {
-                    size_t vb = ((size_t)rows + 7) / 8;
-                    d.owner_validity = dev_alloc(s, vb, false);
-                    d.validity = (uint8_t*)d.owner_validity->ptr;
-                    upload_bytes(backend->b, s, d.validity, c.validity, vb);
-                }
-            }
-            st.bytes_h2d += column_bytes(d);
-            b->cols.push_back(std::move(d));
-        }
-        st.rows_in = st.rows_out = (uint64_t)rows;
+        if (!out) fail(OXB_PLAN, "bad upload arguments");
+        *out = upload_columns(backend, s, columns, ncols, rows, st).release();
+    });
+}
+
+oxb_status oxb_import_arrow(oxb_backend* backend, oxb_stream* stream, struct ArrowArray* array,
+                            struct ArrowSchema* schema, oxb_batch** out) {
+    return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        const StreamRef& s = stream_of(stream);
+        if (!out || !array || !schema) fail(OXB_PLAN, "null Arrow import argument");
+        ArrowImport imp = arrow_import_columns(array, schema);
+        auto b = upload_columns(backend, s, imp.cols.data(), (int32_t)imp.cols.size(), array->length, st);
+        OXB_CUDA(cudaStreamSynchronize(s->stream));  // the Arrow buffers are read before they are released
+        array->release(array);
+        schema->release(schema);
         *out = b.release();
+    });
+}
+
+oxb_status oxb_export_arrow(oxb_backend* backend, oxb_stream* stream, const oxb_batch* batch,
+                            const char* const* names, struct ArrowArray* out_array, struct ArrowSchema* out_schema) {
+    return counted(backend, OXB_OP_TRANSFER, [&](oxb_call_stats& st) {
+        use_device(backend);
+        const StreamRef& s = stream_of(stream);
+        if (!batch || !out_array || !out_schema) fail(OXB_PLAN, "null Arrow export argument");
+        arrow_export_batch(backend->b, s, *batch, names, out_array, out_schema, st);
     });
 }
 

@@ -42,12 +42,18 @@ __global__ void __launch_bounds__(kThreads) filter_mask_kernel(const __grid_cons
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         unsigned int cnt = 0;
+        // The warp's 4 words: row (word0 + j) * 32 + lane, every leaf's loads
+        // for the 4 rows issued together.
+        const long long word0 = tile * kWords + warp * 4;
+        unsigned live = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((word0 + j) * 32 + lane < n) live |= 1u << j;
+        const unsigned sel = predicate_mask<4>(pred, word0 * 32 + lane, 32, live);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            long long word = tile * kWords + warp * 4 + j;
-            long long row = word * 32 + lane;
-            bool sel = row < n && predicate_holds(pred, row);
-            unsigned int bits = __ballot_sync(0xffffffffu, sel);
+            const long long word = word0 + j;
+            unsigned int bits = __ballot_sync(0xffffffffu, (sel >> j) & 1u);
             if (lane == 0 && word * 32 < n) mask[word] = bits;
             cnt += __popc(bits);
         }
@@ -60,19 +66,6 @@ __global__ void __launch_bounds__(kThreads) filter_mask_kernel(const __grid_cons
             tile_counts[tile] = t;
         }
         __syncthreads();
-    }
-}
-
-// Copies one selected row of a projected column (width 4, 8 or 4·dim bytes).
-__device__ __forceinline__ void copy_row(const DevProjCol& c, long long src_row, long long dst_row) {
-    if (c.width == 8) {
-        ((unsigned long long*)c.dst)[dst_row] = __ldg((const unsigned long long*)c.src + src_row);
-    } else if (c.width == 4) {
-        ((unsigned int*)c.dst)[dst_row] = __ldg((const unsigned int*)c.src + src_row);
-    } else {
-        const unsigned int* s = (const unsigned int*)c.src + src_row * (c.width / 4);
-        unsigned int* d = (unsigned int*)c.dst + dst_row * (c.width / 4);
-        for (int k = 0; k < c.width / 4; k++) d[k] = __ldg(s + k);
     }
 }
 
@@ -89,7 +82,7 @@ __device__ __forceinline__ void or_bits(unsigned int* words, unsigned long long 
     }
 }
 
-__global__ void __launch_bounds__(kThreads) filter_gather_kernel(
+__global__ void __launch_bounds__(kThreads, 5) filter_gather_kernel(
     const unsigned int* __restrict__ mask, const unsigned long long* __restrict__ tile_off, long long n,
     long long ntiles, const __grid_constant__ DevProjection proj) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -106,20 +99,50 @@ __global__ void __launch_bounds__(kThreads) filter_gather_kernel(
         }
         unsigned int excl = x - c;
         const unsigned long long toff = tile_off[tile];
+        // The warp's 4 words: each narrow column's kept values are loaded for
+        // all 4 words before any is stored, so 4 loads a lane are in flight.
+        unsigned int wb[4];
+        unsigned long long wbase[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            wb[j] = __shfl_sync(0xffffffffu, wbits, warp * 4 + j);
+            wbase[j] = toff + __shfl_sync(0xffffffffu, excl, warp * 4 + j);
+        }
+        const unsigned int lt = lanemask_lt();
+        for (int ci = 0; ci < proj.ncols; ci++) {
+            const DevProjCol& col = proj.cols[ci];
+            if (col.width == 8 || col.width == 4) {
+                unsigned long long v[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const long long row = (tile * kWords + warp * 4 + j) * 32 + lane;
+                    v[j] = 0;
+                    if ((wb[j] >> lane) & 1u)
+                        v[j] = col.width == 8 ? __ldcs((const unsigned long long*)col.src + row)
+                                              : (unsigned long long)__ldcs((const unsigned int*)col.src + row);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (!((wb[j] >> lane) & 1u)) continue;
+                    const long long drow = (long long)(wbase[j] + __popc(wb[j] & lt));
+                    if (col.width == 8) ((unsigned long long*)col.dst)[drow] = v[j];
+                    else ((unsigned int*)col.dst)[drow] = (unsigned int)v[j];
+                }
+            }
+        }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int wi = warp * 4 + j;
-            unsigned int bits = __shfl_sync(0xffffffffu, wbits, wi);
-            unsigned int pre = __shfl_sync(0xffffffffu, excl, wi);
+            unsigned int bits = wb[j];
             if (bits == 0) continue;  // uniform across the warp
             const long long row = (tile * kWords + wi) * 32 + lane;
             const bool sel = (bits >> lane) & 1u;
-            const unsigned int rank = __popc(bits & lanemask_lt());
-            const unsigned long long base = toff + pre;
+            const unsigned int rank = __popc(bits & lt);
+            const unsigned long long base = wbase[j];
             for (int ci = 0; ci < proj.ncols; ci++) {
                 const DevProjCol& col = proj.cols[ci];
                 if (col.width <= 8) {
-                    if (sel) copy_row(col, row, (long long)(base + rank));
+                    // narrow values were copied above
                 } else {
                     // Wide rows: the warp copies one selected row at a time.
                     unsigned int m = bits;

@@ -236,6 +236,18 @@ inline int grid_for(const Backend& b, long long work, int threads, int per_sm = 
 }
 
 DevPredicate make_predicate(const oxb_batch& in, const oxb_leaf* leaves, int nleaves);
+
+// ---- the Arrow C data interface (arrow_c.cu) ---------------------------------
+// Host column descriptors over an exported struct array's buffers (bitmaps
+// at an odd bit offset re-based into `rebased`).
+struct ArrowImport {
+    std::vector<oxb_column> cols;
+    std::vector<std::vector<uint8_t>> rebased;
+};
+ArrowImport arrow_import_columns(const ArrowArray* array, const ArrowSchema* schema);
+// A device batch copied to host memory and described as a struct array.
+void arrow_export_batch(Backend& b, const StreamRef& s, const oxb_batch& batch, const char* const* names,
+                        ArrowArray* out_array, ArrowSchema* out_schema, oxb_call_stats& st);
 void check_status_word(uint32_t status, const char* what);
 
 // Exclusive scan of n u32 counts into n + 1 u64 offsets (offsets[n] = total).
@@ -246,6 +258,12 @@ void scan_u32_to_u64(const StreamRef& s, const Backend& b, const unsigned int* c
 long long scan_partials_needed(long long n);
 void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsigned long long* offsets, long long n,
                           unsigned long long* partials);
+// The scan when the producer of the counts already wrote each block's total
+// (block b: counts [b * scan_block_rows(), (b + 1) * scan_block_rows())) into
+// partials[b]: the reduce pass is skipped.
+long long scan_block_rows();
+void scan_u32_to_u64_from_totals(const StreamRef& s, const unsigned int* counts, unsigned long long* offsets,
+                                 long long n, unsigned long long* partials);
 
 // Stable LSD radix sort of (key, value) pairs on bits [0, bits) of the key.
 void radix_sort_pairs(const StreamRef& s, const Backend& b, unsigned long long* keys,

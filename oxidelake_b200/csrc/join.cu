@@ -161,15 +161,53 @@ __device__ __forceinline__ bool join_lookup(const JoinTableDev& t, long long key
     return false;
 }
 
-__global__ void join_probe_kernel(const __grid_constant__ JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid,
-                                  int type, long long n, unsigned int* __restrict__ counts,
-                                  unsigned int* __restrict__ starts) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        unsigned int st = 0, c = 0;
-        if (valid_at(kvalid, i) && !join_lookup(t, join_key_at(kv, type, i), &st, &c)) st = c = 0;
-        counts[i] = c;
-        starts[i] = st;
+// The probe writes each row's match count and first build row, and each
+// block of scan_block_rows() rows its total, so the offsets' scan needs no
+// reduce pass of its own.
+constexpr int kProbeThreads = 256;
+
+__global__ void __launch_bounds__(kProbeThreads) join_probe_kernel(
+    const __grid_constant__ JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid, int type,
+    long long n, long long block_rows, unsigned int* __restrict__ counts, unsigned int* __restrict__ starts,
+    unsigned long long* __restrict__ totals) {
+    __shared__ unsigned long long warp_sums[kProbeThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long nblocks = (n + block_rows - 1) / block_rows;
+    for (long long blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+        const long long end = (blk + 1) * block_rows < n ? (blk + 1) * block_rows : n;
+        unsigned long long sum = 0;
+        for (long long i0 = blk * block_rows; i0 < end; i0 += 4 * kProbeThreads) {
+            // four rows a thread: their keys, then their lookups, in flight together
+            long long key[4];
+            bool live[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const long long i = i0 + k * kProbeThreads + threadIdx.x;
+                live[k] = i < end && valid_at(kvalid, i);
+                key[k] = live[k] ? join_key_at(kv, type, i) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const long long i = i0 + k * kProbeThreads + threadIdx.x;
+                if (i >= end) continue;
+                unsigned int st = 0, c = 0;
+                if (live[k] && !join_lookup(t, key[k], &st, &c)) st = c = 0;
+                counts[i] = c;
+                starts[i] = st;
+                sum += c;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) warp_sums[warp] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long tot = 0;
+#pragma unroll
+            for (int w = 0; w < kProbeThreads / 32; w++) tot += warp_sums[w];
+            totals[blk] = tot;
+        }
+        __syncthreads();
     }
 }
 
@@ -187,57 +225,132 @@ struct DevGather {
     DevGatherCol cols[kMaxOut];
 };
 
-// One thread per output row: the probe row holding match p is the last one
-// whose offset is <= p (cpu/kernels.rs:378-384), found by binary search.
-__global__ void join_gather_kernel(const unsigned long long* __restrict__ offsets,
-                                   const unsigned int* __restrict__ starts, long long nprobe,
-                                   const unsigned int* __restrict__ trows, long long ntrows,
-                                   long long right_rows, unsigned long long first, long long rows, const __grid_constant__ DevGather g,
-                                   unsigned int* __restrict__ status) {
+// The probe row holding match p is the last one whose offset is <= p
+// (cpu/kernels.rs:378-384).  Output rows are cut into kGatherTile-row
+// tiles; join_tile_rows_kernel finds the probe row of each tile's first
+// output by one binary search over the whole offsets array, and the gather
+// then searches only its tile's rows: in shared memory when their offsets
+// fit (kGatherRegion rows, the case whenever at least one probe row in two
+// matches), else in HBM over that range.
+constexpr int kGatherTile = 2048;
+constexpr int kGatherThreads = 256;
+constexpr int kGatherRegion = 4096;
+
+// offsets[lo] <= p < offsets[hi] on entry; the last i in [lo, hi) with
+// offsets[i] <= p.
+__device__ __forceinline__ long long last_at_or_below(const unsigned long long* offsets, long long lo, long long hi,
+                                                     unsigned long long p) {
+    while (hi - lo > 1) {
+        const long long mid = lo + (hi - lo) / 2;
+        if (offsets[mid] <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// tile_row[k] = the probe row of output min(k * kGatherTile, rows - 1), for
+// k in [0, ntiles]: tile k's outputs come from probe rows tile_row[k] ..
+// tile_row[k + 1].
+__global__ void join_tile_rows_kernel(const unsigned long long* __restrict__ offsets, long long nprobe,
+                                      unsigned long long first, long long rows, long long ntiles,
+                                      long long* __restrict__ tile_row) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k <= ntiles;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long t = k * kGatherTile < rows ? k * kGatherTile : rows - 1;
+        tile_row[k] = last_at_or_below(offsets, 0, nprobe, first + (unsigned long long)t);
+    }
+}
+
+__global__ void __launch_bounds__(kGatherThreads) join_gather_kernel(
+    const unsigned long long* __restrict__ offsets, const unsigned int* __restrict__ starts,
+    const long long* __restrict__ tile_row, long long ntiles, const unsigned int* __restrict__ trows,
+    long long ntrows, long long right_rows, unsigned long long first, long long rows,
+    const __grid_constant__ DevGather g, unsigned int* __restrict__ status) {
+    __shared__ unsigned long long offs[kGatherRegion + 1];
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t0 = blockIdx.x * (long long)blockDim.x; t0 < rows; t0 += stride) {
-        const long long t = t0 + threadIdx.x;
-        const bool live = t < rows;
-        long long lrow = 0, rrow = 0;
-        if (live) {
-            unsigned long long p = first + (unsigned long long)t;
-            long long lo = 0, hi = nprobe;  // invariant offsets[lo] <= p < offsets[hi]
-            while (hi - lo > 1) {
-                long long mid = lo + (hi - lo) / 2;
-                if (offsets[mid] <= p) lo = mid;
-                else hi = mid;
-            }
-            lrow = lo;
-            unsigned long long at = (unsigned long long)starts[lo] + (p - offsets[lo]);
-            if (at < (unsigned long long)ntrows) {
-                rrow = trows[at];
-                if (rrow >= right_rows) {
-                    rrow = 0;
-                    atomicOr(status, kStatusBounds);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long r0 = tile_row[tile], r1 = tile_row[tile + 1];
+        const long long span = r1 - r0 + 2;  // offsets[r0 .. r1 + 1]
+        const bool local = span <= kGatherRegion + 1;
+        __syncthreads();  // the previous tile's searches are done with offs
+        if (local)
+            for (long long i = threadIdx.x; i < span; i += blockDim.x) offs[i] = offsets[r0 + i];
+        __syncthreads();
+        const long long t0 = tile * kGatherTile;
+        constexpr int R = kGatherTile / kGatherThreads;
+        // Each output's probe and build rows first, all R of a thread's
+        // outputs, then every column's R values loaded before any is stored.
+        unsigned int lr[R], rr[R];
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const long long t = t0 + k * kGatherThreads + threadIdx.x;
+            lr[k] = rr[k] = 0;
+            if (t >= rows) continue;
+            const unsigned long long p = first + (unsigned long long)t;
+            long long lrow;
+            unsigned long long base;
+            if (local) {  // offs[0] <= p < offs[span - 1]
+                long long lo = 0, hi = span - 1;
+                while (hi - lo > 1) {
+                    const long long mid = (lo + hi) >> 1;
+                    if (offs[mid] <= p) lo = mid;
+                    else hi = mid;
                 }
+                lrow = r0 + lo;
+                base = offs[lo];
+            } else {
+                lrow = last_at_or_below(offsets, r0, r1 + 1, p);
+                base = offsets[lrow];
+            }
+            lr[k] = (unsigned int)lrow;
+            const unsigned long long at = (unsigned long long)starts[lrow] + (p - base);
+            if (at < (unsigned long long)ntrows) {
+                const unsigned int rrow = trows[at];
+                if (rrow >= right_rows) atomicOr(status, kStatusBounds);
+                else rr[k] = rrow;
             } else {
                 atomicOr(status, kStatusBounds);
             }
         }
         for (int ci = 0; ci < g.ncols; ci++) {
             const DevGatherCol& c = g.cols[ci];
-            const long long srow = c.side == 0 ? lrow : rrow;
-            if (live) {
-                if (c.width == 8)
-                    ((unsigned long long*)c.dst)[t] = __ldg((const unsigned long long*)c.src + srow);
-                else if (c.width == 4)
-                    ((unsigned int*)c.dst)[t] = __ldg((const unsigned int*)c.src + srow);
-                else {
+            if (c.width == 8 || c.width == 4) {
+                unsigned long long v[R];
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    const long long srow = c.side == 0 ? lr[k] : rr[k];
+                    v[k] = t >= rows ? 0ull
+                           : c.width == 8 ? __ldg((const unsigned long long*)c.src + srow)
+                                          : (unsigned long long)__ldg((const unsigned int*)c.src + srow);
+                }
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    if (t >= rows) continue;
+                    if (c.width == 8) ((unsigned long long*)c.dst)[t] = v[k];
+                    else ((unsigned int*)c.dst)[t] = (unsigned int)v[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    if (t >= rows) continue;
+                    const long long srow = c.side == 0 ? lr[k] : rr[k];
                     const int w = c.width / 4;
-                    const unsigned int* s = (const unsigned int*)c.src + srow * w;
+                    const unsigned int* src = (const unsigned int*)c.src + srow * w;
                     unsigned int* d = (unsigned int*)c.dst + t * w;
-                    for (int k = 0; k < w; k++) d[k] = __ldg(s + k);
+                    for (int q = 0; q < w; q++) d[q] = __ldg(src + q);
                 }
             }
             if (c.dst_valid) {
-                unsigned int bits = __ballot_sync(0xffffffffu, live && valid_at(c.src_valid, srow));
-                if (lane == 0 && t < rows) c.dst_valid[t >> 5] = bits;
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    const long long srow = c.side == 0 ? lr[k] : rr[k];
+                    const unsigned int bits = __ballot_sync(0xffffffffu, t < rows && valid_at(c.src_valid, srow));
+                    if (lane == 0 && t < rows) c.dst_valid[t >> 5] = bits;
+                }
             }
         }
     }
@@ -465,13 +578,17 @@ oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_joi
     auto* offsets = (unsigned long long*)m->offsets_mem->ptr;
     auto* starts = (unsigned int*)m->starts_mem->ptr;
     if (n > 0) {
+        const long long block_rows = scan_block_rows();
+        const long long nblocks = (n + block_rows - 1) / block_rows;
         Scratch<unsigned int> counts(s, n);
+        Scratch<unsigned long long> totals(s, nblocks + 1);
         KernelTimer timer(b, s, "join_probe_kernel+scan");  // the probe and its offsets' scan
         timer.begin();
-        note_launch(), join_probe_kernel<<<grid_for(b, n, 256, 8), 256, 0, s->stream>>>(a.table->t, key.values, key.validity,
-                                                                          key.type, n, counts.get(), starts);
+        note_launch(), join_probe_kernel<<<grid_for(b, nblocks * kProbeThreads, kProbeThreads, 8), kProbeThreads, 0,
+                                           s->stream>>>(a.table->t, key.values, key.validity, key.type, n, block_rows,
+                                                        counts.get(), starts, totals.get());
         OXB_CUDA(cudaGetLastError());
-        scan_u32_to_u64(s, b, counts.get(), offsets, n);
+        scan_u32_to_u64_from_totals(s, counts.get(), offsets, n, totals.get());
         timer.end();
     } else {
         OXB_CUDA(cudaMemsetAsync(offsets, 0, 8, s->stream));
@@ -537,11 +654,17 @@ oxb_batch* hash_join(const StreamRef& s, const Backend& b, const oxb_hash_join_a
     }
     if (rows > 0) {
         Scratch<unsigned int> status(s, 1, true);
-        KernelTimer timer(b, s, "join_gather_kernel");
+        const long long ntiles = (rows + kGatherTile - 1) / kGatherTile;
+        Scratch<long long> tile_row(s, ntiles + 1);
+        const auto* offsets = (const unsigned long long*)m.offsets_mem->ptr;
+        KernelTimer timer(b, s, "join_tile_rows_kernel+join_gather_kernel");
         timer.begin();
-        note_launch(), join_gather_kernel<<<grid_for(b, rows, 256, 8), 256, 0, s->stream>>>(
-            (const unsigned long long*)m.offsets_mem->ptr, (const unsigned int*)m.starts_mem->ptr, m.probe_rows,
-            a.table->t.rows, a.table->t.nrows, right.rows, a.first, rows, g, status.get());
+        note_launch(), join_tile_rows_kernel<<<grid_for(b, ntiles + 1, 256, 8), 256, 0, s->stream>>>(
+            offsets, m.probe_rows, a.first, rows, ntiles, tile_row.get());
+        note_launch(), join_gather_kernel<<<grid_for(b, ntiles * kGatherThreads, kGatherThreads, 8), kGatherThreads, 0,
+                                            s->stream>>>(offsets, (const unsigned int*)m.starts_mem->ptr, tile_row.get(),
+                                                         ntiles, a.table->t.rows, a.table->t.nrows, right.rows, a.first,
+                                                         rows, g, status.get());
         timer.end();
         OXB_CUDA(cudaGetLastError());
         uint32_t st = 0;

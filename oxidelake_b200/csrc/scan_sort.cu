@@ -272,6 +272,20 @@ void scan_u32_to_u64_into(const StreamRef& s, const unsigned int* counts, unsign
     OXB_CUDA(cudaGetLastError());
 }
 
+long long scan_block_rows() { return kScanChunk; }
+
+void scan_u32_to_u64_from_totals(const StreamRef& s, const unsigned int* counts, unsigned long long* offsets,
+                                 long long n, unsigned long long* partials) {
+    if (n <= 0) {
+        OXB_CUDA(cudaMemsetAsync(offsets, 0, sizeof(unsigned long long), s->stream));
+        return;
+    }
+    const long long blocks = (n + kScanChunk - 1) / kScanChunk;
+    note_launch(), scan_partials_kernel<<<1, 1024, 0, s->stream>>>(partials, blocks);
+    note_launch(), scan_apply_kernel<<<(unsigned)blocks, kScanThreads, 0, s->stream>>>(counts, n, partials, offsets);
+    OXB_CUDA(cudaGetLastError());
+}
+
 namespace {
 
 constexpr int kOrderWords = 1024;  // presence bits for keys below 32768

@@ -167,3 +167,47 @@ def test_dense_keys_placed_without_sort(backend, stream, key_type, dup):
     got = backend.download(stream, backend.hash_join(stream, ldev, rdev, table, m, 0, len(m), [1, 3, 0, 2]))
     want = oracle.hash_join_gather(probe, build, otable, om, 0, len(om), [1, 3, 0, 2])
     assert_batches_equal(got, want)
+
+
+@pytest.mark.parametrize("shape", ["sparse", "dense-dups", "mixed"])
+def test_gather_tiles_over_sparse_and_duplicate_matches(backend, stream, shape):
+    """The gather cuts its output into 2048-row tiles and searches each
+    tile's probe rows in shared memory when they fit (4096 rows), in HBM
+    otherwise.  Sparse matches (one probe row in 20 matches: a tile spans
+    about 40K probe rows), one build key repeated 5000 times (a tile inside
+    one probe row) and a mix, each gathered whole and in windows that cut
+    tiles at odd places, equal the oracle's rows."""
+    rng = np.random.default_rng({"sparse": 1, "dense-dups": 2, "mixed": 3}[shape])
+    nb, npr = 20_000, 400_000
+    rk = np.arange(nb, dtype=np.int64)
+    if shape != "sparse":
+        rk[:5000] = 7  # key 7: 5000 build rows
+    right = pa.RecordBatch.from_arrays([pa.array(rk), pa.array(rng.integers(0, 1 << 40, nb), pa.int64())],
+                                       names=["rk", "tag"])
+    if shape == "sparse":
+        fk = np.where(rng.random(npr) < 0.05, rng.integers(0, nb, npr), -1 - rng.integers(0, 1000, npr))
+    elif shape == "dense-dups":
+        fk = np.where(rng.random(npr) < 0.001, 7, rng.integers(nb, 2 * nb, npr))
+    else:
+        fk = np.where(rng.random(npr) < 0.5, rng.integers(0, nb, npr), -5)
+        fk[rng.random(npr) < 0.0005] = 7
+    left = pa.RecordBatch.from_arrays(
+        [pa.array(fk.astype(np.int64), mask=rng.random(npr) < 0.01),
+         pa.array(rng.standard_normal(npr), mask=rng.random(npr) < 0.02),
+         pa.array(rng.integers(-9, 9, npr).astype(np.int32))],
+        names=["fk", "v", "q"],
+    )
+    otable = oracle.JoinTable(right, 0)
+    om = oracle.JoinMatches(left, 0, otable)
+    ldev, rdev = backend.upload(stream, left), backend.upload(stream, right)
+    table = backend.prepare_join_build(stream, rdev, 0)
+    m = backend.probe_join(stream, ldev, 0, table)
+    total = len(m)
+    assert total == len(om) and total > 10_000
+    proj = [0, 1, 2, 4]
+    whole = oracle.hash_join_gather(left, right, otable, om, 0, total, proj)
+    got = backend.download(stream, backend.hash_join(stream, ldev, rdev, table, m, 0, total, proj))
+    assert_batches_equal(got, whole)
+    for first, rows in [(1, 2047), (2047, 2050), (total // 3, 4097), (total - 5001, 5001), (total - 1, 1)]:
+        got = backend.download(stream, backend.hash_join(stream, ldev, rdev, table, m, first, rows, proj))
+        assert_batches_equal(got, whole.slice(first, rows))

@@ -58,3 +58,20 @@ def test_null_element_in_a_valid_row_is_refused(backend, stream):
     vec = pa.FixedSizeListArray.from_arrays(child, 2)
     with pytest.raises(Unsupported):
         backend.upload(stream, pa.RecordBatch.from_arrays([vec], names=["v"]))
+
+
+@pytest.mark.parametrize("dim", [32, 132, 768])
+@pytest.mark.parametrize("metric", [DistanceMetric.L2, DistanceMetric.Cosine])
+def test_many_row_blocks_per_cta(backend, stream, dim, metric):
+    """Enough rows that each CTA of the pipelined kernel (dim a multiple of
+    4, at least 32) folds several 128-row blocks through its copy ring, and
+    a ragged last block; bit-exact against the sequential reference."""
+    rng = np.random.default_rng(dim + 3 * int(metric))
+    n = 150_001 if dim < 768 else 60_013
+    vals = rng.standard_normal(n * dim).astype(np.float32)
+    vec = pa.FixedSizeListArray.from_arrays(pa.array(vals), dim, mask=pa.array(rng.random(n) < 0.01))
+    batch = pa.RecordBatch.from_arrays([pa.array(np.arange(n)), vec], names=["id", "emb"])
+    q = rng.standard_normal(dim).astype(np.float32)
+    got = backend.download(stream, backend.vector_distance(stream, backend.upload(stream, batch), 1, q, metric, "d"))
+    want = oracle.vector_distance(batch, 1, q, int(metric))
+    assert_columns_equal(got.column(2), want, f"dim={dim} {metric.name}")
