@@ -3390,6 +3390,8 @@ constexpr int kMaxF1 = 128;
 constexpr int kMaxF2 = kMaxParts / kMaxF1;
 constexpr int kPartKeys = 256;   // keys per final partition the sizing aims at
 constexpr int kPartSlots = 1024; // shared slots of the fold (3/4 may fill)
+constexpr int kPartSlotBits = 10;
+static_assert(kPartSlots == 1 << kPartSlotBits, "the fold's slots are a power of two");
 constexpr int kFoldRows = 4;     // rows in flight per thread in the fold
 constexpr int kScanThreads = 1024;  // the scan pass: one CTA per SM (shared fine histogram)
 constexpr int kFineBits = 15;       // fine histogram buckets: the top 15 bits of the partition hash
@@ -3576,7 +3578,8 @@ __device__ __noinline__ void part_null_row_to_hbm(const AggProgram& P, const Bat
 #ifndef OXB_SPLIT1_BLOCKS
 #define OXB_SPLIT1_BLOCKS 4  // resident CTAs an SM split1 is compiled for (64 registers)
 #endif
-template <int MAXACC>
+// COMPACT: 16-byte records of one Int32 column (PartPlan::compact), else wider ones.
+template <int MAXACC, bool COMPACT>
 __global__ void __launch_bounds__(kThreads, OXB_SPLIT1_BLOCKS) part_split1_kernel(const __grid_constant__ AggProgram P,
                                                                const __grid_constant__ DevPredicate pred, int key_type,
                                                                const BatchCols* __restrict__ batches, int nb,
@@ -3609,7 +3612,7 @@ __global__ void __launch_bounds__(kThreads, OXB_SPLIT1_BLOCKS) part_split1_kerne
             // are loaded now, while the partition cursors are reserved.
             int xv[kSplitRows];
             unsigned xvalid = 0;
-            if (pp.compact) {
+            if (COMPACT) {
                 const int q = pp.src_of_col[0];
 #pragma unroll
                 for (int j = 0; j < kSplitRows; j++) {
@@ -3633,18 +3636,28 @@ __global__ void __launch_bounds__(kThreads, OXB_SPLIT1_BLOCKS) part_split1_kerne
             if (threadIdx.x < f1 && hist[threadIdx.x])
                 base1[threadIdx.x] = atomicAdd(&cursor1[threadIdx.x], (unsigned long long)hist[threadIdx.x]);
             __syncthreads();
-            // One row at a time from a register queue: a single copy of the
-            // row code, which stays in the instruction cache.
+            if (COMPACT) {
+                // 16-byte records: a short store a row, unrolled.
+#pragma unroll
+                for (int j = 0; j < kSplitRows; j++) {
+                    if ((nk >> j) & 1u) {
+                        part_null_row_to_hbm<MAXACC>(P, B, sub + threadIdx.x + (long long)j * kThreads);
+                    } else if ((m >> j) & 1u) {
+                        const unsigned long long pos = base1[rank[j] >> 24] + (rank[j] & 0xFFFFFFu);
+                        pp.recs[pos] = make_uint4((unsigned)key[j], (unsigned)((unsigned long long)key[j] >> 32),
+                                                  (unsigned)xv[j], (xvalid >> j) & 1u);
+                    }
+                }
+                continue;
+            }
+            // Wider records one row at a time from a register queue: a
+            // single copy of the row code, which stays in the instruction cache.
             unsigned mm = m, nn = nk;
 #pragma unroll 1
             for (int j = 0; j < kSplitRows && (mm | nn); j++) {
                 const long long r = sub + threadIdx.x + (long long)j * kThreads;
                 if (nn & 1u) {
                     part_null_row_to_hbm<MAXACC>(P, B, r);
-                } else if ((mm & 1u) && pp.compact) {
-                    const unsigned long long pos = base1[rank[0] >> 24] + (rank[0] & 0xFFFFFFu);
-                    pp.recs[pos] = make_uint4((unsigned)key[0], (unsigned)((unsigned long long)key[0] >> 32),
-                                              (unsigned)xv[0], xvalid & 1u);
                 } else if (mm & 1u) {
                     const unsigned long long pos = base1[rank[0] >> 24] + (rank[0] & 0xFFFFFFu);
                     unsigned long long w[MAXACC + 2];  // key, columns, validity
@@ -3675,12 +3688,10 @@ __global__ void __launch_bounds__(kThreads, OXB_SPLIT1_BLOCKS) part_split1_kerne
                 }
                 mm >>= 1;
                 nn >>= 1;
-                xvalid >>= 1;
 #pragma unroll
                 for (int t = 0; t + 1 < kSplitRows; t++) {
                     key[t] = key[t + 1];
                     rank[t] = rank[t + 1];
-                    xv[t] = xv[t + 1];
                 }
             }
         }
@@ -4013,7 +4024,9 @@ __global__ void __launch_bounds__(kThreads) part_fold_compact_kernel(const __gri
                 if (b0 + (unsigned long long)j * kThreads >= hi) break;
                 const long long key = (long long)((unsigned long long)rec[j].x | (unsigned long long)rec[j].y << 32);
                 int slot = -1;
-                unsigned int h = (unsigned int)(fmix64((unsigned long long)key) & (unsigned)(S - 1));
+                // the slot: multiply-shift (Fibonacci) hashing of the key, the
+                // top log2(S) bits of key * 2^64 / phi
+                unsigned int h = (unsigned int)(((unsigned long long)key * 0x9E3779B97F4A7C15ull) >> (64 - kPartSlotBits));
                 for (int q = 0; q < 64; q++) {
                     const long long k = ((volatile long long*)keys)[h];
                     if (k == key) {
@@ -4913,7 +4926,8 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
         }
         timer.rename("agg_batches_partitioned");
     }
-    auto psplit1 = maxacc == 2 ? part_split1_kernel<2> : part_split1_kernel<4>;
+    auto psplit1 = pp.compact ? (maxacc == 2 ? part_split1_kernel<2, true> : part_split1_kernel<4, true>)
+                              : (maxacc == 2 ? part_split1_kernel<2, false> : part_split1_kernel<4, false>);
     auto psplit2 = units == 1 ? part_split2_kernel<1> : (units == 2 ? part_split2_kernel<2> : part_split2_kernel<3>);
     auto pfold = maxacc == 2 ? (units == 1 ? part_fold_kernel<2, 1> : part_fold_kernel<2, 2>)
                              : (units == 1 ? part_fold_kernel<4, 1>
