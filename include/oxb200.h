@@ -617,7 +617,11 @@ OXB_API oxb_status oxb_set_autotune(oxb_backend* backend, int32_t enabled);
  * (join-aggregate only: 5 or 6 compiled for the accumulator shape, when the
  * inputs are at most two sums and no column has a validity bitmap), 15 or
  * 16 (13 or 14 reading each column two rows per vector load, when every
- * column starts on a 16-byte boundary; otherwise 13 or 14);
+ * column starts on a 16-byte boundary; otherwise 13 or 14), 17
+ * (oxb_aggregate_batches only: the dense-range passes, partitioned by the
+ * key's offset in the sampled key range, when every aggregate is COUNT,
+ * SUM, MIN or MAX of one Int32 column and the range holds at most 2^25
+ * keys; otherwise the single persistent kernel);
  * rows_per_thread 0 (automatic), 1, 2, 4 or 8 (the row loops take
  * 1 or 2, the fused kernels 2 or 4, the compiled ones 1, 2 or 4, the vector
  * ones 4 or 8; other values round to the nearest the kernel has). */

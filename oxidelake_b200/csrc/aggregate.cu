@@ -4109,6 +4109,430 @@ int compact_ops_of(const AggProgram& P, CompactOps* ops) {
     return m;
 }
 
+// ---- dense key ranges ----------------------------------------------------
+// When the kept keys fill a range of at most kDenseMaxParts * kDenseKeys
+// values (a sampled estimate, then checked row by row by the count pass),
+// the partitioned fold needs no hash at all: a key's partition is its offset
+// from the range's low end divided by kDenseKeys, and its slot in the fold's
+// shared table the remainder.  Records shrink to 8 bytes (the Int32 value;
+// the offset shifted left once, with the value's validity in bit 0).  The
+// count pass keeps one histogram per CTA, so every CTA of the split owns a
+// known slice of every partition and reserves nothing with global atomics
+// (which reach only about 80 G/s on random addresses on the B200).  The
+// groups leave the fold compacted and already in key order, so the emit
+// needs no sort.
+
+constexpr int kDenseBits = 13;
+constexpr int kDenseKeys = 1 << kDenseBits;  // keys a partition: the fold's shared table
+constexpr int kDenseMaxParts = 4096;        // so a range of at most 2^25 keys
+constexpr int kDenseThreads = 512;          // the count and split passes
+constexpr int kDenseRows = 8;               // rows a thread in a split sub-tile
+constexpr int kDenseSub = kDenseThreads * kDenseRows;
+constexpr int kDenseFoldThreads = 1024;
+constexpr int kDenseSamples = 16384;
+constexpr unsigned long long kSignBit = 0x8000000000000000ull;
+static_assert(kDenseSub <= 65536 && kDenseMaxParts <= 65536, "ranks and partitions pack into 16 bits each");
+
+struct DensePlan {
+    unsigned long long lo;    // the range's low end as an ordered key (key ^ sign bit)
+    unsigned long long span;  // keys in the range: np * kDenseKeys
+    int np;                   // partitions
+    int grid;                 // CTAs of the count and split passes (the same tile ranges)
+    int q;                    // the accumulator whose Int32 column the records carry
+    unsigned int* counts;     // [np][grid]: kept rows a partition and CTA
+    const unsigned long long* offs;  // their exclusive scan, [np * grid + 1]
+    uint2* recs;              // records: the value, offset << 1 | validity
+    unsigned long long nrecs;
+    unsigned int* status;
+};
+
+// A strided sample of the rows, spread over the partitioning tiles.
+// out[0] rows sampled, [1] rows the WHERE keeps, [2] and [3] the least and
+// greatest ordered key (key ^ sign bit) of the kept rows with a valid key.
+__global__ void part_dense_sample_kernel(const __grid_constant__ DevPredicate pred, int key_type,
+                                         const BatchCols* __restrict__ batches, int nb, long long ntiles, int samples,
+                                         unsigned long long* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < samples;
+    bool kept = false, kv = false;
+    unsigned long long ok = 0;
+    if (live) {
+        const long long t = (long long)i * ntiles / samples;
+        const BatchCols& B = batches[batch_of_tile(batches, nb, t)];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long rows = B.n - base < kPartTile ? B.n - base : kPartTile;
+        const long long r = base + (long long)(fmix64((unsigned long long)i + 1u) % (unsigned long long)rows);
+        long long key[1];
+        unsigned nk;
+        const unsigned m = kept_keys<1, 1>(pred, B, key_type, r, r + 1, key, &nk);
+        kept = ((m | nk) & 1u) != 0;
+        kv = (m & 1u) != 0;
+        ok = (unsigned long long)key[0] ^ kSignBit;
+    }
+    unsigned long long lo = kv ? ok : ~0ull, hi = kv ? ok : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o), c = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = c > hi ? c : hi;
+    }
+    const unsigned nlive = __popc(__ballot_sync(0xffffffffu, live)), nkept = __popc(__ballot_sync(0xffffffffu, kept));
+    const bool any = __ballot_sync(0xffffffffu, kv) != 0;
+    if ((threadIdx.x & 31) == 0) {
+        if (nlive) atomicAdd(&out[0], (unsigned long long)nlive);
+        if (nkept) atomicAdd(&out[1], (unsigned long long)nkept);
+        if (any) {
+            atomicMin(&out[2], lo);
+            atomicMax(&out[3], hi);
+        }
+    }
+}
+
+// The count pass, over a contiguous range of tiles a CTA (the split takes
+// the same ranges): the kept rows with a valid key in each partition, stored
+// as counts[p * grid + cta].  out[0] gets their number, out[1] the number of
+// kept rows whose key falls outside the range (the host then takes the
+// hashed passes instead).
+__global__ void __launch_bounds__(kDenseThreads) part_dense_count_kernel(const __grid_constant__ DevPredicate pred,
+                                                                         int key_type,
+                                                                         const BatchCols* __restrict__ batches, int nb,
+                                                                         long long ntiles,
+                                                                         const __grid_constant__ DensePlan dp,
+                                                                         unsigned long long* __restrict__ out) {
+    extern __shared__ unsigned int dhist[];
+    for (int i = threadIdx.x; i < dp.np; i += blockDim.x) dhist[i] = 0;
+    __syncthreads();
+    unsigned n = 0, outside = 0;
+    const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int bi = t0 < t1 ? batch_of_tile(batches, nb, t0) : 0;
+    for (long long t = t0; t < t1; t++) {
+        while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
+        const BatchCols& B = batches[bi];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
+        for (long long sub = base; sub < end; sub += kDenseSub) {
+            long long key[kDenseRows];
+            unsigned nk;
+            const unsigned m = kept_keys<kDenseRows, kDenseThreads>(pred, B, key_type, sub + threadIdx.x, end, key, &nk);
+#pragma unroll
+            for (int j = 0; j < kDenseRows; j++) {
+                if (!((m >> j) & 1u)) continue;
+                const unsigned long long rel = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
+                if (rel < dp.span) {
+                    atomicAdd(&dhist[rel >> kDenseBits], 1u);
+                    n++;
+                } else {
+                    outside++;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        outside += __shfl_xor_sync(0xffffffffu, outside, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (n) atomicAdd(&out[0], (unsigned long long)n);
+        if (outside) atomicAdd(&out[1], (unsigned long long)outside);
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) dp.counts[(long long)p * gridDim.x + blockIdx.x] = dhist[p];
+}
+
+// Exclusive scan of in[0, n) into out[0, n) by the whole block (a multiple
+// of 32 threads, at most 1024); *total gets the sum.  Ends synchronised.
+__device__ void block_exclusive_scan(const unsigned* in, unsigned* out, int n, unsigned* wsum, unsigned* total) {
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int b0 = threadIdx.x * per;
+    unsigned s = 0;
+    for (int i = 0; i < per; i++)
+        if (b0 + i < n) s += in[b0 + i];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = (int)blockDim.x >> 5;
+        const unsigned v = lane < nw ? wsum[lane] : 0u;
+        unsigned vi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
+            if (lane >= o) vi += y;
+        }
+        if (lane < nw) wsum[lane] = vi - v;
+        if (lane == 31) *total = vi;
+    }
+    __syncthreads();
+    unsigned run = wsum[w] + inc - s;
+    for (int i = 0; i < per; i++)
+        if (b0 + i < n) {
+            out[b0 + i] = run;
+            run += in[b0 + i];
+        }
+    __syncthreads();
+}
+
+size_t dense_split_smem(int np) { return (size_t)kDenseSub * (8 + 2) + (size_t)np * 12; }
+
+// The split, over the count pass's tile ranges.  Each sub-tile of kDenseSub
+// rows ranks its kept rows per partition in shared memory, orders their
+// records by partition there, and stores each partition's run at the CTA's
+// own cursor into that partition.  Kept rows whose key is NULL or INT64_MIN
+// fold straight into their HBM slots.
+template <int MAXACC>
+__global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(const __grid_constant__ AggProgram P,
+                                                                            const __grid_constant__ DevPredicate pred,
+                                                                            int key_type,
+                                                                            const BatchCols* __restrict__ batches,
+                                                                            int nb, long long ntiles,
+                                                                            const __grid_constant__ DensePlan dp) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    uint2* srec = (uint2*)dsm;                         // kDenseSub records, by partition
+    unsigned* cursor = (unsigned*)(srec + kDenseSub);  // np: the CTA's next record in each partition
+    unsigned* hist = cursor + dp.np;                   // np: the sub-tile's records a partition
+    unsigned* start = hist + dp.np;                    // np: their exclusive scan
+    unsigned short* spart = (unsigned short*)(start + dp.np);  // kDenseSub: each ordered record's partition
+    __shared__ unsigned wsum[kDenseThreads / 32];
+    __shared__ unsigned s_total;
+    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
+        cursor[p] = (unsigned)dp.offs[(long long)p * gridDim.x + blockIdx.x];
+        hist[p] = 0;
+    }
+    __syncthreads();
+    const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int bi = t0 < t1 ? batch_of_tile(batches, nb, t0) : 0;
+    for (long long t = t0; t < t1; t++) {
+        while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
+        const BatchCols& B = batches[bi];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
+        for (long long sub = base; sub < end; sub += kDenseSub) {
+            long long key[kDenseRows];
+            unsigned nk;
+            unsigned m = kept_keys<kDenseRows, kDenseThreads>(pred, B, key_type, sub + threadIdx.x, end, key, &nk);
+            uint2 rec[kDenseRows];
+            unsigned pr[kDenseRows];
+            const int q = dp.q;
+#pragma unroll
+            for (int j = 0; j < kDenseRows; j++) {
+                rec[j] = make_uint2(0u, 0u);
+                pr[j] = 0;
+                if (!((m >> j) & 1u)) continue;
+                const long long r = sub + threadIdx.x + (long long)j * kDenseThreads;
+                const unsigned long long rel = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
+                if (rel >= dp.span) {  // the count pass found none; never written out of range
+                    atomicOr(dp.status, kStatusBounds);
+                    m &= ~(1u << j);
+                    continue;
+                }
+                const bool v = valid_at(B.valid[q], r);
+                const int x = v ? __ldg((const int*)B.vals[q] + r) : 0;
+                rec[j] = make_uint2((unsigned)x, (unsigned)rel << 1 | (v ? 1u : 0u));
+                const unsigned p = (unsigned)(rel >> kDenseBits);
+                pr[j] = p << 16 | atomicAdd(&hist[p], 1u);
+            }
+#pragma unroll
+            for (int j = 0; j < kDenseRows; j++)
+                if ((nk >> j) & 1u) part_null_row_to_hbm<MAXACC>(P, B, sub + threadIdx.x + (long long)j * kDenseThreads);
+            __syncthreads();
+            block_exclusive_scan(hist, start, dp.np, wsum, &s_total);
+#pragma unroll
+            for (int j = 0; j < kDenseRows; j++) {
+                if (!((m >> j) & 1u)) continue;
+                const unsigned p = pr[j] >> 16;
+                const unsigned sidx = start[p] + (pr[j] & 0xFFFFu);
+                srec[sidx] = rec[j];
+                spart[sidx] = (unsigned short)p;
+            }
+            __syncthreads();
+            const unsigned total = s_total;
+            for (unsigned sidx = threadIdx.x; sidx < total; sidx += blockDim.x) {
+                const unsigned p = spart[sidx];
+                const unsigned long long pos = (unsigned long long)cursor[p] + (sidx - start[p]);
+                if (pos < dp.nrecs) dp.recs[pos] = srec[sidx];
+                else atomicOr(dp.status, kStatusBounds);
+            }
+            __syncthreads();
+            for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
+                cursor[p] += hist[p];
+                hist[p] = 0;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Slots [capacity] (the NULL group) and [capacity + 1] (the key INT64_MIN)
+// of every array: the only HBM slots the dense path folds into with atomics.
+__global__ void dense_special_init_kernel(const __grid_constant__ AggProgram P) {
+    for (int a = threadIdx.x; a < P.narrays; a += blockDim.x) {
+        P.arr[(long long)a * P.stride + P.capacity] = init_value(P.init[a]);
+        P.arr[(long long)a * P.stride + P.capacity + 1] = init_value(P.init[a]);
+    }
+}
+
+size_t dense_fold_smem(int ops) {
+    int arrays = 1 + ((ops & 1) ? 1 : 0) + ((ops & 2) ? 2 : 0) + ((ops & 4) ? 1 : 0) + ((ops & 8) ? 1 : 0);
+    return (size_t)arrays * kDenseKeys * 4;
+}
+
+// The fold, one partition a CTA at a time, into a shared table indexed by
+// the key's offset: 32-bit shared atomics only (the row count, COUNT, the
+// Int64 SUM as a 32-bit add and its carry, and MIN and MAX, each of those
+// two only after a plain read shows the value would change it).  The
+// partition's groups then go to the HBM table compacted and in key order,
+// at the partition's own slots [p * kDenseKeys, ...), and their number to
+// gcount[p].  OPS: bit 0 COUNT, 1 SUM, 2 MIN, 3 MAX (CompactOps).
+template <int OPS>
+__global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(const __grid_constant__ AggProgram P,
+                                                                               const __grid_constant__ DensePlan dp,
+                                                                               const __grid_constant__ CompactOps ops,
+                                                                               unsigned int* __restrict__ gcount) {
+    extern __shared__ __align__(16) unsigned int fsm[];
+    unsigned* rows = fsm;
+    unsigned* cnt = rows + kDenseKeys;
+    unsigned* slo = cnt + ((OPS & 1) ? kDenseKeys : 0);
+    unsigned* shi = slo + ((OPS & 2) ? kDenseKeys : 0);
+    int* mn = (int*)(shi + ((OPS & 2) ? kDenseKeys : 0));
+    int* mx = mn + ((OPS & 4) ? kDenseKeys : 0);
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned s_total;
+    constexpr int kPer = kDenseKeys / kDenseFoldThreads;  // slots a thread in the flush
+    constexpr int kInFlight = 4;                            // records a thread loads together
+    const long long st = P.stride;
+    for (int part = blockIdx.x; part < dp.np; part += gridDim.x) {
+        for (int i = threadIdx.x; i < kDenseKeys; i += blockDim.x) {
+            rows[i] = 0;
+            if (OPS & 1) cnt[i] = 0;
+            if (OPS & 2) {
+                slo[i] = 0;
+                shi[i] = 0;
+            }
+            if (OPS & 4) mn[i] = 0x7fffffff;
+            if (OPS & 8) mx[i] = (int)0x80000000;
+        }
+        __syncthreads();
+        const unsigned long long lo = dp.offs[(long long)part * dp.grid], hi = dp.offs[(long long)(part + 1) * dp.grid];
+        for (unsigned long long b0 = lo + threadIdx.x; b0 < hi; b0 += (unsigned long long)kDenseFoldThreads * kInFlight) {
+            uint2 rec[kInFlight];
+#pragma unroll
+            for (int j = 0; j < kInFlight; j++) {
+                const unsigned long long i = b0 + (unsigned long long)j * kDenseFoldThreads;
+                rec[j] = i < hi ? __ldcs(dp.recs + i) : make_uint2(0u, 0u);
+            }
+#pragma unroll
+            for (int j = 0; j < kInFlight; j++) {
+                if (b0 + (unsigned long long)j * kDenseFoldThreads >= hi) break;
+                const unsigned off = (rec[j].y >> 1) & (unsigned)(kDenseKeys - 1);
+                atomicAdd(&rows[off], 1u);
+                if (!(rec[j].y & 1u)) continue;  // a NULL value: the row counts, nothing else
+                const int x = (int)rec[j].x;
+                if (OPS & 1) atomicAdd(&cnt[off], 1u);
+                if (OPS & 2) {
+                    // x sign-extended to 64 bits: a 32-bit add and its carry
+                    const unsigned vlo = (unsigned)x, vhi = x < 0 ? 0xffffffffu : 0u;
+                    const unsigned old = vlo ? atomicAdd(&slo[off], vlo) : 0u;
+                    const unsigned up = vhi + (old + vlo < old ? 1u : 0u);
+                    if (up) atomicAdd(&shi[off], up);
+                }
+                if (OPS & 4)
+                    if (x < ((volatile int*)mn)[off]) atomicMin(&mn[off], x);
+                if (OPS & 8)
+                    if (x > ((volatile int*)mx)[off]) atomicMax(&mx[off], x);
+            }
+        }
+        __syncthreads();
+        // Flush: kPer consecutive slots a thread, ranked by a block scan of
+        // the occupied ones.
+        const int s0 = threadIdx.x * kPer;
+        unsigned c = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; k++) c += rows[s0 + k] != 0u ? 1u : 0u;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        unsigned inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wsum[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            const unsigned v = lane < (kDenseFoldThreads >> 5) ? wsum[lane] : 0u;
+            unsigned vi = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
+                if (lane >= o) vi += y;
+            }
+            if (lane < (kDenseFoldThreads >> 5)) wsum[lane] = vi - v;
+            if (lane == 31) s_total = vi;
+        }
+        __syncthreads();
+        long long g = (long long)part * kDenseKeys + wsum[w] + inc - c;
+        const unsigned long long kbase = dp.lo + (unsigned long long)part * kDenseKeys;
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            const int sl = s0 + k;
+            const unsigned nrows = rows[sl];
+            if (!nrows) continue;
+            P.keys[g] = (long long)((kbase + (unsigned long long)sl) ^ kSignBit);
+            P.arr[g] = nrows;
+            if (OPS & 1) P.arr[ops.count_arr * st + g] = cnt[sl];
+            if (OPS & 2) P.arr[ops.sum_arr * st + g] = (unsigned long long)shi[sl] << 32 | slo[sl];
+            if (OPS & 4) P.arr[ops.min_arr * st + g] = (unsigned long long)(long long)mn[sl];
+            if (OPS & 8) P.arr[ops.max_arr * st + g] = (unsigned long long)(long long)mx[sl];
+            g++;
+        }
+        if (threadIdx.x == 0) gcount[part] = s_total;
+        __syncthreads();
+    }
+}
+
+using DenseFold = void (*)(const AggProgram, const DensePlan, const CompactOps, unsigned int*);
+DenseFold dense_fold_for(int ops) {
+    switch (ops) {
+#define OXB_DF(m) \
+    case m: return part_dense_fold_kernel<m>;
+        OXB_DF(1) OXB_DF(2) OXB_DF(3) OXB_DF(4) OXB_DF(5) OXB_DF(6) OXB_DF(7) OXB_DF(8) OXB_DF(9) OXB_DF(10)
+        OXB_DF(11) OXB_DF(12) OXB_DF(13) OXB_DF(14) OXB_DF(15)
+#undef OXB_DF
+        default: return nullptr;
+    }
+}
+
+// The dense fold's groups in key order for agg_emit_kernel (whose key is
+// skeys[r] ^ sign bit, with lo = 0): the key INT64_MIN first when its slot
+// [capacity + 1] holds rows, then every partition's compacted groups.
+__global__ void dense_order_kernel(const __grid_constant__ AggProgram P, const unsigned long long* __restrict__ gpre,
+                                   int np, long long G, int has_min, unsigned long long* __restrict__ skeys,
+                                   unsigned int* __restrict__ sslots) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < G; r += (long long)gridDim.x * blockDim.x) {
+        if (has_min && r == 0) {
+            skeys[0] = 0;  // INT64_MIN ^ sign bit
+            sslots[0] = (unsigned)(P.capacity + 1);
+            continue;
+        }
+        const unsigned long long rr = (unsigned long long)(r - has_min);
+        int a = 0, b = np - 1;  // the last partition whose first group is at or before rr
+        while (a < b) {
+            const int mid = (a + b + 1) >> 1;
+            if (gpre[mid] <= rr) a = mid;
+            else b = mid - 1;
+        }
+        const long long slot = (long long)a * kDenseKeys + (long long)(rr - gpre[a]);
+        sslots[r] = (unsigned)slot;
+        skeys[r] = (unsigned long long)P.keys[slot] ^ kSignBit;
+    }
+}
+
 size_t part_fold_smem(int narrays) { return (size_t)kPartSlots * (8 + 4 + 8 * (narrays - 1)); }
 
 int maxacc_for(int nacc) { return nacc <= 2 ? 2 : (nacc <= 4 ? 4 : kMaxAccs); }
@@ -4335,6 +4759,10 @@ std::string variant_name(const char* base, const AggVariant& v) {
            std::to_string(v.rpt) + ">";
 }
 
+oxb_batch* emit_ordered(const StreamRef& s, const Backend& b, const AggPlan& plan, const AggProgram& P,
+                        const unsigned long long* okeys, const unsigned int* oslots, unsigned long long lo, long long G,
+                        bool has_null);
+
 // Collects the occupied slots of a filled table into the output batch: the
 // groups sorted by key with the NULL group last (aggregate.rs:35-66), one
 // column per aggregate.  nullptr when the table overflowed and the caller
@@ -4365,7 +4793,6 @@ oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan
 
     const long long G = (long long)h.G;
     const bool has_null = h.null_rows > 0;
-    const long long rows = G + (has_null ? 1 : 0);
     Scratch<unsigned long long> skeys(s, G + 1);
     Scratch<unsigned int> sslots(s, G + 1);
     unsigned long long lo = G > 0 ? h.lo : 0;
@@ -4391,7 +4818,15 @@ oxb_batch* emit_groups(const StreamRef& s, const Backend& b, const AggPlan& plan
             radix_sort_pairs(s, b, skeys.get(), sslots.get(), G, bits);
         }
     }
+    return emit_ordered(s, b, plan, P, okeys, oslots, lo, G, has_null);
+}
 
+// The output batch from the groups in key order (okeys[r] + lo is the
+// ordered key, oslots[r] the HBM slot of group r), the NULL group last.
+oxb_batch* emit_ordered(const StreamRef& s, const Backend& b, const AggPlan& plan, const AggProgram& P,
+                        const unsigned long long* okeys, const unsigned int* oslots, unsigned long long lo, long long G,
+                        bool has_null) {
+    const long long rows = G + (has_null ? 1 : 0);
     auto out = std::make_unique<oxb_batch>();
     out->rows = rows;
     AggOutput O{};
@@ -4776,6 +5211,133 @@ int resident_grid(const Backend& b, K kernel, size_t smem, long long work) {
 }  // namespace
 
 
+// The dense fold's output: groups numbered by a scan of the partitions'
+// group counts, the key INT64_MIN first and the NULL group last.
+oxb_batch* emit_dense(const StreamRef& s, const Backend& b, const AggPlan& plan, const AggProgram& P,
+                      const DensePlan& dp, const unsigned int* gcount) {
+    Scratch<unsigned long long> gpre(s, (size_t)dp.np + 1);
+    scan_u32_to_u64(s, b, gcount, gpre.get(), dp.np);
+    struct {
+        unsigned long long G, null_rows, min_rows;
+        uint32_t status;
+    } h{};
+    OXB_CUDA(cudaMemcpyAsync(&h.G, gpre.get() + dp.np, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.null_rows, P.arr + P.capacity, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.min_rows, P.arr + P.capacity + 1, 8, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaMemcpyAsync(&h.status, dp.status, 4, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    check_status_word(h.status, "aggregate");
+    const int has_min = h.min_rows > 0 ? 1 : 0;
+    const long long G = (long long)h.G + has_min;
+    Scratch<unsigned long long> skeys(s, G + 1);
+    Scratch<unsigned int> sslots(s, G + 1);
+    if (G > 0) {
+        note_launch(), dense_order_kernel<<<grid_for(b, G, 256, 8), 256, 0, s->stream>>>(P, gpre.get(), dp.np, G, has_min,
+                                                                                        skeys.get(), sslots.get());
+        OXB_CUDA(cudaGetLastError());
+    }
+    return emit_ordered(s, b, plan, P, skeys.get(), sslots.get(), 0, G, h.null_rows > 0);
+}
+
+// The dense-range passes (part_dense_*) when they apply: every accumulator
+// reads one Int32 column and is among COUNT, SUM, MIN and MAX of it (with
+// COUNT(*) beside them), the kept keys span at most 2^25 values, and, unless
+// pinned (variant 17), enough rows are kept for the passes to pay.  nullptr
+// otherwise, and the caller takes the direct or hashed passes.
+oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& plan, AggProgram P,
+                           const DevPredicate& pred, int key_type, const BatchCols* dbatches, int nb,
+                           long long nptiles, long long total, const int* acc_col, KernelTimer& timer) {
+    const bool pinned = b.force_combine == 17;
+    if (b.force_combine >= 0 && !pinned) return nullptr;
+    if (nptiles == 0 || total >= (1ll << 32) || P.nacc < 1 || P.nacc > 4) return nullptr;
+    for (int j = 1; j < P.nacc; j++)
+        if (acc_col[j] != acc_col[0]) return nullptr;
+    CompactOps ops;
+    const int mask = compact_ops_of(P, &ops);
+    if (!mask) return nullptr;
+
+    // The sampled key range, widened by an eighth of it and a partition on
+    // each side; the count pass then checks every kept key against it.
+    Scratch<unsigned long long> smp(s, 4);
+    unsigned long long hs[4] = {0, 0, ~0ull, 0};
+    OXB_CUDA(cudaMemcpyAsync(smp.get(), hs, sizeof hs, cudaMemcpyHostToDevice, s->stream));
+    note_launch(), part_dense_sample_kernel<<<kDenseSamples / 256, 256, 0, s->stream>>>(pred, key_type, dbatches, nb,
+                                                                                      nptiles, kDenseSamples, smp.get());
+    OXB_CUDA(cudaGetLastError());
+    OXB_CUDA(cudaMemcpyAsync(hs, smp.get(), sizeof hs, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    if (hs[1] == 0 || hs[2] > hs[3]) return nullptr;
+    const double kept_est = (double)hs[1] / (double)std::max<unsigned long long>(hs[0], 1) * (double)total;
+    const unsigned long long margin = (hs[3] - hs[2]) / 8 + kDenseKeys;
+    const unsigned long long lo = hs[2] > margin ? hs[2] - margin : 0ull;
+    const unsigned long long hi = hs[3] < ~0ull - margin ? hs[3] + margin : ~0ull;
+    const unsigned long long range = hi - lo;  // keys in the range, less one
+    if (range >= (unsigned long long)kDenseMaxParts * kDenseKeys) return nullptr;
+    const int np = (int)((range + kDenseKeys) / kDenseKeys);
+    // Worth it when the kept rows would make the direct fold's HBM table
+    // miss L2 (it reaches about 80 G atomics/s) and outnumber the range's
+    // slots, which the fold initialises and flushes partition by partition.
+    auto worth = [&](double kept) { return pinned || (kept >= 4e6 && kept >= 0.25 * (double)np * kDenseKeys); };
+    if (!worth(kept_est)) return nullptr;
+
+    DensePlan dp{};
+    dp.lo = lo;
+    dp.span = (unsigned long long)np * kDenseKeys;
+    dp.np = np;
+    dp.grid = b.sms * 2;
+    dp.q = 0;
+    Scratch<unsigned int> counts(s, (size_t)np * dp.grid);
+    Scratch<unsigned long long> cnt_out(s, 2, true);
+    dp.counts = counts.get();
+    timer.begin();
+    note_launch(), part_dense_count_kernel<<<dp.grid, kDenseThreads, (size_t)np * 4, s->stream>>>(
+        pred, key_type, dbatches, nb, nptiles, dp, cnt_out.get());
+    OXB_CUDA(cudaGetLastError());
+    timer.end();
+    unsigned long long hc[2] = {0, 0};
+    OXB_CUDA(cudaMemcpyAsync(hc, cnt_out.get(), sizeof hc, cudaMemcpyDeviceToHost, s->stream));
+    OXB_CUDA(cudaStreamSynchronize(s->stream));
+    if (hc[1] > 0 || !worth((double)hc[0])) return nullptr;
+
+    Scratch<unsigned long long> offs(s, (size_t)np * dp.grid + 1);
+    scan_u32_to_u64(s, b, counts.get(), offs.get(), (long long)np * dp.grid);
+    dp.offs = offs.get();
+    dp.nrecs = hc[0];
+    AllocRef recs_mem = dev_alloc(s, (size_t)std::max<unsigned long long>(hc[0], 1) * sizeof(uint2), false);
+    dp.recs = (uint2*)recs_mem->ptr;
+    Scratch<unsigned int> status(s, 1, true);
+    dp.status = status.get();
+    Scratch<unsigned int> gcount(s, (size_t)np);
+
+    const long long cap = (long long)np * kDenseKeys;
+    P.capacity = (unsigned int)cap;
+    P.probe_limit = cap;
+    P.stride = cap + 2;
+    P.smem_slots = 0;
+    P.wslots = 0;
+    AllocRef keys_mem = dev_alloc(s, (size_t)cap * 8, false);
+    AllocRef arr_mem = dev_alloc(s, (size_t)P.narrays * P.stride * 8, false);
+    P.keys = (long long*)keys_mem->ptr;
+    P.arr = (unsigned long long*)arr_mem->ptr;
+    P.status = status.get();
+
+    const int maxacc = maxacc_for(P.nacc);
+    auto split = maxacc == 2 ? part_dense_split_kernel<2> : part_dense_split_kernel<4>;
+    const size_t ssmem = dense_split_smem(np);
+    set_smem(split, ssmem);
+    DenseFold fold = dense_fold_for(mask);
+    const size_t fsmem = dense_fold_smem(mask);
+    set_smem(fold, fsmem);
+    timer.rename("agg_batches_dense");
+    timer.begin();
+    note_launch(), dense_special_init_kernel<<<1, 64, 0, s->stream>>>(P);
+    note_launch(), split<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, pred, key_type, dbatches, nb, nptiles, dp);
+    note_launch(), fold<<<std::min(np, b.sms), kDenseFoldThreads, fsmem, s->stream>>>(P, dp, ops, gcount.get());
+    OXB_CUDA(cudaGetLastError());
+    timer.end();
+    return emit_dense(s, b, plan, P, dp, gcount.get());
+}
+
 oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_aggregate_batches_args& a) {
     if (a.ninputs < 1 || !a.inputs || !a.spec) fail(OXB_PLAN, "aggregate_batches: no inputs or no spec");
     for (int i = 0; i < a.ninputs; i++)
@@ -4846,6 +5408,9 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
     // One pass over the input: distinct keys and count of the kept rows, and
     // their fine partition histogram (KernelTimer: this pass plus the fold).
     KernelTimer timer(b, s, "agg_batches_kernel");
+    if (oxb_batch* out = aggregate_dense(s, b, plan, P, pred, key.type, dbatches.get(), a.ninputs, nptiles, total,
+                                         acc_col, timer))
+        return out;
     Scratch<unsigned> regs(s, kHllRegs, true);
     Scratch<unsigned int> fine(s, kFine, true);
     Scratch<unsigned long long> kept_dev(s, 1, true);

@@ -836,7 +836,7 @@ uint64_t oxb_kernel_launches(void) { return g_launches.load(); }
 oxb_status oxb_set_agg_variant(oxb_backend* backend, int32_t combine, int32_t rows_per_thread) {
     OXB_TRY
     if (!backend) fail(OXB_PLAN, "backend is null");
-    if (combine < -1 || combine > 16) fail(OXB_PLAN, "combine must be -1 or 0..16");
+    if (combine < -1 || combine > 17) fail(OXB_PLAN, "combine must be -1 or 0..17");
     if (rows_per_thread != 0 && rows_per_thread != 1 && rows_per_thread != 2 && rows_per_thread != 4 &&
         rows_per_thread != 8)
         fail(OXB_UNSUPPORTED, "rows per thread must be 0 (automatic), 1, 2 or 4");

@@ -179,3 +179,106 @@ def test_partitioned_wide_records(backend, stream, ncols):
     scale = oracle.aggregate(abs_columns(whole, {1}), 0, [(int(f), c) for f, c in spec.aggregates], [])
     assert got.num_rows == w.num_rows
     assert_batches_equal(got, w, float_sum_cols=(1,), scale=scale)
+
+
+def _fold_named(backend, stream, batches, spec, pred, variant):
+    """The fold with the variant pinned, and the name of the timed passes."""
+    backend.set_agg_variant(variant, 0)
+    backend.set_kernel_timing(True)
+    try:
+        got = fold(backend, stream, batches, spec, pred)
+        name = backend.last_kernel_time()[0]
+    finally:
+        backend.set_agg_variant(-1, 0)
+        backend.set_kernel_timing(False)
+    return got, name
+
+
+@pytest.mark.parametrize("selectivity", [1, 50, 99])
+def test_dense_range_pinned(backend, stream, selectivity):
+    """Keys that fill their range, through the dense passes (variant 17:
+    partitions by key offset, 8-byte records, no hashing, groups emitted in
+    key order without a sort): bit-exact against the oracle."""
+    batches = config3_batches(3_000_000, 200_000, seed=100 + selectivity, min_rows=800, max_rows=400_000)
+    pred = compare(2, Cmp.Lt, Literal.int32(selectivity))
+    got, name = _fold_named(backend, stream, batches, SPEC, pred, 17)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, SPEC, pred)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_chosen_automatically(backend, stream):
+    """Enough kept rows over a filled range: the automatic choice is the
+    dense passes, with the oracle's groups."""
+    batches = config3_batches(6_000_000, 1_000_000, seed=5, min_rows=8192, max_rows=1 << 20)
+    pred = compare(2, Cmp.Lt, Literal.int32(99))
+    got, name = _fold_named(backend, stream, batches, SPEC, pred, -1)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, SPEC, pred)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_null_and_min_keys_and_carries(backend, stream):
+    """NULL keys (the NULL group last), the key INT64_MIN (first), groups
+    whose values are all NULL, COUNT(*) beside COUNT(x), empty batches, and
+    Int64 sums of Int32 extremes that carry across 32 bits both ways."""
+    rng = np.random.default_rng(123)
+    batches = []
+    for n in (0, 40_000, 1, 250_000, 7, 123_456):
+        g = rng.integers(-3000, 3000, n).astype(np.int64)
+        x = rng.choice(np.array([2**31 - 1, -(2**31), 1, -1, 0, 123_456_789], dtype=np.int32), n)
+        xm = (rng.random(n) < 0.05) | ((g >= 100) & (g < 110))
+        if n > 10:
+            g[:3] = np.iinfo(np.int64).min
+        batches.append(
+            pa.RecordBatch.from_arrays(
+                [pa.array(g, mask=rng.random(n) < 0.01), pa.array(x, mask=xm),
+                 pa.array(rng.integers(0, 100, n).astype(np.int32))],
+                names=["g", "x", "f"],
+            )
+        )
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Min, 1), (F.Max, 1), (F.Count, 1), (F.CountStar, 0)])
+    pred = compare(2, Cmp.Lt, Literal.int32(90))
+    got, name = _fold_named(backend, stream, batches, spec, pred, 17)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, spec, pred)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_int32_key_without_bitmaps(backend, stream):
+    """An Int32 group key over negative and positive values with gaps, and
+    an Int32 input without a validity bitmap (COUNT(x) is then the row
+    count), with no WHERE."""
+    rng = np.random.default_rng(321)
+    batches = []
+    for n in (90_000, 3, 410_000):
+        g = (rng.integers(-100_000, 100_000, n) * 3).astype(np.int32)
+        x = rng.integers(np.iinfo(np.int32).min, np.iinfo(np.int32).max, n, dtype=np.int64).astype(np.int32)
+        batches.append(pa.RecordBatch.from_arrays([pa.array(g), pa.array(x)], names=["g", "x"]))
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Max, 1), (F.Count, 1)])
+    got, name = _fold_named(backend, stream, batches, spec, None, 17)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, spec, None)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_outlier_keys_fall_back(backend, stream):
+    """A handful of keys far outside the sampled range: the count pass sees
+    them, and the fold takes the other passes, with the oracle's groups."""
+    rng = np.random.default_rng(11)
+    batches = []
+    for n in (300_000, 200_000):
+        g = rng.integers(0, 100_000, n).astype(np.int64)
+        g[n // 2 + 1] = 10**12
+        g[n // 3 + 7] = -(10**12)
+        x = rng.integers(-1000, 1000, n).astype(np.int32)
+        batches.append(pa.RecordBatch.from_arrays([pa.array(g), pa.array(x, mask=rng.random(n) < 0.02)], names=["g", "x"]))
+    got, name = _fold_named(backend, stream, batches, SPEC, None, 17)
+    assert name != "agg_batches_dense", name
+    _, w = want(batches, SPEC, None)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
