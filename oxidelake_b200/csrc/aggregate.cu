@@ -3496,6 +3496,95 @@ __device__ __forceinline__ unsigned kept_keys(const DevPredicate& pred, const Ba
     return keep & ~nk;
 }
 
+// kept_keys for the dense passes, with every load issued up front: a row
+// index past `end` is clamped to end - 1 (in bounds, its result masked
+// off), so the loads of all R rows are unconditional and independent, and
+// each column's type and bitmap test sits outside the loops over rows.
+// With X, accumulator q's Int32 values and validity come in the same batch
+// (values of rows without a valid value read as 0).
+template <int R, int T, bool X>
+__device__ __forceinline__ unsigned kept_keys_eager(const DevPredicate& pred, const BatchCols& B, int key_type,
+                                                    long long r0, long long end, long long* key, unsigned* nullkey,
+                                                    int q, int* xv, unsigned* xvalid) {
+    unsigned live = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++)
+        if (r0 + (long long)j * T < end) live |= 1u << j;
+    *nullkey = 0;
+    if (!live) return 0;
+    const long long last = end - 1;
+#define OXB_ROW(j) (r0 + (long long)(j) * T < last ? r0 + (long long)(j) * T : last)
+    if (key_type == kInt64) {
+        const long long* kp = (const long long*)B.key;
+#pragma unroll
+        for (int j = 0; j < R; j++) key[j] = __ldg(kp + OXB_ROW(j));
+    } else {
+        const int* kp = (const int*)B.key;
+#pragma unroll
+        for (int j = 0; j < R; j++) key[j] = (long long)__ldg(kp + OXB_ROW(j));
+    }
+    if (X) {
+        const int* xp = (const int*)B.vals[q];
+#pragma unroll
+        for (int j = 0; j < R; j++) xv[j] = __ldg(xp + OXB_ROW(j));
+    }
+    unsigned kvalid = live;
+    if (B.key_valid) {
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (!valid_at(B.key_valid, OXB_ROW(j))) kvalid &= ~(1u << j);
+    }
+    unsigned keep = live;
+    for (int l = 0; l < pred.nleaves; l++) {
+        const DevLeaf& lf = pred.leaves[l];
+        if (lf.type == kInt32) {
+            const int* ap = (const int*)B.lvals[l];
+            int a[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) a[j] = __ldg(ap + OXB_ROW(j));
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (!cmp_holds(lf.op, (long long)a[j], lf.lit)) keep &= ~(1u << j);
+        } else {
+            const long long* ap = (const long long*)B.lvals[l];
+            long long a[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) a[j] = __ldg(ap + OXB_ROW(j));
+            if (lf.type == kFloat64) {
+#pragma unroll
+                for (int j = 0; j < R; j++) a[j] = filter_order_key(__longlong_as_double(a[j]));
+            }
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (!cmp_holds(lf.op, a[j], lf.lit)) keep &= ~(1u << j);
+        }
+        if (B.lvalid[l]) {
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (!valid_at(B.lvalid[l], OXB_ROW(j))) keep &= ~(1u << j);
+        }
+    }
+    if (X) {
+        unsigned xm = keep;
+        if (B.valid[q]) {
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (!valid_at(B.valid[q], OXB_ROW(j))) xm &= ~(1u << j);
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (!((xm >> j) & 1u)) xv[j] = 0;
+        *xvalid = xm;
+    }
+#undef OXB_ROW
+    unsigned nk = keep & ~kvalid;
+#pragma unroll
+    for (int j = 0; j < R; j++)
+        if (((keep & kvalid) >> j) & 1u && key[j] == kEmptyKey) nk |= 1u << j;
+    *nullkey = nk;
+    return keep & ~nk;
+}
+
 // The one pass over the input before the fold: for the kept rows with a
 // valid key (not INT64_MIN), (1) HyperLogLog registers of their keys
 // (2^kHllBits registers: a key's register is the top bits of its partition
@@ -4146,6 +4235,31 @@ struct DensePlan {
     unsigned int* status;
 };
 
+// The columns a dense pass reads for partitioning tile t of batch B (the
+// key, every WHERE column and, when q >= 0, accumulator q's Int32 column),
+// prefetched into L2 while the CTA works on the tile before it.
+__device__ __forceinline__ void prefetch_tile(const DevPredicate& pred, const BatchCols& B, int key_type, long long t,
+                                              int q) {
+    const long long base = (t - B.ptile0) * kPartTile;
+    const long long n = B.n - base < kPartTile ? B.n - base : kPartTile;
+    if (n <= 0) return;
+    const int kw = type_width(key_type, 1);
+    prefetch_l2_range((const char*)B.key + base * kw, (unsigned long long)(n * kw));
+    for (int l = 0; l < pred.nleaves; l++) {
+        const int w = type_width(pred.leaves[l].type, 1);
+        prefetch_l2_range((const char*)B.lvals[l] + base * w, (unsigned long long)(n * w));
+    }
+    if (q >= 0) prefetch_l2_range((const char*)B.vals[q] + base * 4, (unsigned long long)(n * 4));
+}
+
+// Thread 0 prefetches tile t + 1 of the CTA's range [.., t1) (bi: tile t's batch).
+__device__ __forceinline__ void prefetch_next_tile(const DevPredicate& pred, const BatchCols* batches, int nb, int bi,
+                                                   int key_type, long long t, long long t1, int q) {
+    if (threadIdx.x != 0 || t + 1 >= t1) return;
+    while (bi + 1 < nb && batches[bi + 1].ptile0 <= t + 1) bi++;
+    prefetch_tile(pred, batches[bi], key_type, t + 1, q);
+}
+
 // A strided sample of the rows, spread over the partitioning tiles.
 // out[0] rows sampled, [1] rows the WHERE keeps, [2] and [3] the least and
 // greatest ordered key (key ^ sign bit) of the kept rows with a valid key.
@@ -4208,12 +4322,15 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_count_kernel(const _
     for (long long t = t0; t < t1; t++) {
         while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
         const BatchCols& B = batches[bi];
+        if (t == t0 && threadIdx.x == 0) prefetch_tile(pred, B, key_type, t, -1);
+        prefetch_next_tile(pred, batches, nb, bi, key_type, t, t1, -1);
         const long long base = (t - B.ptile0) * kPartTile;
         const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
         for (long long sub = base; sub < end; sub += kDenseSub) {
             long long key[kDenseRows];
             unsigned nk;
-            const unsigned m = kept_keys<kDenseRows, kDenseThreads>(pred, B, key_type, sub + threadIdx.x, end, key, &nk);
+            const unsigned m = kept_keys_eager<kDenseRows, kDenseThreads, false>(pred, B, key_type, sub + threadIdx.x,
+                                                                                end, key, &nk, 0, nullptr, nullptr);
 #pragma unroll
             for (int j = 0; j < kDenseRows; j++) {
                 if (!((m >> j) & 1u)) continue;
@@ -4311,30 +4428,30 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(cons
     for (long long t = t0; t < t1; t++) {
         while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
         const BatchCols& B = batches[bi];
+        if (t == t0 && threadIdx.x == 0) prefetch_tile(pred, B, key_type, t, dp.q);
+        prefetch_next_tile(pred, batches, nb, bi, key_type, t, t1, dp.q);
         const long long base = (t - B.ptile0) * kPartTile;
         const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
         for (long long sub = base; sub < end; sub += kDenseSub) {
             long long key[kDenseRows];
-            unsigned nk;
-            unsigned m = kept_keys<kDenseRows, kDenseThreads>(pred, B, key_type, sub + threadIdx.x, end, key, &nk);
+            int xv[kDenseRows];
+            unsigned nk, xvalid = 0;
+            unsigned m = kept_keys_eager<kDenseRows, kDenseThreads, true>(pred, B, key_type, sub + threadIdx.x, end, key,
+                                                                          &nk, dp.q, xv, &xvalid);
             uint2 rec[kDenseRows];
             unsigned pr[kDenseRows];
-            const int q = dp.q;
 #pragma unroll
             for (int j = 0; j < kDenseRows; j++) {
                 rec[j] = make_uint2(0u, 0u);
                 pr[j] = 0;
                 if (!((m >> j) & 1u)) continue;
-                const long long r = sub + threadIdx.x + (long long)j * kDenseThreads;
                 const unsigned long long rel = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
                 if (rel >= dp.span) {  // the count pass found none; never written out of range
                     atomicOr(dp.status, kStatusBounds);
                     m &= ~(1u << j);
                     continue;
                 }
-                const bool v = valid_at(B.valid[q], r);
-                const int x = v ? __ldg((const int*)B.vals[q] + r) : 0;
-                rec[j] = make_uint2((unsigned)x, (unsigned)rel << 1 | (v ? 1u : 0u));
+                rec[j] = make_uint2((unsigned)xv[j], (unsigned)rel << 1 | ((xvalid >> j) & 1u));
                 const unsigned p = (unsigned)(rel >> kDenseBits);
                 pr[j] = p << 16 | atomicAdd(&hist[p], 1u);
             }
@@ -4369,6 +4486,262 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(cons
     }
 }
 
+// The compiled form of the dense count and split passes, for the common
+// shape: no validity bitmap on the key or the WHERE columns, at most two
+// WHERE leaves, and every column of every batch starting on a 16-byte
+// boundary.  A thread takes four consecutive rows a load (one 128-bit load
+// of an Int32 column, two of a 64-bit one), so loads, index arithmetic and
+// loop overhead a row shrink fourfold, and each comparison is lean_cmp's
+// branch-free mask.  The rows a thread takes are quads g and g + kDenseThreads
+// of a sub-tile, so a warp's loads stay contiguous.
+struct DenseLean {
+    int nleaves;
+    int leaf_w8[2];   // the leaf's column is 64-bit (Int64 or Float64)
+    int leaf_f64[2];
+    int leaf_mask[2];
+    long long lit[2];
+};
+
+// The 64-bit values of rows 4g .. 4g+3 (below end; the others read 0).
+__device__ __forceinline__ void quad_load64(const void* col, long long g, long long end, long long v[4]) {
+    const long long r = 4 * g;
+    if (r + 4 <= end) {
+        const longlong2 a = __ldg((const longlong2*)col + 2 * g), b = __ldg((const longlong2*)col + 2 * g + 1);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = r + i < end ? __ldg((const long long*)col + r + i) : 0;
+    }
+}
+
+// The Int32 values of rows 4g .. 4g+3 (below end; the others read 0).
+__device__ __forceinline__ void quad_load32(const void* col, long long g, long long end, int v[4]) {
+    const long long r = 4 * g;
+    if (r + 4 <= end) {
+        const int4 a = __ldg((const int4*)col + g);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = a.z;
+        v[3] = a.w;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = r + i < end ? __ldg((const int*)col + r + i) : 0;
+    }
+}
+
+// Rows 4g .. 4g+3 for q in {0, 1}, g = g0 + q * kDenseThreads: their keys
+// (key[4q + i]) and a mask (bit 4q + i) of the live rows the WHERE keeps.
+// *minkey gets those whose key is INT64_MIN, left out of the mask.
+template <bool K8>
+__device__ __forceinline__ unsigned lean_rows(const DenseLean& L, const BatchCols& B, long long g0, long long end,
+                                              long long key[8], unsigned* minkey) {
+    unsigned live = 0;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const long long r = 4 * (g0 + q * kDenseThreads);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if (r + i < end) live |= 1u << (4 * q + i);
+    }
+    if (!live) {
+        *minkey = 0;
+        return 0;
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const long long g = g0 + q * kDenseThreads;
+        if (K8) {
+            quad_load64(B.key, g, end, key + 4 * q);
+        } else {
+            int k32[4];
+            quad_load32(B.key, g, end, k32);
+#pragma unroll
+            for (int i = 0; i < 4; i++) key[4 * q + i] = k32[i];
+        }
+    }
+    unsigned keep = live;
+#pragma unroll
+    for (int l = 0; l < 2; l++) {
+        if (l >= L.nleaves) break;
+        const void* col = B.lvals[l];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const long long g = g0 + q * kDenseThreads;
+            long long a[4];
+            if (L.leaf_w8[l]) {
+                quad_load64(col, g, end, a);
+                if (L.leaf_f64[l]) {
+#pragma unroll
+                    for (int i = 0; i < 4; i++) a[i] = filter_order_key(__longlong_as_double(a[i]));
+                }
+            } else {
+                int a32[4];
+                quad_load32(col, g, end, a32);
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i] = a32[i];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (!lean_cmp(L.leaf_mask[l], a[i], L.lit[l])) keep &= ~(1u << (4 * q + i));
+        }
+    }
+    unsigned mk = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        if (((keep >> j) & 1u) && key[j] == kEmptyKey) mk |= 1u << j;
+    *minkey = mk;
+    return keep & ~mk;
+}
+
+// The count pass, compiled (part_dense_count_kernel's contract).
+template <bool K8>
+__global__ void __launch_bounds__(kDenseThreads) part_dense_count_lean_kernel(const __grid_constant__ DenseLean L,
+                                                                              const BatchCols* __restrict__ batches,
+                                                                              int nb, long long ntiles,
+                                                                              const __grid_constant__ DensePlan dp,
+                                                                              unsigned long long* __restrict__ out) {
+    extern __shared__ unsigned int dhist[];
+    for (int i = threadIdx.x; i < dp.np; i += blockDim.x) dhist[i] = 0;
+    __syncthreads();
+    unsigned n = 0, outside = 0;
+    const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int bi = t0 < t1 ? batch_of_tile(batches, nb, t0) : 0;
+    for (long long t = t0; t < t1; t++) {
+        while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
+        const BatchCols& B = batches[bi];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
+        for (long long sub = base; sub < end; sub += kDenseSub) {
+            long long key[8];
+            unsigned mk;
+            const unsigned m = lean_rows<K8>(L, B, sub / 4 + threadIdx.x, end, key, &mk);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (!((m >> j) & 1u)) continue;
+                const unsigned long long rel = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
+                if (rel < dp.span) {
+                    atomicAdd(&dhist[rel >> kDenseBits], 1u);
+                    n++;
+                } else {
+                    outside++;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+        outside += __shfl_xor_sync(0xffffffffu, outside, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (n) atomicAdd(&out[0], (unsigned long long)n);
+        if (outside) atomicAdd(&out[1], (unsigned long long)outside);
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) dp.counts[(long long)p * gridDim.x + blockIdx.x] = dhist[p];
+}
+
+// The split, compiled (part_dense_split_kernel's contract; rows whose key
+// is INT64_MIN fold into their HBM slot).
+template <int MAXACC, bool K8>
+__global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel(
+    const __grid_constant__ AggProgram P, const __grid_constant__ DenseLean L, const BatchCols* __restrict__ batches,
+    int nb, long long ntiles, const __grid_constant__ DensePlan dp) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    uint2* srec = (uint2*)dsm;
+    unsigned* cursor = (unsigned*)(srec + kDenseSub);
+    unsigned* hist = cursor + dp.np;
+    unsigned* start = hist + dp.np;
+    unsigned short* spart = (unsigned short*)(start + dp.np);
+    __shared__ unsigned wsum[kDenseThreads / 32];
+    __shared__ unsigned s_total;
+    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
+        cursor[p] = (unsigned)dp.offs[(long long)p * gridDim.x + blockIdx.x];
+        hist[p] = 0;
+    }
+    __syncthreads();
+    const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int bi = t0 < t1 ? batch_of_tile(batches, nb, t0) : 0;
+    for (long long t = t0; t < t1; t++) {
+        while (bi + 1 < nb && batches[bi + 1].ptile0 <= t) bi++;
+        const BatchCols& B = batches[bi];
+        const long long base = (t - B.ptile0) * kPartTile;
+        const long long end = base + kPartTile < B.n ? base + kPartTile : B.n;
+        for (long long sub = base; sub < end; sub += kDenseSub) {
+            const long long g0 = sub / 4 + threadIdx.x;
+            // the carried values first, so they load with the keys and the WHERE columns
+            int xv[8];
+            unsigned xvalid = 0xFFu;
+            const uint8_t* xbits = B.valid[dp.q];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const long long g = g0 + q * kDenseThreads;
+                quad_load32(B.vals[dp.q], g, end, xv + 4 * q);
+                if (xbits && 4 * g < end)
+                    xvalid &= ~(0xFu << (4 * q)) | ((unsigned)(__ldg(xbits + ((4 * g) >> 3)) >> ((4 * g) & 7)) & 0xFu)
+                                                       << (4 * q);
+            }
+            unsigned rel[8], mk;
+            unsigned m;
+            {
+                long long key[8];
+                m = lean_rows<K8>(L, B, g0, end, key, &mk);
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const unsigned long long r64 = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
+                    rel[j] = (unsigned)r64;
+                    if (((m >> j) & 1u) && r64 >= dp.span) {  // the count pass found none; never written out of range
+                        atomicOr(dp.status, kStatusBounds);
+                        m &= ~(1u << j);
+                    }
+                }
+            }
+            unsigned pr[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                pr[j] = 0;
+                if (!((m >> j) & 1u)) continue;
+                const unsigned p = rel[j] >> kDenseBits;
+                pr[j] = p << 16 | atomicAdd(&hist[p], 1u);
+            }
+            if (mk) {
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if ((mk >> j) & 1u)
+                        part_null_row_to_hbm<MAXACC>(P, B, 4 * (g0 + (j >> 2) * kDenseThreads) + (j & 3));
+            }
+            __syncthreads();
+            block_exclusive_scan(hist, start, dp.np, wsum, &s_total);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                if (!((m >> j) & 1u)) continue;
+                const unsigned p = pr[j] >> 16;
+                const unsigned sidx = start[p] + (pr[j] & 0xFFFFu);
+                const unsigned v = (xvalid >> j) & 1u;
+                srec[sidx] = make_uint2(v ? (unsigned)xv[j] : 0u, rel[j] << 1 | v);
+                spart[sidx] = (unsigned short)p;
+            }
+            __syncthreads();
+            const unsigned total = s_total;
+            for (unsigned sidx = threadIdx.x; sidx < total; sidx += blockDim.x) {
+                const unsigned p = spart[sidx];
+                const unsigned long long pos = (unsigned long long)cursor[p] + (sidx - start[p]);
+                if (pos < dp.nrecs) dp.recs[pos] = srec[sidx];
+                else atomicOr(dp.status, kStatusBounds);
+            }
+            __syncthreads();
+            for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
+                cursor[p] += hist[p];
+                hist[p] = 0;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // Slots [capacity] (the NULL group) and [capacity + 1] (the key INT64_MIN)
 // of every array: the only HBM slots the dense path folds into with atomics.
 __global__ void dense_special_init_kernel(const __grid_constant__ AggProgram P) {
@@ -4379,14 +4752,15 @@ __global__ void dense_special_init_kernel(const __grid_constant__ AggProgram P) 
 }
 
 size_t dense_fold_smem(int ops) {
-    int arrays = 1 + ((ops & 1) ? 1 : 0) + ((ops & 2) ? 2 : 0) + ((ops & 4) ? 1 : 0) + ((ops & 8) ? 1 : 0);
+    int arrays = 2 + ((ops & 2) ? 2 : 0) + ((ops & 4) ? 1 : 0) + ((ops & 8) ? 1 : 0);
     return (size_t)arrays * kDenseKeys * 4;
 }
 
 // The fold, one partition a CTA at a time, into a shared table indexed by
-// the key's offset: 32-bit shared atomics only (the row count, COUNT, the
-// Int64 SUM as a 32-bit add and its carry, and MIN and MAX, each of those
-// two only after a plain read shows the value would change it).  The
+// the key's offset: 32-bit shared atomics only (the rows with a NULL value
+// or else the rows with a value, which is COUNT; the Int64 SUM as a 32-bit
+// add and its carry; MIN and MAX, each only after a plain read shows the
+// value would change it), so one counting atomic a record.  The
 // partition's groups then go to the HBM table compacted and in key order,
 // at the partition's own slots [p * kDenseKeys, ...), and their number to
 // gcount[p].  OPS: bit 0 COUNT, 1 SUM, 2 MIN, 3 MAX (CompactOps).
@@ -4396,9 +4770,9 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
                                                                                const __grid_constant__ CompactOps ops,
                                                                                unsigned int* __restrict__ gcount) {
     extern __shared__ __align__(16) unsigned int fsm[];
-    unsigned* rows = fsm;
-    unsigned* cnt = rows + kDenseKeys;
-    unsigned* slo = cnt + ((OPS & 1) ? kDenseKeys : 0);
+    unsigned* nul = fsm;                // rows whose value is NULL
+    unsigned* cnt = nul + kDenseKeys;   // rows whose value is not: a group's rows are their sum
+    unsigned* slo = cnt + kDenseKeys;
     unsigned* shi = slo + ((OPS & 2) ? kDenseKeys : 0);
     int* mn = (int*)(shi + ((OPS & 2) ? kDenseKeys : 0));
     int* mx = mn + ((OPS & 4) ? kDenseKeys : 0);
@@ -4409,8 +4783,8 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
     const long long st = P.stride;
     for (int part = blockIdx.x; part < dp.np; part += gridDim.x) {
         for (int i = threadIdx.x; i < kDenseKeys; i += blockDim.x) {
-            rows[i] = 0;
-            if (OPS & 1) cnt[i] = 0;
+            nul[i] = 0;
+            cnt[i] = 0;
             if (OPS & 2) {
                 slo[i] = 0;
                 shi[i] = 0;
@@ -4431,10 +4805,12 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
             for (int j = 0; j < kInFlight; j++) {
                 if (b0 + (unsigned long long)j * kDenseFoldThreads >= hi) break;
                 const unsigned off = (rec[j].y >> 1) & (unsigned)(kDenseKeys - 1);
-                atomicAdd(&rows[off], 1u);
-                if (!(rec[j].y & 1u)) continue;  // a NULL value: the row counts, nothing else
+                if (!(rec[j].y & 1u)) {  // a NULL value: the row counts, nothing else
+                    atomicAdd(&nul[off], 1u);
+                    continue;
+                }
                 const int x = (int)rec[j].x;
-                if (OPS & 1) atomicAdd(&cnt[off], 1u);
+                atomicAdd(&cnt[off], 1u);
                 if (OPS & 2) {
                     // x sign-extended to 64 bits: a 32-bit add and its carry
                     const unsigned vlo = (unsigned)x, vhi = x < 0 ? 0xffffffffu : 0u;
@@ -4454,7 +4830,7 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
         const int s0 = threadIdx.x * kPer;
         unsigned c = 0;
 #pragma unroll
-        for (int k = 0; k < kPer; k++) c += rows[s0 + k] != 0u ? 1u : 0u;
+        for (int k = 0; k < kPer; k++) c += (nul[s0 + k] | cnt[s0 + k]) != 0u ? 1u : 0u;
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
         unsigned inc = c;
 #pragma unroll
@@ -4481,7 +4857,7 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
             const int sl = s0 + k;
-            const unsigned nrows = rows[sl];
+            const unsigned nrows = nul[sl] + cnt[sl];
             if (!nrows) continue;
             P.keys[g] = (long long)((kbase + (unsigned long long)sl) ^ kSignBit);
             P.arr[g] = nrows;
@@ -5244,9 +5620,36 @@ oxb_batch* emit_dense(const StreamRef& s, const Backend& b, const AggPlan& plan,
 // COUNT(*) beside them), the kept keys span at most 2^25 values, and, unless
 // pinned (variant 17), enough rows are kept for the passes to pay.  nullptr
 // otherwise, and the caller takes the direct or hashed passes.
+// The compiled dense passes apply (DenseLean): no bitmap on the key or a
+// WHERE column in any batch, at most two leaves, 16-byte aligned columns.
+bool dense_lean_plan(const DevPredicate& pred, const std::vector<BatchCols>& hb, int q, DenseLean* L) {
+    if (pred.nleaves > 2) return false;
+    *L = DenseLean{};
+    L->nleaves = pred.nleaves;
+    static const int kMask[5] = {2, 1, 3, 4, 6};  // ==, <, <=, >, >= (cmp_holds' codes)
+    for (int l = 0; l < pred.nleaves; l++) {
+        const DevLeaf& lf = pred.leaves[l];
+        if (lf.type != kInt32 && lf.type != kInt64 && lf.type != kFloat64) return false;
+        L->leaf_w8[l] = lf.type != kInt32;
+        L->leaf_f64[l] = lf.type == kFloat64;
+        L->leaf_mask[l] = kMask[lf.op < 0 || lf.op > 4 ? 4 : lf.op];
+        L->lit[l] = lf.lit;
+    }
+    auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+    for (const BatchCols& c : hb) {
+        if (c.n == 0) continue;
+        if (c.key_valid || !aligned(c.key) || !aligned(c.vals[q])) return false;
+        for (int l = 0; l < pred.nleaves; l++)
+            if (c.lvalid[l] || !aligned(c.lvals[l])) return false;
+    }
+    return true;
+}
+
 oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& plan, AggProgram P,
-                           const DevPredicate& pred, int key_type, const BatchCols* dbatches, int nb,
-                           long long nptiles, long long total, const int* acc_col, KernelTimer& timer) {
+                           const DevPredicate& pred, int key_type, const BatchCols* dbatches,
+                           const std::vector<BatchCols>& hb, long long nptiles, long long total, const int* acc_col,
+                           KernelTimer& timer) {
+    const int nb = (int)hb.size();
     const bool pinned = b.force_combine == 17;
     if (b.force_combine >= 0 && !pinned) return nullptr;
     if (nptiles == 0 || total >= (1ll << 32) || P.nacc < 1 || P.nacc > 4) return nullptr;
@@ -5289,9 +5692,18 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
     Scratch<unsigned int> counts(s, (size_t)np * dp.grid);
     Scratch<unsigned long long> cnt_out(s, 2, true);
     dp.counts = counts.get();
+    DenseLean L;
+    const bool lean = dense_lean_plan(pred, hb, dp.q, &L);
+    const bool k8 = key_type == kInt64;
     timer.begin();
-    note_launch(), part_dense_count_kernel<<<dp.grid, kDenseThreads, (size_t)np * 4, s->stream>>>(
-        pred, key_type, dbatches, nb, nptiles, dp, cnt_out.get());
+    if (lean) {
+        auto count = k8 ? part_dense_count_lean_kernel<true> : part_dense_count_lean_kernel<false>;
+        note_launch(), count<<<dp.grid, kDenseThreads, (size_t)np * 4, s->stream>>>(L, dbatches, nb, nptiles, dp,
+                                                                                    cnt_out.get());
+    } else {
+        note_launch(), part_dense_count_kernel<<<dp.grid, kDenseThreads, (size_t)np * 4, s->stream>>>(
+            pred, key_type, dbatches, nb, nptiles, dp, cnt_out.get());
+    }
     OXB_CUDA(cudaGetLastError());
     timer.end();
     unsigned long long hc[2] = {0, 0};
@@ -5323,15 +5735,21 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
 
     const int maxacc = maxacc_for(P.nacc);
     auto split = maxacc == 2 ? part_dense_split_kernel<2> : part_dense_split_kernel<4>;
+    auto split_lean = maxacc == 2 ? (k8 ? part_dense_split_lean_kernel<2, true> : part_dense_split_lean_kernel<2, false>)
+                                  : (k8 ? part_dense_split_lean_kernel<4, true> : part_dense_split_lean_kernel<4, false>);
     const size_t ssmem = dense_split_smem(np);
     set_smem(split, ssmem);
+    set_smem(split_lean, ssmem);
     DenseFold fold = dense_fold_for(mask);
     const size_t fsmem = dense_fold_smem(mask);
     set_smem(fold, fsmem);
     timer.rename("agg_batches_dense");
     timer.begin();
     note_launch(), dense_special_init_kernel<<<1, 64, 0, s->stream>>>(P);
-    note_launch(), split<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, pred, key_type, dbatches, nb, nptiles, dp);
+    if (lean)
+        note_launch(), split_lean<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, L, dbatches, nb, nptiles, dp);
+    else
+        note_launch(), split<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, pred, key_type, dbatches, nb, nptiles, dp);
     note_launch(), fold<<<std::min(np, b.sms), kDenseFoldThreads, fsmem, s->stream>>>(P, dp, ops, gcount.get());
     OXB_CUDA(cudaGetLastError());
     timer.end();
@@ -5408,8 +5826,8 @@ oxb_batch* aggregate_batches(const StreamRef& s, const Backend& b, const oxb_agg
     // One pass over the input: distinct keys and count of the kept rows, and
     // their fine partition histogram (KernelTimer: this pass plus the fold).
     KernelTimer timer(b, s, "agg_batches_kernel");
-    if (oxb_batch* out = aggregate_dense(s, b, plan, P, pred, key.type, dbatches.get(), a.ninputs, nptiles, total,
-                                         acc_col, timer))
+    if (oxb_batch* out = aggregate_dense(s, b, plan, P, pred, key.type, dbatches.get(), hb, nptiles, total, acc_col,
+                                         timer))
         return out;
     Scratch<unsigned> regs(s, kHllRegs, true);
     Scratch<unsigned int> fine(s, kFine, true);

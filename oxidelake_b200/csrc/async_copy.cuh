@@ -80,6 +80,20 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsign
         : "memory");
 }
 
+// Asks the TMA unit to bring [p, p + bytes) from HBM into L2, with nothing
+// written to shared memory and nothing to wait on.  The range is rounded
+// inward to 16-byte boundaries (as the bulk copy requires), so no byte
+// outside it is touched; it goes in pieces of at most 64 KB.
+__device__ __forceinline__ void prefetch_l2_range(const void* p, unsigned long long bytes) {
+    unsigned long long a = ((unsigned long long)p + 15ull) & ~15ull;
+    const unsigned long long e = ((unsigned long long)p + bytes) & ~15ull;
+    while (a < e) {
+        const unsigned n = (unsigned)(e - a < 65536ull ? e - a : 65536ull);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+        a += n;
+    }
+}
+
 __device__ __forceinline__ int4 ld_keep_v4(const void* p, unsigned long long policy) {
     int4 v;
     asm volatile("ld.global.nc.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"

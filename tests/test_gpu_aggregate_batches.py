@@ -10,7 +10,7 @@ import oracle
 from compare import abs_columns, assert_batches_equal
 from datagen import config3_batches
 from oxidelake_b200.params import AggregateFunction as F
-from oxidelake_b200.params import AggregateSpec, Literal, compare, leaves
+from oxidelake_b200.params import AggregateSpec, Literal, and_, compare, leaves
 from oxidelake_b200.params import Comparison as Cmp
 
 pytestmark = pytest.mark.gpu
@@ -280,5 +280,33 @@ def test_dense_range_outlier_keys_fall_back(backend, stream):
     got, name = _fold_named(backend, stream, batches, SPEC, None, 17)
     assert name != "agg_batches_dense", name
     _, w = want(batches, SPEC, None)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_two_leaf_where(backend, stream):
+    """A WHERE of a Float64 and an Int64 leaf (signed zeros, NaN and
+    infinities in the Float64 column) through the compiled dense passes:
+    four rows a load, the comparisons as masks; ragged batch ends."""
+    rng = np.random.default_rng(77)
+    batches = []
+    for n in (131_071, 5, 262_147, 40_001):
+        g = rng.integers(-500_000, 500_000, n).astype(np.int64)
+        x = rng.integers(-(2**31), 2**31 - 1, n, dtype=np.int64).astype(np.int32)
+        v = rng.uniform(-1, 1, n)
+        if n > 10:
+            v[:6] = [np.nan, -0.0, 0.0, np.inf, -np.inf, 0.25]
+        w = rng.integers(0, 100, n).astype(np.int64)
+        batches.append(
+            pa.RecordBatch.from_arrays(
+                [pa.array(g), pa.array(x, mask=rng.random(n) < 0.03), pa.array(v), pa.array(w)],
+                names=["g", "x", "v", "w"],
+            )
+        )
+    pred = and_(compare(2, Cmp.GtEq, Literal.float64(-0.0)), compare(3, Cmp.LtEq, Literal.int64(50)))
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Min, 1), (F.Max, 1), (F.Count, 1), (F.CountStar, 0)])
+    got, name = _fold_named(backend, stream, batches, spec, pred, 17)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, spec, pred)
     assert got.num_rows == w.num_rows
     assert_batches_equal(got, w)
