@@ -4219,18 +4219,25 @@ constexpr int kDenseRows = 8;               // rows a thread in a split sub-tile
 constexpr int kDenseSub = kDenseThreads * kDenseRows;
 constexpr int kDenseFoldThreads = 1024;
 constexpr int kDenseSamples = 16384;
+constexpr int kDenseFanBits = 4;  // final partitions a first-level partition
+constexpr int kDenseFan = 1 << kDenseFanBits;
+constexpr int kDenseChunk = 4096;  // records a chunk of the second split
 constexpr unsigned long long kSignBit = 0x8000000000000000ull;
 static_assert(kDenseSub <= 65536 && kDenseMaxParts <= 65536, "ranks and partitions pack into 16 bits each");
 
 struct DensePlan {
     unsigned long long lo;    // the range's low end as an ordered key (key ^ sign bit)
     unsigned long long span;  // keys in the range: np * kDenseKeys
-    int np;                   // partitions
-    int grid;                 // CTAs of the count and split passes (the same tile ranges)
+    int np;                   // final partitions (the fold's)
+    int np1;                  // first-level partitions: kDenseFan final partitions each
+    int grid;                 // CTAs of the count and first split passes (the same tile ranges)
     int q;                    // the accumulator whose Int32 column the records carry
-    unsigned int* counts;     // [np][grid]: kept rows a partition and CTA
-    const unsigned long long* offs;  // their exclusive scan, [np * grid + 1]
-    uint2* recs;              // records: the value, offset << 1 | validity
+    unsigned int* counts1;    // [np1][grid]: kept rows a first-level partition and CTA
+    unsigned int* totals;     // [np]: kept rows a final partition
+    const unsigned long long* offs1;  // exclusive scan of counts1, [np1 * grid + 1]
+    const unsigned long long* offs;   // exclusive scan of totals, [np + 1]
+    uint2* recs1;             // records by first-level partition: the value, offset << 1 | validity
+    uint2* recs;              // the same records by final partition
     unsigned long long nrecs;
     unsigned int* status;
 };
@@ -4302,9 +4309,21 @@ __global__ void part_dense_sample_kernel(const __grid_constant__ DevPredicate pr
     }
 }
 
-// The count pass, over a contiguous range of tiles a CTA (the split takes
-// the same ranges): the kept rows with a valid key in each partition, stored
-// as counts[p * grid + cta].  out[0] gets their number, out[1] the number of
+// The end of a count pass: the CTA's kept rows per first-level partition
+// (its slice of each), and its share of every final partition's total.
+__device__ __forceinline__ void dense_count_store(const DensePlan& dp, const unsigned* dhist) {
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) {
+        unsigned n = 0;
+        for (int p = k << kDenseFanBits; p < ((k + 1) << kDenseFanBits) && p < dp.np; p++) n += dhist[p];
+        dp.counts1[(long long)k * gridDim.x + blockIdx.x] = n;
+    }
+    for (int p = threadIdx.x; p < dp.np; p += blockDim.x)
+        if (dhist[p]) atomicAdd(&dp.totals[p], dhist[p]);
+}
+
+// The count pass, over a contiguous range of tiles a CTA (the first split
+// takes the same ranges): the kept rows with a valid key in each partition
+// (dense_count_store).  out[0] gets their number, out[1] the number of
 // kept rows whose key falls outside the range (the host then takes the
 // hashed passes instead).
 __global__ void __launch_bounds__(kDenseThreads) part_dense_count_kernel(const __grid_constant__ DevPredicate pred,
@@ -4354,7 +4373,7 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_count_kernel(const _
         if (outside) atomicAdd(&out[1], (unsigned long long)outside);
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) dp.counts[(long long)p * gridDim.x + blockIdx.x] = dhist[p];
+    dense_count_store(dp, dhist);
 }
 
 // Exclusive scan of in[0, n) into out[0, n) by the whole block (a multiple
@@ -4396,12 +4415,53 @@ __device__ void block_exclusive_scan(const unsigned* in, unsigned* out, int n, u
     __syncthreads();
 }
 
-size_t dense_split_smem(int np) { return (size_t)kDenseSub * (8 + 2) + (size_t)np * 12; }
+// A sub-tile's records staged in shared memory, ordered by first-level
+// partition, so that each partition's run reaches HBM as whole 32-byte
+// sectors: a sector written in part is first filled from DRAM by L2, which
+// (measured) doubled the split's DRAM reads when each row was stored alone.
+struct DenseStage {
+    uint2* rec;             // kDenseSub records, by partition
+    unsigned* cursor;       // np1: the CTA's next record in each first-level partition
+    unsigned* hist;         // np1: the sub-tile's records a partition
+    unsigned* start;        // np1: their exclusive scan
+    unsigned short* part;   // kDenseSub: each ordered record's partition
+};
 
-// The split, over the count pass's tile ranges.  Each sub-tile of kDenseSub
-// rows ranks its kept rows per partition in shared memory, orders their
-// records by partition there, and stores each partition's run at the CTA's
-// own cursor into that partition.  Kept rows whose key is NULL or INT64_MIN
+size_t dense_split_smem(int np1) { return (size_t)kDenseSub * (8 + 2) + (size_t)np1 * 12; }
+
+__device__ __forceinline__ DenseStage dense_stage(unsigned char* smem, int np1) {
+    DenseStage st;
+    st.rec = (uint2*)smem;
+    st.cursor = (unsigned*)(st.rec + kDenseSub);
+    st.hist = st.cursor + np1;
+    st.start = st.hist + np1;
+    st.part = (unsigned short*)(st.start + np1);
+    return st;
+}
+
+// After the records are ordered (and a barrier): each partition's run to
+// the CTA's cursor into it, consecutive threads on consecutive records; then
+// the cursors advance and the counts clear.  Ends synchronised.
+__device__ __forceinline__ void dense_stage_store(const DenseStage& st, const DensePlan& dp, unsigned total) {
+    for (unsigned sidx = threadIdx.x; sidx < total; sidx += blockDim.x) {
+        const unsigned k = st.part[sidx];
+        const unsigned long long pos = (unsigned long long)st.cursor[k] + (sidx - st.start[k]);
+        if (pos < dp.nrecs) dp.recs1[pos] = st.rec[sidx];
+        else atomicOr(dp.status, kStatusBounds);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) {
+        st.cursor[k] += st.hist[k];
+        st.hist[k] = 0;
+    }
+    __syncthreads();
+}
+
+// The first split, over the count pass's tile ranges: each sub-tile of
+// kDenseSub rows ranks its kept rows per first-level partition (kDenseFan
+// final partitions each) in shared memory, orders their records there, and
+// stores each partition's run at the CTA's own cursor into it (the CTA's
+// slice, from the count pass).  Kept rows whose key is NULL or INT64_MIN
 // fold straight into their HBM slots.
 template <int MAXACC>
 __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(const __grid_constant__ AggProgram P,
@@ -4411,16 +4471,12 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(cons
                                                                             int nb, long long ntiles,
                                                                             const __grid_constant__ DensePlan dp) {
     extern __shared__ __align__(16) unsigned char dsm[];
-    uint2* srec = (uint2*)dsm;                         // kDenseSub records, by partition
-    unsigned* cursor = (unsigned*)(srec + kDenseSub);  // np: the CTA's next record in each partition
-    unsigned* hist = cursor + dp.np;                   // np: the sub-tile's records a partition
-    unsigned* start = hist + dp.np;                    // np: their exclusive scan
-    unsigned short* spart = (unsigned short*)(start + dp.np);  // kDenseSub: each ordered record's partition
+    DenseStage st = dense_stage(dsm, dp.np1);
     __shared__ unsigned wsum[kDenseThreads / 32];
     __shared__ unsigned s_total;
-    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
-        cursor[p] = (unsigned)dp.offs[(long long)p * gridDim.x + blockIdx.x];
-        hist[p] = 0;
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) {
+        st.cursor[k] = (unsigned)dp.offs1[(long long)k * gridDim.x + blockIdx.x];
+        st.hist[k] = 0;
     }
     __syncthreads();
     const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
@@ -4438,50 +4494,36 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(cons
             unsigned nk, xvalid = 0;
             unsigned m = kept_keys_eager<kDenseRows, kDenseThreads, true>(pred, B, key_type, sub + threadIdx.x, end, key,
                                                                           &nk, dp.q, xv, &xvalid);
-            uint2 rec[kDenseRows];
-            unsigned pr[kDenseRows];
+            unsigned rel[kDenseRows], pr[kDenseRows];
 #pragma unroll
             for (int j = 0; j < kDenseRows; j++) {
-                rec[j] = make_uint2(0u, 0u);
                 pr[j] = 0;
+                const unsigned long long r64 = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
+                rel[j] = (unsigned)r64;
                 if (!((m >> j) & 1u)) continue;
-                const unsigned long long rel = ((unsigned long long)key[j] ^ kSignBit) - dp.lo;
-                if (rel >= dp.span) {  // the count pass found none; never written out of range
+                if (r64 >= dp.span) {  // the count pass found none; never written out of range
                     atomicOr(dp.status, kStatusBounds);
                     m &= ~(1u << j);
                     continue;
                 }
-                rec[j] = make_uint2((unsigned)xv[j], (unsigned)rel << 1 | ((xvalid >> j) & 1u));
-                const unsigned p = (unsigned)(rel >> kDenseBits);
-                pr[j] = p << 16 | atomicAdd(&hist[p], 1u);
+                const unsigned k = rel[j] >> (kDenseBits + kDenseFanBits);
+                pr[j] = k << 16 | atomicAdd(&st.hist[k], 1u);
             }
 #pragma unroll
             for (int j = 0; j < kDenseRows; j++)
                 if ((nk >> j) & 1u) part_null_row_to_hbm<MAXACC>(P, B, sub + threadIdx.x + (long long)j * kDenseThreads);
             __syncthreads();
-            block_exclusive_scan(hist, start, dp.np, wsum, &s_total);
+            block_exclusive_scan(st.hist, st.start, dp.np1, wsum, &s_total);
 #pragma unroll
             for (int j = 0; j < kDenseRows; j++) {
                 if (!((m >> j) & 1u)) continue;
-                const unsigned p = pr[j] >> 16;
-                const unsigned sidx = start[p] + (pr[j] & 0xFFFFu);
-                srec[sidx] = rec[j];
-                spart[sidx] = (unsigned short)p;
+                const unsigned k = pr[j] >> 16;
+                const unsigned sidx = st.start[k] + (pr[j] & 0xFFFFu);
+                st.rec[sidx] = make_uint2((unsigned)xv[j], rel[j] << 1 | ((xvalid >> j) & 1u));
+                st.part[sidx] = (unsigned short)k;
             }
             __syncthreads();
-            const unsigned total = s_total;
-            for (unsigned sidx = threadIdx.x; sidx < total; sidx += blockDim.x) {
-                const unsigned p = spart[sidx];
-                const unsigned long long pos = (unsigned long long)cursor[p] + (sidx - start[p]);
-                if (pos < dp.nrecs) dp.recs[pos] = srec[sidx];
-                else atomicOr(dp.status, kStatusBounds);
-            }
-            __syncthreads();
-            for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
-                cursor[p] += hist[p];
-                hist[p] = 0;
-            }
-            __syncthreads();
+            dense_stage_store(st, dp, s_total);
         }
     }
 }
@@ -4641,26 +4683,22 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_count_lean_kernel(co
         if (outside) atomicAdd(&out[1], (unsigned long long)outside);
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) dp.counts[(long long)p * gridDim.x + blockIdx.x] = dhist[p];
+    dense_count_store(dp, dhist);
 }
 
-// The split, compiled (part_dense_split_kernel's contract; rows whose key
-// is INT64_MIN fold into their HBM slot).
+// The first split, compiled (part_dense_split_kernel's contract; rows
+// whose key is INT64_MIN fold into their HBM slot).
 template <int MAXACC, bool K8>
 __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DenseLean L, const BatchCols* __restrict__ batches,
     int nb, long long ntiles, const __grid_constant__ DensePlan dp) {
     extern __shared__ __align__(16) unsigned char dsm[];
-    uint2* srec = (uint2*)dsm;
-    unsigned* cursor = (unsigned*)(srec + kDenseSub);
-    unsigned* hist = cursor + dp.np;
-    unsigned* start = hist + dp.np;
-    unsigned short* spart = (unsigned short*)(start + dp.np);
+    DenseStage st = dense_stage(dsm, dp.np1);
     __shared__ unsigned wsum[kDenseThreads / 32];
     __shared__ unsigned s_total;
-    for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
-        cursor[p] = (unsigned)dp.offs[(long long)p * gridDim.x + blockIdx.x];
-        hist[p] = 0;
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) {
+        st.cursor[k] = (unsigned)dp.offs1[(long long)k * gridDim.x + blockIdx.x];
+        st.hist[k] = 0;
     }
     __syncthreads();
     const long long t0 = ntiles * blockIdx.x / gridDim.x, t1 = ntiles * (blockIdx.x + 1) / gridDim.x;
@@ -4684,8 +4722,7 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel
                     xvalid &= ~(0xFu << (4 * q)) | ((unsigned)(__ldg(xbits + ((4 * g) >> 3)) >> ((4 * g) & 7)) & 0xFu)
                                                        << (4 * q);
             }
-            unsigned rel[8], mk;
-            unsigned m;
+            unsigned rel[8], mk, m;
             {
                 long long key[8];
                 m = lean_rows<K8>(L, B, g0, end, key, &mk);
@@ -4704,8 +4741,9 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel
             for (int j = 0; j < 8; j++) {
                 pr[j] = 0;
                 if (!((m >> j) & 1u)) continue;
-                const unsigned p = rel[j] >> kDenseBits;
-                pr[j] = p << 16 | atomicAdd(&hist[p], 1u);
+                const unsigned k = rel[j] >> (kDenseBits + kDenseFanBits);
+                pr[j] = k << 16 | atomicAdd(&st.hist[k], 1u);
+                xv[j] = ((xvalid >> j) & 1u) ? xv[j] : 0;
             }
             if (mk) {
 #pragma unroll
@@ -4714,31 +4752,124 @@ __global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel
                         part_null_row_to_hbm<MAXACC>(P, B, 4 * (g0 + (j >> 2) * kDenseThreads) + (j & 3));
             }
             __syncthreads();
-            block_exclusive_scan(hist, start, dp.np, wsum, &s_total);
+            block_exclusive_scan(st.hist, st.start, dp.np1, wsum, &s_total);
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 if (!((m >> j) & 1u)) continue;
-                const unsigned p = pr[j] >> 16;
-                const unsigned sidx = start[p] + (pr[j] & 0xFFFFu);
-                const unsigned v = (xvalid >> j) & 1u;
-                srec[sidx] = make_uint2(v ? (unsigned)xv[j] : 0u, rel[j] << 1 | v);
-                spart[sidx] = (unsigned short)p;
+                const unsigned k = pr[j] >> 16;
+                const unsigned sidx = st.start[k] + (pr[j] & 0xFFFFu);
+                st.rec[sidx] = make_uint2((unsigned)xv[j], rel[j] << 1 | ((xvalid >> j) & 1u));
+                st.part[sidx] = (unsigned short)k;
             }
             __syncthreads();
-            const unsigned total = s_total;
-            for (unsigned sidx = threadIdx.x; sidx < total; sidx += blockDim.x) {
-                const unsigned p = spart[sidx];
-                const unsigned long long pos = (unsigned long long)cursor[p] + (sidx - start[p]);
-                if (pos < dp.nrecs) dp.recs[pos] = srec[sidx];
-                else atomicOr(dp.status, kStatusBounds);
-            }
-            __syncthreads();
-            for (int p = threadIdx.x; p < dp.np; p += blockDim.x) {
-                cursor[p] += hist[p];
-                hist[p] = 0;
-            }
-            __syncthreads();
+            dense_stage_store(st, dp, s_total);
         }
+    }
+}
+
+// The first chunk of each first-level partition's records (kDenseChunk a
+// chunk) and, at [np1], their total: one thread, np1 is small.
+__global__ void dense_chunks_kernel(const __grid_constant__ DensePlan dp, long long* __restrict__ cstart) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    long long c = 0;
+    for (int k = 0; k < dp.np1; k++) {
+        cstart[k] = c;
+        const unsigned long long n = dp.offs1[(long long)(k + 1) * dp.grid] - dp.offs1[(long long)k * dp.grid];
+        c += (long long)((n + kDenseChunk - 1) / kDenseChunk);
+    }
+    cstart[dp.np1] = c;
+}
+
+// Each final partition's next record in the second split: its start.
+__global__ void dense_cursor_kernel(const __grid_constant__ DensePlan dp, unsigned int* __restrict__ gcursor) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < dp.np; p += gridDim.x * blockDim.x)
+        gcursor[p] = (unsigned)dp.offs[p];
+}
+
+// The second split: chunks of one first-level partition's records from a
+// queue, each spread over its kDenseFan final partitions.  A record's rank
+// among the chunk's records of its final partition comes from a warp-wide
+// match and one shared atomic a group; the chunk then reserves each final
+// partition's run with one global atomic, and the records are stored from
+// shared memory in run order (runs of about kDenseChunk / kDenseFan records,
+// whole sectors).
+constexpr int kSplit2Rows = kDenseChunk / kDenseThreads;
+__global__ void __launch_bounds__(kDenseThreads) part_dense_split2_kernel(const __grid_constant__ DensePlan dp,
+                                                                          const long long* __restrict__ cstart,
+                                                                          unsigned long long* __restrict__ queue,
+                                                                          unsigned int* __restrict__ gcursor) {
+    __shared__ unsigned hist[kDenseFan], gbase[kDenseFan], start[kDenseFan];
+    __shared__ __align__(16) uint2 srec[kDenseChunk];
+    __shared__ long long s_c;
+    const int lane = threadIdx.x & 31;
+    const long long nchunks = cstart[dp.np1];
+    for (;;) {
+        if (threadIdx.x < kDenseFan) hist[threadIdx.x] = 0;
+        if (threadIdx.x == 0) s_c = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const long long c = s_c;
+        if (c >= nchunks) break;
+        int a = 0, b = dp.np1 - 1;  // the first-level partition holding chunk c
+        while (a < b) {
+            const int mid = (a + b + 1) >> 1;
+            if (cstart[mid] <= c) a = mid;
+            else b = mid - 1;
+        }
+        const unsigned long long r0 = dp.offs1[(long long)a * dp.grid] + (unsigned long long)(c - cstart[a]) * kDenseChunk;
+        const unsigned long long rend = dp.offs1[(long long)(a + 1) * dp.grid];
+        uint2 rec[kSplit2Rows];
+        unsigned rank[kSplit2Rows];
+#pragma unroll
+        for (int j = 0; j < kSplit2Rows; j++) {
+            const unsigned long long i = r0 + threadIdx.x + (unsigned long long)j * kDenseThreads;
+            rec[j] = i < rend && i < r0 + kDenseChunk ? __ldcs(dp.recs1 + i) : make_uint2(0u, 0xFFFFFFFFu);
+        }
+#pragma unroll
+        for (int j = 0; j < kSplit2Rows; j++) {
+            const unsigned long long i = r0 + threadIdx.x + (unsigned long long)j * kDenseThreads;
+            const bool live = i < rend && i < r0 + kDenseChunk;
+            // a lane without a record matches no other (a tag of its own above the bins)
+            const unsigned bin = live ? ((rec[j].y >> (1 + kDenseBits)) & (kDenseFan - 1)) : (unsigned)(kDenseFan + lane);
+            const unsigned peers = __match_any_sync(0xffffffffu, bin);
+            const int leader = __ffs(peers) - 1;
+            unsigned base = 0;
+            if (live && lane == leader) base = atomicAdd(&hist[bin], (unsigned)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // the runs' places in shared memory and in HBM
+            const unsigned h = threadIdx.x < kDenseFan ? hist[threadIdx.x] : 0u;
+            unsigned inc = h;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (threadIdx.x < kDenseFan) {
+                start[threadIdx.x] = inc - h;
+                if (h) gbase[threadIdx.x] = atomicAdd(&gcursor[(a << kDenseFanBits) + threadIdx.x], h);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSplit2Rows; j++) {
+            const unsigned long long i = r0 + threadIdx.x + (unsigned long long)j * kDenseThreads;
+            if (!(i < rend && i < r0 + kDenseChunk)) continue;
+            const unsigned bin = (rec[j].y >> (1 + kDenseBits)) & (kDenseFan - 1);
+            srec[start[bin] + rank[j]] = rec[j];
+        }
+        __syncthreads();
+        // consecutive threads store consecutive records of a run: whole sectors
+        const unsigned n = (unsigned)((rend < r0 + kDenseChunk ? rend : r0 + kDenseChunk) - r0);
+        for (unsigned sidx = threadIdx.x; sidx < n; sidx += blockDim.x) {
+            const uint2 r = srec[sidx];
+            const unsigned bin = (r.y >> (1 + kDenseBits)) & (kDenseFan - 1);
+            const unsigned long long pos = (unsigned long long)gbase[bin] + (sidx - start[bin]);
+            if (pos < dp.nrecs) dp.recs[pos] = r;
+            else atomicOr(dp.status, kStatusBounds);
+        }
+        __syncthreads();
     }
 }
 
@@ -4779,7 +4910,7 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
     __shared__ unsigned wsum[32];
     __shared__ unsigned s_total;
     constexpr int kPer = kDenseKeys / kDenseFoldThreads;  // slots a thread in the flush
-    constexpr int kInFlight = 4;                            // records a thread loads together
+    constexpr int kInFlight = 4;                            // record pairs a thread loads together
     const long long st = P.stride;
     for (int part = blockIdx.x; part < dp.np; part += gridDim.x) {
         for (int i = threadIdx.x; i < kDenseKeys; i += blockDim.x) {
@@ -4793,23 +4924,38 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
             if (OPS & 8) mx[i] = (int)0x80000000;
         }
         __syncthreads();
-        const unsigned long long lo = dp.offs[(long long)part * dp.grid], hi = dp.offs[(long long)(part + 1) * dp.grid];
-        for (unsigned long long b0 = lo + threadIdx.x; b0 < hi; b0 += (unsigned long long)kDenseFoldThreads * kInFlight) {
-            uint2 rec[kInFlight];
+        const unsigned long long lo = dp.offs[part], hi = dp.offs[part + 1];
+        // Records in pairs (one 128-bit load) from the first even index at
+        // or below lo, kInFlight pairs a thread in flight; the pairs' halves
+        // outside [lo, hi) are skipped.  Thread 0 keeps the L2 prefetch four
+        // iterations (256 KB) ahead of the loads.
+        const unsigned long long p0 = lo >> 1, p1 = (hi + 1) >> 1;
+        const uint4* pairs = (const uint4*)dp.recs;
+        constexpr unsigned long long kStep = (unsigned long long)kDenseFoldThreads * kInFlight;  // pairs an iteration
+        if (threadIdx.x == 0 && p0 < p1)
+            prefetch_l2_range(pairs + p0, (p1 - p0 < 4 * kStep ? p1 - p0 : 4 * kStep) * sizeof(uint4));
+        for (unsigned long long b0 = p0 + threadIdx.x; b0 < p1; b0 += kStep) {
+            if (threadIdx.x == 0 && b0 + 4 * kStep < p1) {
+                const unsigned long long a = b0 + 4 * kStep;
+                prefetch_l2_range(pairs + a, (p1 - a < kStep ? p1 - a : kStep) * sizeof(uint4));
+            }
+            uint4 pr2[kInFlight];
 #pragma unroll
             for (int j = 0; j < kInFlight; j++) {
                 const unsigned long long i = b0 + (unsigned long long)j * kDenseFoldThreads;
-                rec[j] = i < hi ? __ldcs(dp.recs + i) : make_uint2(0u, 0u);
+                pr2[j] = i < p1 ? __ldcs(pairs + i) : make_uint4(0u, 0u, 0u, 0u);
             }
 #pragma unroll
-            for (int j = 0; j < kInFlight; j++) {
-                if (b0 + (unsigned long long)j * kDenseFoldThreads >= hi) break;
-                const unsigned off = (rec[j].y >> 1) & (unsigned)(kDenseKeys - 1);
-                if (!(rec[j].y & 1u)) {  // a NULL value: the row counts, nothing else
+            for (int h = 0; h < 2 * kInFlight; h++) {
+                const unsigned long long idx = 2 * (b0 + (unsigned long long)(h >> 1) * kDenseFoldThreads) + (h & 1);
+                if (idx < lo || idx >= hi) continue;
+                const uint2 r = (h & 1) ? make_uint2(pr2[h >> 1].z, pr2[h >> 1].w) : make_uint2(pr2[h >> 1].x, pr2[h >> 1].y);
+                const unsigned off = (r.y >> 1) & (unsigned)(kDenseKeys - 1);
+                if (!(r.y & 1u)) {  // a NULL value: the row counts, nothing else
                     atomicAdd(&nul[off], 1u);
                     continue;
                 }
-                const int x = (int)rec[j].x;
+                const int x = (int)r.x;
                 atomicAdd(&cnt[off], 1u);
                 if (OPS & 2) {
                     // x sign-extended to 64 bits: a 32-bit add and its carry
@@ -5677,21 +5823,28 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
     const unsigned long long range = hi - lo;  // keys in the range, less one
     if (range >= (unsigned long long)kDenseMaxParts * kDenseKeys) return nullptr;
     const int np = (int)((range + kDenseKeys) / kDenseKeys);
-    // Worth it when the kept rows would make the direct fold's HBM table
-    // miss L2 (it reaches about 80 G atomics/s) and outnumber the range's
-    // slots, which the fold initialises and flushes partition by partition.
-    auto worth = [&](double kept) { return pinned || (kept >= 4e6 && kept >= 0.25 * (double)np * kDenseKeys); };
+    // Worth it from a million kept rows (below, the direct fold's table sits
+    // in L2), unless the range's slots, which the fold initialises and scans
+    // partition by partition, far outnumber the kept rows.  Measured at 200M
+    // rows over 10M keys: 1.7 ms at 1 % kept against 3.0 ms for the direct
+    // fold, whose HBM table misses L2 (about 80 G atomics/s there).
+    auto worth = [&](double kept) {
+        return pinned || (kept >= 1e6 && (double)np * kDenseKeys <= 16.0 * kept + (double)(1 << 22));
+    };
     if (!worth(kept_est)) return nullptr;
 
     DensePlan dp{};
     dp.lo = lo;
     dp.span = (unsigned long long)np * kDenseKeys;
     dp.np = np;
+    dp.np1 = (np + kDenseFan - 1) >> kDenseFanBits;
     dp.grid = b.sms * 2;
     dp.q = 0;
-    Scratch<unsigned int> counts(s, (size_t)np * dp.grid);
+    Scratch<unsigned int> counts1(s, (size_t)dp.np1 * dp.grid);
+    Scratch<unsigned int> totals(s, (size_t)np, true);
     Scratch<unsigned long long> cnt_out(s, 2, true);
-    dp.counts = counts.get();
+    dp.counts1 = counts1.get();
+    dp.totals = totals.get();
     DenseLean L;
     const bool lean = dense_lean_plan(pred, hb, dp.q, &L);
     const bool k8 = key_type == kInt64;
@@ -5711,15 +5864,25 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
     OXB_CUDA(cudaStreamSynchronize(s->stream));
     if (hc[1] > 0 || !worth((double)hc[0])) return nullptr;
 
-    Scratch<unsigned long long> offs(s, (size_t)np * dp.grid + 1);
-    scan_u32_to_u64(s, b, counts.get(), offs.get(), (long long)np * dp.grid);
+    Scratch<unsigned long long> offs1(s, (size_t)dp.np1 * dp.grid + 1);
+    Scratch<unsigned long long> offs(s, (size_t)np + 1);
+    scan_u32_to_u64(s, b, counts1.get(), offs1.get(), (long long)dp.np1 * dp.grid);
+    scan_u32_to_u64(s, b, totals.get(), offs.get(), np);
+    dp.offs1 = offs1.get();
     dp.offs = offs.get();
     dp.nrecs = hc[0];
-    AllocRef recs_mem = dev_alloc(s, (size_t)std::max<unsigned long long>(hc[0], 1) * sizeof(uint2), false);
+    // an even number of records, so the fold's pair loads stay inside
+    const size_t rec_bytes = (size_t)((hc[0] + 2) & ~1ull) * sizeof(uint2);
+    AllocRef recs1_mem = dev_alloc(s, rec_bytes, false);
+    AllocRef recs_mem = dev_alloc(s, rec_bytes, false);
+    dp.recs1 = (uint2*)recs1_mem->ptr;
     dp.recs = (uint2*)recs_mem->ptr;
     Scratch<unsigned int> status(s, 1, true);
     dp.status = status.get();
     Scratch<unsigned int> gcount(s, (size_t)np);
+    Scratch<long long> cstart(s, (size_t)dp.np1 + 1);
+    Scratch<unsigned int> gcursor(s, (size_t)np);
+    Scratch<unsigned long long> queue(s, 1, true);
 
     const long long cap = (long long)np * kDenseKeys;
     P.capacity = (unsigned int)cap;
@@ -5737,12 +5900,16 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
     auto split = maxacc == 2 ? part_dense_split_kernel<2> : part_dense_split_kernel<4>;
     auto split_lean = maxacc == 2 ? (k8 ? part_dense_split_lean_kernel<2, true> : part_dense_split_lean_kernel<2, false>)
                                   : (k8 ? part_dense_split_lean_kernel<4, true> : part_dense_split_lean_kernel<4, false>);
-    const size_t ssmem = dense_split_smem(np);
+    const size_t ssmem = dense_split_smem(dp.np1);
     set_smem(split, ssmem);
     set_smem(split_lean, ssmem);
     DenseFold fold = dense_fold_for(mask);
     const size_t fsmem = dense_fold_smem(mask);
     set_smem(fold, fsmem);
+    int s2occ = 0;
+    OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s2occ, part_dense_split2_kernel, kDenseThreads, 0));
+    const long long chunks_max = (long long)(hc[0] / kDenseChunk) + dp.np1;
+    const int s2grid = (int)std::max<long long>(1, std::min<long long>(chunks_max, (long long)b.sms * std::max(s2occ, 1)));
     timer.rename("agg_batches_dense");
     timer.begin();
     note_launch(), dense_special_init_kernel<<<1, 64, 0, s->stream>>>(P);
@@ -5750,6 +5917,10 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
         note_launch(), split_lean<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, L, dbatches, nb, nptiles, dp);
     else
         note_launch(), split<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, pred, key_type, dbatches, nb, nptiles, dp);
+    note_launch(), dense_chunks_kernel<<<1, 32, 0, s->stream>>>(dp, cstart.get());
+    note_launch(), dense_cursor_kernel<<<grid_for(b, np, 256, 4), 256, 0, s->stream>>>(dp, gcursor.get());
+    note_launch(), part_dense_split2_kernel<<<s2grid, kDenseThreads, 0, s->stream>>>(dp, cstart.get(), queue.get(),
+                                                                                    gcursor.get());
     note_launch(), fold<<<std::min(np, b.sms), kDenseFoldThreads, fsmem, s->stream>>>(P, dp, ops, gcount.get());
     OXB_CUDA(cudaGetLastError());
     timer.end();
