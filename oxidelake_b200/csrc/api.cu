@@ -546,20 +546,20 @@ oxb_status oxb_download(oxb_backend* backend, oxb_stream* stream, const oxb_batc
             fail(OXB_PLAN, "the batch has " + std::to_string(batch->cols.size()) + " columns, not " +
                                std::to_string(ncols));
         if (ncols > 0 && (!values || !has_validity)) fail(OXB_PLAN, "null output arrays");
+        std::vector<DownloadPiece> pieces;
         for (int i = 0; i < ncols; i++) {
             const Column& c = batch->cols[i];
             has_validity[i] = c.validity ? 1 : 0;
             if (c.length == 0) continue;
             if (!values[i]) fail(OXB_PLAN, "values buffer of column " + std::to_string(i) + " is null");
-            download_bytes(backend->b, s, values[i], c.values, (size_t)c.length * c.width());
+            pieces.push_back(DownloadPiece{values[i], c.values, (size_t)c.length * c.width()});
             st.bytes_d2h += (uint64_t)c.length * c.width();
             if (c.validity && validity && validity[i]) {
-                OXB_CUDA(cudaMemcpyAsync(validity[i], c.validity, ((size_t)c.length + 7) / 8, cudaMemcpyDeviceToHost,
-                                         s->stream));
+                pieces.push_back(DownloadPiece{validity[i], c.validity, ((size_t)c.length + 7) / 8});
                 st.bytes_d2h += ((uint64_t)c.length + 7) / 8;
             }
         }
-        OXB_CUDA(cudaStreamSynchronize(s->stream));
+        download_pieces(backend->b, s, pieces);
         st.rows_in = st.rows_out = (uint64_t)batch->rows;
     });
 }

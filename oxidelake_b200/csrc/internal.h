@@ -83,6 +83,7 @@ struct Backend {
     int force_rpt = 0;
     int stage_threads = 8;            // oxb_set_upload_staging: 0 = off
     std::shared_ptr<Stager> stager;   // made on the first staged upload
+    std::shared_ptr<struct SmallDownloads> small_dl;  // made on the first gathered download
 };
 
 // Queues the copy of n host bytes to device memory on s.  A large pageable
@@ -92,6 +93,16 @@ void upload_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, si
 // The way back: a large pageable `dst` is filled through the same ring and
 // holds every byte on return; any other `dst` is one queued cudaMemcpyAsync.
 void download_bytes(Backend& b, const StreamRef& s, void* dst, const void* src, size_t n);
+// Copies every piece (device src -> host dst, n bytes) and returns once all
+// are in host memory (one stream synchronization).  Small pageable pieces
+// go through one page-locked buffer of the backend, so their copies queue
+// without waiting on each other; large ones through download_bytes.
+struct DownloadPiece {
+    void* dst;
+    const void* src;
+    size_t n;
+};
+void download_pieces(Backend& b, const StreamRef& s, const std::vector<DownloadPiece>& pieces);
 void set_upload_staging(Backend& b, int threads);
 
 // Counts every kernel this library launches (oxb_kernel_launches).
