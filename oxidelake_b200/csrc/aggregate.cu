@@ -4838,7 +4838,7 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_split2_kernel(const 
             rank[j] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
         }
         __syncthreads();
-        if (threadIdx.x < 32) {  // the runs' places in shared memory and in HBM
+        if (threadIdx.x < 32) {  // the runs' places in shared memory
             const unsigned h = threadIdx.x < kDenseFan ? hist[threadIdx.x] : 0u;
             unsigned inc = h;
 #pragma unroll
@@ -4846,12 +4846,13 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_split2_kernel(const 
                 const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
                 if (lane >= o) inc += y;
             }
-            if (threadIdx.x < kDenseFan) {
-                start[threadIdx.x] = inc - h;
-                if (h) gbase[threadIdx.x] = atomicAdd(&gcursor[(a << kDenseFanBits) + threadIdx.x], h);
-            }
+            if (threadIdx.x < kDenseFan) start[threadIdx.x] = inc - h;
         }
         __syncthreads();
+        // ... and in HBM: the reservations' round trip overlaps the other
+        // warps' ordering of the records
+        if (threadIdx.x < kDenseFan && hist[threadIdx.x])
+            gbase[threadIdx.x] = atomicAdd(&gcursor[(a << kDenseFanBits) + threadIdx.x], hist[threadIdx.x]);
 #pragma unroll
         for (int j = 0; j < kSplit2Rows; j++) {
             const unsigned long long i = r0 + threadIdx.x + (unsigned long long)j * kDenseThreads;
@@ -4971,49 +4972,44 @@ __global__ void __launch_bounds__(kDenseFoldThreads, 1) part_dense_fold_kernel(c
             }
         }
         __syncthreads();
-        // Flush: kPer consecutive slots a thread, ranked by a block scan of
-        // the occupied ones.
-        const int s0 = threadIdx.x * kPer;
-        unsigned c = 0;
-#pragma unroll
-        for (int k = 0; k < kPer; k++) c += (nul[s0 + k] | cnt[s0 + k]) != 0u ? 1u : 0u;
+        // Flush in kPer rounds of kDenseFoldThreads consecutive slots, a slot a
+        // thread: the occupied ones, ranked by a block prefix each round, go
+        // to consecutive groups, so consecutive lanes store whole sectors.
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        unsigned inc = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        if (lane == 31) wsum[w] = inc;
-        __syncthreads();
-        if (w == 0) {
-            const unsigned v = lane < (kDenseFoldThreads >> 5) ? wsum[lane] : 0u;
-            unsigned vi = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
-                if (lane >= o) vi += y;
-            }
-            if (lane < (kDenseFoldThreads >> 5)) wsum[lane] = vi - v;
-            if (lane == 31) s_total = vi;
-        }
-        __syncthreads();
-        long long g = (long long)part * kDenseKeys + wsum[w] + inc - c;
         const unsigned long long kbase = dp.lo + (unsigned long long)part * kDenseKeys;
-#pragma unroll
+        unsigned done = 0;  // groups of the rounds before
+#pragma unroll 1
         for (int k = 0; k < kPer; k++) {
-            const int sl = s0 + k;
+            const int sl = k * kDenseFoldThreads + threadIdx.x;
             const unsigned nrows = nul[sl] + cnt[sl];
-            if (!nrows) continue;
-            P.keys[g] = (long long)((kbase + (unsigned long long)sl) ^ kSignBit);
-            P.arr[g] = nrows;
-            if (OPS & 1) P.arr[ops.count_arr * st + g] = cnt[sl];
-            if (OPS & 2) P.arr[ops.sum_arr * st + g] = (unsigned long long)shi[sl] << 32 | slo[sl];
-            if (OPS & 4) P.arr[ops.min_arr * st + g] = (unsigned long long)(long long)mn[sl];
-            if (OPS & 8) P.arr[ops.max_arr * st + g] = (unsigned long long)(long long)mx[sl];
-            g++;
+            const unsigned ball = __ballot_sync(0xffffffffu, nrows != 0u);
+            if (lane == 0) wsum[w] = __popc(ball);
+            __syncthreads();
+            if (w == 0) {
+                const unsigned v = lane < (kDenseFoldThreads >> 5) ? wsum[lane] : 0u;
+                unsigned vi = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, vi, o);
+                    if (lane >= o) vi += y;
+                }
+                if (lane < (kDenseFoldThreads >> 5)) wsum[lane] = vi - v;
+                if (lane == 31) s_total = vi;
+            }
+            __syncthreads();
+            if (nrows) {
+                const long long g = (long long)part * kDenseKeys + done + wsum[w] + __popc(ball & ((1u << lane) - 1u));
+                P.keys[g] = (long long)((kbase + (unsigned long long)sl) ^ kSignBit);
+                P.arr[g] = nrows;
+                if (OPS & 1) P.arr[ops.count_arr * st + g] = cnt[sl];
+                if (OPS & 2) P.arr[ops.sum_arr * st + g] = (unsigned long long)shi[sl] << 32 | slo[sl];
+                if (OPS & 4) P.arr[ops.min_arr * st + g] = (unsigned long long)(long long)mn[sl];
+                if (OPS & 8) P.arr[ops.max_arr * st + g] = (unsigned long long)(long long)mx[sl];
+            }
+            done += s_total;
+            __syncthreads();
         }
-        if (threadIdx.x == 0) gcount[part] = s_total;
+        if (threadIdx.x == 0) gcount[part] = done;
         __syncthreads();
     }
 }
