@@ -4214,14 +4214,15 @@ int compact_ops_of(const AggProgram& P, CompactOps* ops) {
 constexpr int kDenseBits = 13;
 constexpr int kDenseKeys = 1 << kDenseBits;  // keys a partition: the fold's shared table
 constexpr int kDenseMaxParts = 4096;        // so a range of at most 2^25 keys
-constexpr int kDenseThreads = 512;          // the count and split passes
+constexpr int kDenseThreads = 256;          // the count and split passes
+constexpr int kDenseCtas = 4;               // their CTAs an SM (64 registers a thread)
 constexpr int kDenseRows = 8;               // rows a thread in a split sub-tile
 constexpr int kDenseSub = kDenseThreads * kDenseRows;
 constexpr int kDenseFoldThreads = 1024;
 constexpr int kDenseSamples = 16384;
 constexpr int kDenseFanBits = 4;  // final partitions a first-level partition
 constexpr int kDenseFan = 1 << kDenseFanBits;
-constexpr int kDenseChunk = 4096;  // records a chunk of the second split
+constexpr int kDenseChunk = 2048;  // records a chunk of the second split
 constexpr unsigned long long kSignBit = 0x8000000000000000ull;
 static_assert(kDenseSub <= 65536 && kDenseMaxParts <= 65536, "ranks and partitions pack into 16 bits each");
 
@@ -4326,7 +4327,7 @@ __device__ __forceinline__ void dense_count_store(const DensePlan& dp, const uns
 // (dense_count_store).  out[0] gets their number, out[1] the number of
 // kept rows whose key falls outside the range (the host then takes the
 // hashed passes instead).
-__global__ void __launch_bounds__(kDenseThreads) part_dense_count_kernel(const __grid_constant__ DevPredicate pred,
+__global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_count_kernel(const __grid_constant__ DevPredicate pred,
                                                                          int key_type,
                                                                          const BatchCols* __restrict__ batches, int nb,
                                                                          long long ntiles,
@@ -4464,7 +4465,7 @@ __device__ __forceinline__ void dense_stage_store(const DenseStage& st, const De
 // slice, from the count pass).  Kept rows whose key is NULL or INT64_MIN
 // fold straight into their HBM slots.
 template <int MAXACC>
-__global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_kernel(const __grid_constant__ AggProgram P,
+__global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_split_kernel(const __grid_constant__ AggProgram P,
                                                                             const __grid_constant__ DevPredicate pred,
                                                                             int key_type,
                                                                             const BatchCols* __restrict__ batches,
@@ -4640,7 +4641,7 @@ __device__ __forceinline__ unsigned lean_rows(const DenseLean& L, const BatchCol
 
 // The count pass, compiled (part_dense_count_kernel's contract).
 template <bool K8>
-__global__ void __launch_bounds__(kDenseThreads) part_dense_count_lean_kernel(const __grid_constant__ DenseLean L,
+__global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_count_lean_kernel(const __grid_constant__ DenseLean L,
                                                                               const BatchCols* __restrict__ batches,
                                                                               int nb, long long ntiles,
                                                                               const __grid_constant__ DensePlan dp,
@@ -4689,7 +4690,7 @@ __global__ void __launch_bounds__(kDenseThreads) part_dense_count_lean_kernel(co
 // The first split, compiled (part_dense_split_kernel's contract; rows
 // whose key is INT64_MIN fold into their HBM slot).
 template <int MAXACC, bool K8>
-__global__ void __launch_bounds__(kDenseThreads, 2) part_dense_split_lean_kernel(
+__global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_split_lean_kernel(
     const __grid_constant__ AggProgram P, const __grid_constant__ DenseLean L, const BatchCols* __restrict__ batches,
     int nb, long long ntiles, const __grid_constant__ DensePlan dp) {
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -4794,7 +4795,7 @@ __global__ void dense_cursor_kernel(const __grid_constant__ DensePlan dp, unsign
 // shared memory in run order (runs of about kDenseChunk / kDenseFan records,
 // whole sectors).
 constexpr int kSplit2Rows = kDenseChunk / kDenseThreads;
-__global__ void __launch_bounds__(kDenseThreads) part_dense_split2_kernel(const __grid_constant__ DensePlan dp,
+__global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_split2_kernel(const __grid_constant__ DensePlan dp,
                                                                           const long long* __restrict__ cstart,
                                                                           unsigned long long* __restrict__ queue,
                                                                           unsigned int* __restrict__ gcursor) {
@@ -5834,7 +5835,7 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
     dp.span = (unsigned long long)np * kDenseKeys;
     dp.np = np;
     dp.np1 = (np + kDenseFan - 1) >> kDenseFanBits;
-    dp.grid = b.sms * 2;
+    dp.grid = b.sms * kDenseCtas;
     dp.q = 0;
     Scratch<unsigned int> counts1(s, (size_t)dp.np1 * dp.grid);
     Scratch<unsigned int> totals(s, (size_t)np, true);
