@@ -50,6 +50,7 @@ def measure(backend, stream, batches, selectivity_pct: int, repeats: int = 2, do
     kms, call = [], []
     name, groups, out = None, 0, None
     for _ in range(repeats):
+        out = None  # the last call's groups freed first, so the pool already holds this call's memory
         t0 = time.perf_counter()
         out = b.aggregate_batches(s, batches, spec, pred)
         groups = out.num_rows()
