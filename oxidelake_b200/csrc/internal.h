@@ -204,7 +204,14 @@ struct JoinTableDev {
     // Smallest and largest key placed in the slots (key_lo > key_hi: none).
     long long key_lo = 0;
     long long key_hi = -1;
+    // Unique keys that fill their range (the dense build): the run start of
+    // key dense_lo + d at dense[d], or kNoRun for a key the build lacks;
+    // null otherwise.  A probe then reads 4 bytes instead of a 16-byte slot.
+    const unsigned int* dense = nullptr;
+    long long dense_lo = 0;
+    unsigned long long dense_n = 0;
 };
+constexpr unsigned int kNoRun = 0xffffffffu;
 
 }  // namespace oxb
 
@@ -221,7 +228,7 @@ struct oxb_vector_index {
 
 struct oxb_join_table {
     oxb::JoinTableDev t;
-    oxb::AllocRef slots_mem, rows_mem;
+    oxb::AllocRef slots_mem, rows_mem, dense_mem;
     const oxb_batch* build = nullptr;
     long long build_rows = 0;
 };

@@ -107,6 +107,14 @@ __global__ void join_dense_place_kernel(const void* __restrict__ kv, const uint8
     }
 }
 
+// Dense build, step 3: the direct index of the probe, the run start of each
+// key offset (its position in key order) or kNoRun where no row has it.
+__global__ void join_dense_index_kernel(const unsigned int* __restrict__ cnt, const unsigned long long* __restrict__ pos,
+                                        long long m, unsigned int* __restrict__ index) {
+    for (long long d = blockIdx.x * (long long)blockDim.x + threadIdx.x; d < m; d += (long long)gridDim.x * blockDim.x)
+        index[d] = cnt[d] ? (unsigned int)pos[d] : kNoRun;
+}
+
 // Device build step 2: 1 where a run of equal keys starts.
 __global__ void join_heads_kernel(const unsigned long long* __restrict__ ukeys, long long nvalid,
                                   unsigned int* __restrict__ heads) {
@@ -145,6 +153,15 @@ __device__ __forceinline__ bool join_lookup(const JoinTableDev& t, long long key
         *start = t.special_start;
         *count = t.special_count;
         return *count > 0;
+    }
+    if (t.dense) {  // unique keys filling their range: one 4-byte read
+        const unsigned long long d = (unsigned long long)key - (unsigned long long)t.dense_lo;
+        if (d >= t.dense_n) return false;
+        const unsigned int v = __ldg(t.dense + d);
+        if (v == kNoRun) return false;
+        *start = v;
+        *count = 1u;
+        return true;
     }
     unsigned int s = (unsigned int)(fmix64((unsigned long long)key) & (t.capacity - 1u));
     for (unsigned int p = 0; p < t.capacity; p++) {
@@ -471,7 +488,13 @@ oxb_join_table* prepare_join_build_impl(const StreamRef& s, const Backend& b, co
                 note_launch(), join_dense_place_kernel<<<grid, 256, 0, s->stream>>>(
                     key.values, key.validity, key.type, n, lo, pos.get(), t.rows, rkeys.get(), rstart.get(),
                     rcount.get());
+                out->dense_mem = dev_alloc(s, (size_t)m * 4, false);
+                note_launch(), join_dense_index_kernel<<<grid_for(b, m, 256, 8), 256, 0, s->stream>>>(
+                    cnt.get(), pos.get(), m, (unsigned int*)out->dense_mem->ptr);
                 OXB_CUDA(cudaGetLastError());
+                t.dense = (const unsigned int*)out->dense_mem->ptr;
+                t.dense_lo = lo;
+                t.dense_n = (unsigned long long)m;
                 placed = true;
             }
         }

@@ -143,14 +143,18 @@ def test_one_key_everywhere(backend, stream):
 @pytest.mark.parametrize("dup", [False, True], ids=["unique", "one-repeat"])
 def test_dense_keys_placed_without_sort(backend, stream, key_type, dup):
     """Build keys that fill their range: unique ones are placed by key offset
-    (no sort), a single repeated key sends the build back to the sort; both
-    give the oracle's table, matches and gathered rows."""
+    (no sort) and probed through the direct index, a single repeated key
+    sends the build back to the sort; both give the oracle's table, matches
+    and gathered rows, for probe keys missing inside the range and outside
+    it on both sides."""
     rng = np.random.default_rng(11 + dup)
     nb, npr = 200_000, 600_000
     bk = (rng.permutation(nb) - 70_000).astype(key_type.to_pandas_dtype())
     if dup:
         bk[5] = bk[123_456]
     pk = rng.integers(-80_000, 140_000, npr).astype(key_type.to_pandas_dtype())
+    if key_type == pa.int64():
+        pk[7] = np.iinfo(np.int64).min  # no build row has it: no match through the direct index
     build = pa.RecordBatch.from_arrays(
         [pa.array(bk, key_type, mask=rng.random(nb) < 0.03), pa.array(np.arange(nb, dtype=np.int64))], names=["bk", "bv"]
     )
