@@ -310,3 +310,43 @@ def test_dense_range_two_leaf_where(backend, stream):
     _, w = want(batches, spec, pred)
     assert got.num_rows == w.num_rows
     assert_batches_equal(got, w)
+
+
+@pytest.mark.parametrize("end", ["top", "bottom"])
+def test_dense_range_at_the_ends_of_int64(backend, stream, end):
+    """Keys within 100K of INT64_MAX, or of INT64_MIN with INT64_MIN itself
+    among them (its own slot, emitted first): the widened range is clamped
+    at the ends of the Int64 order, and the groups still equal the oracle's."""
+    rng = np.random.default_rng(5 if end == "top" else 6)
+    i64 = np.iinfo(np.int64)
+    batches = []
+    for n in (70_000, 3, 130_001):
+        off = rng.integers(0, 100_000, n).astype(np.int64)
+        g = i64.max - off if end == "top" else i64.min + 1 + off
+        if end == "bottom" and n > 10:
+            g[:4] = i64.min
+        x = rng.integers(-1000, 1000, n).astype(np.int32)
+        batches.append(pa.RecordBatch.from_arrays([pa.array(g), pa.array(x, mask=rng.random(n) < 0.05)], names=["g", "x"]))
+    spec = AggregateSpec(0, [(F.Sum, 1), (F.Min, 1), (F.Max, 1), (F.Count, 1), (F.CountStar, 0)])
+    got, name = _fold_named(backend, stream, batches, spec, None, 17)
+    assert name == "agg_batches_dense", name
+    _, w = want(batches, spec, None)
+    assert got.num_rows == w.num_rows
+    assert_batches_equal(got, w)
+
+
+def test_dense_range_where_keeping_nothing_in_range(backend, stream):
+    """A WHERE that keeps only rows whose key is NULL: no record reaches the
+    dense passes, and the only group is the NULL one."""
+    rng = np.random.default_rng(9)
+    n = 300_000
+    g = rng.integers(0, 50_000, n).astype(np.int64)
+    nullkey = rng.random(n) < 0.1
+    f = np.where(nullkey, 1, 0).astype(np.int32)
+    x = rng.integers(-5, 5, n).astype(np.int32)
+    batch = pa.RecordBatch.from_arrays([pa.array(g, mask=nullkey), pa.array(x), pa.array(f)], names=["g", "x", "f"])
+    pred = compare(2, Cmp.Eq, Literal.int32(1))
+    got, _ = _fold_named(backend, stream, [batch], SPEC, pred, 17)
+    _, w = want([batch], SPEC, pred)
+    assert got.num_rows == w.num_rows == 1
+    assert_batches_equal(got, w)
