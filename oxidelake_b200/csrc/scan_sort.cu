@@ -103,32 +103,46 @@ __global__ void scan_partials_kernel(unsigned long long* __restrict__ p, long lo
     if (threadIdx.x == 0) p[m] = total;
 }
 
+// The offsets of one block's counts.  A thread scans 16 consecutive counts,
+// so its 16 offsets are consecutive too; they are staged in shared memory
+// (one u64 of padding every 16, so the lanes' rows fall in different banks)
+// and stored by consecutive threads to consecutive addresses.  Stored
+// straight from registers, each warp store touched 32 lines with 8 bytes
+// apiece, and L2 filled the part-written sectors from DRAM.
+constexpr int kScanPad = kScanChunk + kScanChunk / kScanItems;
 __global__ void scan_apply_kernel(const unsigned int* __restrict__ counts, long long n,
                                   const unsigned long long* __restrict__ partials,
                                   unsigned long long* __restrict__ offsets) {
-    __shared__ unsigned int tile[kScanChunk];
+    __shared__ unsigned long long stage[kScanPad];  // the counts first (as u32), then the offsets
     __shared__ unsigned long long warp_sums[32];
-    long long base = (long long)blockIdx.x * kScanChunk;
+    unsigned int* tile = (unsigned int*)stage;
+    const long long base = (long long)blockIdx.x * kScanChunk;
     for (int i = threadIdx.x; i < kScanChunk; i += kScanThreads) {
-        long long idx = base + i;
+        const long long idx = base + i;
         tile[i] = idx < n ? counts[idx] : 0u;
     }
     __syncthreads();
+    unsigned int c[kScanItems];
     unsigned long long s = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) s += tile[threadIdx.x * kScanItems + i];
-    unsigned long long total;
-    unsigned long long run = block_exclusive_scan(s, warp_sums, &total) + partials[blockIdx.x];
-    unsigned long long out[kScanItems];
-#pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        out[i] = run;
-        run += tile[threadIdx.x * kScanItems + i];
+        c[i] = tile[threadIdx.x * kScanItems + i];
+        s += c[i];
     }
+    unsigned long long total;
+    unsigned long long run = block_exclusive_scan(s, warp_sums, &total) + partials[blockIdx.x];  // ends synchronised
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        long long idx = base + (long long)threadIdx.x * kScanItems + i;
-        if (idx < n) offsets[idx] = out[i];
+        const int j = threadIdx.x * kScanItems + i;
+        stage[j + j / kScanItems] = run;
+        run += c[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const int j = k * kScanThreads + threadIdx.x;
+        const long long idx = base + j;
+        if (idx < n) offsets[idx] = stage[j + j / kScanItems];
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) offsets[n] = partials[gridDim.x];
 }
