@@ -284,16 +284,30 @@ __global__ void __launch_bounds__(kGatherThreads) join_gather_kernel(
     long long ntrows, long long right_rows, unsigned long long first, long long rows,
     const __grid_constant__ DevGather g, unsigned int* __restrict__ status) {
     __shared__ unsigned long long offs[kGatherRegion + 1];
+    __shared__ unsigned short out_row[kGatherTile];  // each output's probe row, less r0
     const int lane = threadIdx.x & 31;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long r0 = tile_row[tile], r1 = tile_row[tile + 1];
         const long long span = r1 - r0 + 2;  // offsets[r0 .. r1 + 1]
         const bool local = span <= kGatherRegion + 1;
-        __syncthreads();  // the previous tile's searches are done with offs
+        __syncthreads();  // the previous tile's outputs are done with offs and out_row
         if (local)
             for (long long i = threadIdx.x; i < span; i += blockDim.x) offs[i] = offsets[r0 + i];
         __syncthreads();
         const long long t0 = tile * kGatherTile;
+        if (local) {
+            // Each probe row of the tile marks its outputs' slots with its
+            // index, so an output finds its row with one shared read instead
+            // of a binary search.
+            const unsigned long long tlo = first + (unsigned long long)t0;
+            const unsigned long long thi = tlo + kGatherTile;
+            for (long long i = threadIdx.x; i < span - 1; i += blockDim.x) {
+                const unsigned long long a = offs[i] > tlo ? offs[i] : tlo;
+                const unsigned long long e = offs[i + 1] < thi ? offs[i + 1] : thi;
+                for (unsigned long long q = a; q < e; q++) out_row[q - tlo] = (unsigned short)i;
+            }
+            __syncthreads();
+        }
         constexpr int R = kGatherTile / kGatherThreads;
         // Each output's probe and build rows first, all R of a thread's
         // outputs, then every column's R values loaded before any is stored.
@@ -307,12 +321,7 @@ __global__ void __launch_bounds__(kGatherThreads) join_gather_kernel(
             long long lrow;
             unsigned long long base;
             if (local) {  // offs[0] <= p < offs[span - 1]
-                long long lo = 0, hi = span - 1;
-                while (hi - lo > 1) {
-                    const long long mid = (lo + hi) >> 1;
-                    if (offs[mid] <= p) lo = mid;
-                    else hi = mid;
-                }
+                const int lo = out_row[t - t0];
                 lrow = r0 + lo;
                 base = offs[lo];
             } else {
