@@ -183,8 +183,24 @@ __device__ __forceinline__ bool join_lookup(const JoinTableDev& t, long long key
 // reduce pass of its own.
 constexpr int kProbeThreads = 256;
 
+// Compiled for the key's type (KT: kInt64 or kInt32) and for a table with a
+// direct index (DENSE), so a row's lookup carries no switch on either.
+template <int KT, bool DENSE>
+__device__ __forceinline__ bool probe_lookup(const JoinTableDev& t, long long key, unsigned int* start,
+                                             unsigned int* count) {
+    if (DENSE && key != kEmptyKey) {
+        const unsigned long long d = (unsigned long long)key - (unsigned long long)t.dense_lo;
+        const unsigned int v = d < t.dense_n ? __ldg(t.dense + d) : kNoRun;
+        *start = v;
+        *count = v != kNoRun ? 1u : 0u;
+        return v != kNoRun;
+    }
+    return join_lookup(t, key, start, count);
+}
+
+template <int KT, bool DENSE>
 __global__ void __launch_bounds__(kProbeThreads) join_probe_kernel(
-    const __grid_constant__ JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid, int type,
+    const __grid_constant__ JoinTableDev t, const void* __restrict__ kv, const uint8_t* __restrict__ kvalid,
     long long n, long long block_rows, unsigned int* __restrict__ counts, unsigned int* __restrict__ starts,
     unsigned long long* __restrict__ totals) {
     __shared__ unsigned long long warp_sums[kProbeThreads / 32];
@@ -201,14 +217,14 @@ __global__ void __launch_bounds__(kProbeThreads) join_probe_kernel(
             for (int k = 0; k < 4; k++) {
                 const long long i = i0 + k * kProbeThreads + threadIdx.x;
                 live[k] = i < end && valid_at(kvalid, i);
-                key[k] = live[k] ? join_key_at(kv, type, i) : 0;
+                key[k] = !live[k] ? 0 : KT == kInt64 ? __ldg((const long long*)kv + i) : (long long)__ldg((const int*)kv + i);
             }
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const long long i = i0 + k * kProbeThreads + threadIdx.x;
                 if (i >= end) continue;
                 unsigned int st = 0, c = 0;
-                if (live[k] && !join_lookup(t, key[k], &st, &c)) st = c = 0;
+                if (live[k] && !probe_lookup<KT, DENSE>(t, key[k], &st, &c)) st = c = 0;
                 counts[i] = c;
                 starts[i] = st;
                 sum += c;
@@ -616,9 +632,11 @@ oxb_join_matches* probe_join(const StreamRef& s, const Backend& b, const oxb_joi
         Scratch<unsigned long long> totals(s, nblocks + 1);
         KernelTimer timer(b, s, "join_probe_kernel+scan");  // the probe and its offsets' scan
         timer.begin();
-        note_launch(), join_probe_kernel<<<grid_for(b, nblocks * kProbeThreads, kProbeThreads, 8), kProbeThreads, 0,
-                                           s->stream>>>(a.table->t, key.values, key.validity, key.type, n, block_rows,
-                                                        counts.get(), starts, totals.get());
+        const bool dense = a.table->t.dense != nullptr;
+        auto probe = key.type == kInt64 ? (dense ? join_probe_kernel<kInt64, true> : join_probe_kernel<kInt64, false>)
+                                        : (dense ? join_probe_kernel<kInt32, true> : join_probe_kernel<kInt32, false>);
+        note_launch(), probe<<<grid_for(b, nblocks * kProbeThreads, kProbeThreads, 8), kProbeThreads, 0, s->stream>>>(
+            a.table->t, key.values, key.validity, n, block_rows, counts.get(), starts, totals.get());
         OXB_CUDA(cudaGetLastError());
         scan_u32_to_u64_from_totals(s, counts.get(), offsets, n, totals.get());
         timer.end();
