@@ -5714,7 +5714,7 @@ oxb_batch* run_aggregate(const StreamRef& s, const Backend& b, AggPlan& plan, co
 
 template <typename K>
 void set_smem(K kernel, size_t smem) {
-    if (smem > 48 * 1024) OXB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_smem(kernel, smem);
 }
 
 // As many CTAs as fit on the GPU at once (the row loops are grid-strided),

@@ -1075,7 +1075,7 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         sp.bounds = bounds.get();
         sp.status = status.get();
         const size_t smem = scan_smem(stages, C);
-        OXB_CUDA(cudaFuncSetAttribute(topk_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        allow_smem(topk_scan_kernel, smem);
         if (!compact) timer.begin();  // a compacted scan's segment began with the copy
         note_launch(), topk_scan_kernel<<<grid, kScanThreads, smem, s->stream>>>(qmap, compact ? cmap : ix.xmap, sp);
         timer.end();
@@ -1112,7 +1112,7 @@ void vector_topk(const StreamRef& s, const Backend& b, const oxb_vector_topk_arg
         fp.ex_cap = std::min(pool_cap, kExactMax);
         const size_t fsmem = (size_t)(fp.pool_cap + fp.ex_cap) * 8 + (size_t)dim * 4;
         if (fsmem + 12 * 1024 > b.smem_optin) fail(OXB_UNSUPPORTED, "vector dimension too large for the re-rank kernel");
-        OXB_CUDA(cudaFuncSetAttribute(topk_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+        allow_smem(topk_final_kernel, fsmem);
         note_launch(), topk_final_kernel<<<nq, kFinalThreads, fsmem, s->stream>>>(fp);
         OXB_CUDA(cudaGetLastError());
         uint32_t hs = 0;

@@ -190,9 +190,7 @@ void launch_vector_distance(const StreamRef& s, const Backend& b, const Column& 
     if (vec.dim >= kDimChunk && vec.dim % 4 == 0 && ((uintptr_t)vec.values & 15) == 0 &&
         async_smem <= b.smem_optin) {
         const size_t smem = async_smem;
-        if (smem > 48 * 1024)
-            OXB_CUDA(cudaFuncSetAttribute(vector_distance_async_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+        allow_smem(vector_distance_async_kernel, smem);
         int per_sm = 0;
         OXB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vector_distance_async_kernel, kRowsPerBlock, smem));
         const long long blocks = (n + kRowsPerBlock - 1) / kRowsPerBlock;
