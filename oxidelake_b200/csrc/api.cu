@@ -5,6 +5,7 @@
 // and nothing falls back to the CPU.
 #include <chrono>
 #include <cstdio>
+#include <map>
 #include <new>
 #include <thread>
 
@@ -95,6 +96,24 @@ DevAlloc::~DevAlloc() {
         cudaSetDevice(stream->device);
         cudaFreeAsync(ptr, stream->stream);
     }
+}
+
+int allow_smem_cap(const void* kernel) {
+    int dev = 0;
+    OXB_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> caps;
+    std::lock_guard<std::mutex> l(mu);
+    const auto it = caps.find({kernel, dev});
+    if (it != caps.end()) return it->second;
+    int optin = 0;
+    OXB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    OXB_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    const int cap = optin - (int)fa.sharedSizeBytes;
+    if (cap > 48 * 1024) OXB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
+    caps[{kernel, dev}] = cap;
+    return cap;
 }
 
 AllocRef dev_alloc(const StreamRef& s, size_t bytes, bool zero) {

@@ -245,25 +245,23 @@ namespace oxb {
 
 // ---- helpers shared by the operators --------------------------------------
 
-// Lets `kernel` launch with `smem` bytes of dynamic shared memory.  The
-// attribute belongs to the function, not to a launch, so it is raised to the
-// device's opt-in maximum and never set to one call's size: host threads
-// that launch the same kernel with different sizes at once (the serving
-// loop's workers) would otherwise lower it between another thread's setting
-// and its launch, which then fails with "invalid argument".
+// The dynamic shared memory `kernel` may use on the current device: the
+// device's opt-in maximum less the kernel's static shared memory.  The
+// function's limit is raised to it on the first call for a kernel and device
+// (under a lock, so no launch of that kernel precedes it) and never set to
+// one call's size: host threads launching the same kernel with different
+// sizes at once (the serving loop's workers) would otherwise lower it
+// between another thread's setting and its launch, which then fails with
+// "invalid argument".
+int allow_smem_cap(const void* kernel);
+
 template <typename K>
 void allow_smem(K kernel, size_t smem) {
     if (smem <= 48 * 1024) return;
-    int dev = 0, optin = 0;
-    OXB_CUDA(cudaGetDevice(&dev));
-    OXB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fa{};
-    OXB_CUDA(cudaFuncGetAttributes(&fa, kernel));
-    const int cap = optin - (int)fa.sharedSizeBytes;  // what the kernel's static shared memory leaves
-    if (cap < 0 || smem > (size_t)cap)
+    const int cap = allow_smem_cap((const void*)kernel);
+    if (smem > (size_t)cap)
         fail(OXB_UNSUPPORTED, std::to_string(smem) + " bytes of dynamic shared memory exceed the " +
                                   std::to_string(cap) + " the device leaves this kernel");
-    OXB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, cap));
 }
 
 inline int grid_for(const Backend& b, long long work, int threads, int per_sm = 4) {
