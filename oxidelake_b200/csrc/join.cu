@@ -294,7 +294,7 @@ __global__ void join_tile_rows_kernel(const unsigned long long* __restrict__ off
     }
 }
 
-__global__ void __launch_bounds__(kGatherThreads) join_gather_kernel(
+__global__ void __launch_bounds__(kGatherThreads, 4) join_gather_kernel(
     const unsigned long long* __restrict__ offsets, const unsigned int* __restrict__ starts,
     const long long* __restrict__ tile_row, long long ntiles, const unsigned int* __restrict__ trows,
     long long ntrows, long long right_rows, unsigned long long first, long long rows,
@@ -356,7 +356,36 @@ __global__ void __launch_bounds__(kGatherThreads) join_gather_kernel(
         }
         for (int ci = 0; ci < g.ncols; ci++) {
             const DevGatherCol& c = g.cols[ci];
-            if (c.width == 8 || c.width == 4) {
+            const DevGatherCol& c2 = g.cols[ci + 1 < g.ncols ? ci + 1 : ci];
+            const bool narrow = c.width == 8 || c.width == 4;
+            if (narrow && ci + 1 < g.ncols && (c2.width == 8 || c2.width == 4) && !c.dst_valid && !c2.dst_valid) {
+                // Two narrow columns without bitmaps: both columns' values in
+                // flight before either is stored.
+                unsigned long long v[R], w[R];
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    const long long s1 = c.side == 0 ? lr[k] : rr[k], s2 = c2.side == 0 ? lr[k] : rr[k];
+                    v[k] = t >= rows ? 0ull
+                           : c.width == 8 ? __ldg((const unsigned long long*)c.src + s1)
+                                          : (unsigned long long)__ldg((const unsigned int*)c.src + s1);
+                    w[k] = t >= rows ? 0ull
+                           : c2.width == 8 ? __ldg((const unsigned long long*)c2.src + s2)
+                                           : (unsigned long long)__ldg((const unsigned int*)c2.src + s2);
+                }
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const long long t = t0 + k * kGatherThreads + threadIdx.x;
+                    if (t >= rows) continue;
+                    if (c.width == 8) ((unsigned long long*)c.dst)[t] = v[k];
+                    else ((unsigned int*)c.dst)[t] = (unsigned int)v[k];
+                    if (c2.width == 8) ((unsigned long long*)c2.dst)[t] = w[k];
+                    else ((unsigned int*)c2.dst)[t] = (unsigned int)w[k];
+                }
+                ci++;
+                continue;
+            }
+            if (narrow) {
                 unsigned long long v[R];
 #pragma unroll
                 for (int k = 0; k < R; k++) {
