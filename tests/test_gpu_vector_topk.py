@@ -166,3 +166,40 @@ def test_selective_where_with_per_query_literals(backend, stream, metric):
     none = compare(1, Cmp.Lt, Literal.int64(0))
     ids0, dist0, _ = backend.vector_topk(stream, ix, dev, none, q[:3], k, metric)
     assert (ids0 == -1).all() and np.isnan(dist0).all()
+
+
+def test_concurrent_calls_with_different_shared_memory(backend):
+    """Host threads on their own streams run top-k calls with different k at
+    once, so the scan and re-rank launch with different shared-memory sizes
+    concurrently: every call equals the same call made alone."""
+    import threading
+
+    batch, _ = table(60_000, 128, seed=31)
+    s0 = backend.create_stream()
+    dev = backend.upload(s0, batch)
+    ix = backend.vector_index(s0, dev, 2)
+    rng = np.random.default_rng(32)
+    calls = [(rng.standard_normal((3, 128)).astype(np.float32), k, compare(1, Cmp.Lt, Literal.int64(20 + 7 * i)))
+             for i, k in enumerate([1, 5, 10, 32, 64, 100] * 2)]
+    want = [backend.vector_topk(s0, ix, dev, p, q, k, DistanceMetric.L2)[:2] for q, k, p in calls]
+    got = [None] * len(calls)
+    errors = []
+
+    def worker(w):
+        s = backend.create_stream()
+        try:
+            for rep in range(3):
+                for i in range(w, len(calls), 4):
+                    q, k, p = calls[i]
+                    got[i] = backend.vector_topk(s, ix, dev, p, q, k, DistanceMetric.L2)[:2]
+        except Exception as e:  # reported below, on the test's thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(w,)) for w in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for (gi, gd), (wi, wd) in zip(got, want):
+        check(gi, gd, wi, wd)
