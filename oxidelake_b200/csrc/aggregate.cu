@@ -4769,16 +4769,20 @@ __global__ void __launch_bounds__(kDenseThreads, kDenseCtas) part_dense_split_le
 }
 
 // The first chunk of each first-level partition's records (kDenseChunk a
-// chunk) and, at [np1], their total: one thread, np1 is small.
-__global__ void dense_chunks_kernel(const __grid_constant__ DensePlan dp, long long* __restrict__ cstart) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    long long c = 0;
-    for (int k = 0; k < dp.np1; k++) {
-        cstart[k] = c;
+// chunk) and, at [np1], their total: one block of 256 threads (np1 is at
+// most kDenseMaxParts / kDenseFan = 256) and one block scan.
+static_assert(kDenseMaxParts / kDenseFan <= 256, "one thread a first-level partition");
+__global__ void __launch_bounds__(256) dense_chunks_kernel(const __grid_constant__ DensePlan dp,
+                                                           long long* __restrict__ cstart) {
+    __shared__ unsigned cnt[256], pre[256], wsum[8], total;
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) {
         const unsigned long long n = dp.offs1[(long long)(k + 1) * dp.grid] - dp.offs1[(long long)k * dp.grid];
-        c += (long long)((n + kDenseChunk - 1) / kDenseChunk);
+        cnt[k] = (unsigned)((n + kDenseChunk - 1) / kDenseChunk);
     }
-    cstart[dp.np1] = c;
+    __syncthreads();
+    block_exclusive_scan(cnt, pre, dp.np1, wsum, &total);
+    for (int k = threadIdx.x; k < dp.np1; k += blockDim.x) cstart[k] = pre[k];
+    if (threadIdx.x == 0) cstart[dp.np1] = total;
 }
 
 // Each final partition's next record in the second split: its start.
@@ -5914,7 +5918,7 @@ oxb_batch* aggregate_dense(const StreamRef& s, const Backend& b, const AggPlan& 
         note_launch(), split_lean<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, L, dbatches, nb, nptiles, dp);
     else
         note_launch(), split<<<dp.grid, kDenseThreads, ssmem, s->stream>>>(P, pred, key_type, dbatches, nb, nptiles, dp);
-    note_launch(), dense_chunks_kernel<<<1, 32, 0, s->stream>>>(dp, cstart.get());
+    note_launch(), dense_chunks_kernel<<<1, 256, 0, s->stream>>>(dp, cstart.get());
     note_launch(), dense_cursor_kernel<<<grid_for(b, np, 256, 4), 256, 0, s->stream>>>(dp, gcursor.get());
     note_launch(), part_dense_split2_kernel<<<s2grid, kDenseThreads, 0, s->stream>>>(dp, cstart.get(), queue.get(),
                                                                                     gcursor.get());
