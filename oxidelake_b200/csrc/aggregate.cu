@@ -5033,26 +5033,24 @@ DenseFold dense_fold_for(int ops) {
 
 // The dense fold's groups in key order for agg_emit_kernel (whose key is
 // skeys[r] ^ sign bit, with lo = 0): the key INT64_MIN first when its slot
-// [capacity + 1] holds rows, then every partition's compacted groups.
+// [capacity + 1] holds rows, then every partition's compacted groups, one
+// block a partition, so each group's row is its partition's first plus its
+// index there.
 __global__ void dense_order_kernel(const __grid_constant__ AggProgram P, const unsigned long long* __restrict__ gpre,
-                                   int np, long long G, int has_min, unsigned long long* __restrict__ skeys,
+                                   int np, int has_min, unsigned long long* __restrict__ skeys,
                                    unsigned int* __restrict__ sslots) {
-    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < G; r += (long long)gridDim.x * blockDim.x) {
-        if (has_min && r == 0) {
-            skeys[0] = 0;  // INT64_MIN ^ sign bit
-            sslots[0] = (unsigned)(P.capacity + 1);
-            continue;
+    if (has_min && blockIdx.x == 0 && threadIdx.x == 0) {
+        skeys[0] = 0;  // INT64_MIN ^ sign bit
+        sslots[0] = (unsigned)(P.capacity + 1);
+    }
+    for (int p = blockIdx.x; p < np; p += gridDim.x) {
+        const unsigned long long r0 = gpre[p] + (unsigned long long)has_min;
+        const long long n = (long long)(gpre[p + 1] - gpre[p]);
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+            const long long slot = (long long)p * kDenseKeys + i;
+            sslots[r0 + i] = (unsigned)slot;
+            skeys[r0 + i] = (unsigned long long)P.keys[slot] ^ kSignBit;
         }
-        const unsigned long long rr = (unsigned long long)(r - has_min);
-        int a = 0, b = np - 1;  // the last partition whose first group is at or before rr
-        while (a < b) {
-            const int mid = (a + b + 1) >> 1;
-            if (gpre[mid] <= rr) a = mid;
-            else b = mid - 1;
-        }
-        const long long slot = (long long)a * kDenseKeys + (long long)(rr - gpre[a]);
-        sslots[r] = (unsigned)slot;
-        skeys[r] = (unsigned long long)P.keys[slot] ^ kSignBit;
     }
 }
 
@@ -5755,8 +5753,8 @@ oxb_batch* emit_dense(const StreamRef& s, const Backend& b, const AggPlan& plan,
     Scratch<unsigned long long> skeys(s, G + 1);
     Scratch<unsigned int> sslots(s, G + 1);
     if (G > 0) {
-        note_launch(), dense_order_kernel<<<grid_for(b, G, 256, 8), 256, 0, s->stream>>>(P, gpre.get(), dp.np, G, has_min,
-                                                                                        skeys.get(), sslots.get());
+        note_launch(), dense_order_kernel<<<std::min(dp.np, b.sms * 8), 256, 0, s->stream>>>(P, gpre.get(), dp.np, has_min,
+                                                                                           skeys.get(), sslots.get());
         OXB_CUDA(cudaGetLastError());
     }
     return emit_ordered(s, b, plan, P, skeys.get(), sslots.get(), 0, G, h.null_rows > 0);
